@@ -1,0 +1,414 @@
+"""Benchmark: UltraGauss slice splatting fwd+bwd frames/s on B200 (batched vs plain).
+
+Workload (headline scene): 1,000,000 anisotropic Gaussians in a 64 mm cube (means uniform,
+log-scales N(log 1 mm, 0.3), random unit quaternions, intensity U(0,1), opacity
+sigmoid(N(0,1)), seed 0); frames 512x512 px at 0.125 mm from a linear sweep (2 mm steps,
+tilt N(0, 2 deg)); 16 frames per step; L1 loss against seeded U(0,1) targets. A step is
+fwd + loss gradient + bwd of all 16 frames (gradients summed over frames).
+
+  value      batched form: one binning, one forward and one adjoint launch sequence for the
+             16 frames, inputs resident in HBM;
+  plain      one frame per launch sequence (the reference's calling pattern);
+  e2e        batched form through the public autograd API with pinned host inputs: per step
+             H2D of parameters, pixel positions and targets, D2H of loss and gradients.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+Multi-GPU (replicas over frames, no collective): torchrun --nproc-per-node N bench.py --gpus N
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "ultrasound-3d-reconstruction_b200"))
+sys.path.insert(0, str(ROOT))
+
+METRIC = "fwd+bwd frames/s @1M Gaussians 512² (batched vs plain, 1 B200); % HBM roofline"
+UNIT = "frames/s"
+BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (params, grads, outputs, upstream)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--gaussians", type=int, default=1_000_000)
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--spacing", type=float, default=0.125)
+    ap.add_argument("--frames-per-step", type=int, default=16)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(a, world):
+    return {
+        "workload": (f"ultragauss slice splatting fwd+bwd, {a.gaussians} Gaussians (64 mm cube), "
+                     f"{a.size}x{a.size} px @ {a.spacing} mm, {a.frames_per_step} frames/step per GPU"),
+        "gaussians": a.gaussians,
+        "frame_px": [a.size, a.size],
+        "pixel_mm": a.spacing,
+        "frames_per_step": a.frames_per_step * world,
+        "parallelism": f"replicas{world}",
+        "l2": "inputs larger than L2 (params 44 MB + pixel positions 50 MB + per-step instance lists)",
+    }
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_inputs(a, device, rank):
+    import torch
+
+    from us3d_b200 import scenes
+    from us3d_b200 import ultragauss as UG
+
+    sc = scenes.make_scene(a.gaussians, seed=0)
+    n_pool = max(2 * a.frames_per_step, 32)
+    sweep = scenes.linear_sweep(n_pool, a.size, a.size, a.spacing, seed=rank, step_mm=64.0 / n_pool)
+    specs = [UG.SliceSpec(f.height, f.width, f.lateral_spacing, f.axial_spacing, f.axial_near, f.lateral_col_offset,
+                          f.origin, f.axis_lat, f.axis_ax, f.axis_ele) for f in sweep]
+    pixels = torch.cat([f.pixels for f in sweep]).to(device)
+    g = torch.Generator().manual_seed(1234 + rank)
+    targets = torch.rand((n_pool * a.size * a.size,), generator=g).to(device)
+    params = [sc.means.to(device), sc.precision_tril.to(device).contiguous(), sc.opacities.to(device),
+              sc.intensities.to(device)]
+    return sc, specs, pixels, targets, params, n_pool
+
+
+def run_b200(a):
+    import torch
+    import torch.distributed as dist
+
+    from us3d_b200 import _lib
+    from us3d_b200 import ultragauss as UG
+    from us3d_b200.batch import UltraGaussBatchRenderer
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = _lib.load()
+    sc, specs, pixels, targets, params, n_pool = build_inputs(a, dev, rank)
+    F = a.frames_per_step
+    P1 = a.size * a.size
+    batches = []
+    for s in range(0, n_pool, F):
+        ft = UG.build_frame_table(specs[s:s + F], dev)
+        batches.append((ft, pixels[s * P1:(s + F) * P1], targets[s * P1:(s + F) * P1]))
+    single_tables = [UG.build_frame_table([sp], dev) for sp in specs]
+    grad_bufs = [torch.empty_like(p) for p in params]
+    scratch = [None]
+    inst_per_frame = []
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def l1_grad(img, tgt):
+        return torch.sign(img - tgt) / img.numel()
+
+    def batched_step(i):
+        ft, pix, tgt = batches[i % len(batches)]
+        b = UG.bin_gaussians(*params, ft, 7.815, 1e-4, True)
+        img, alpha, depth, _ = UG.forward(b, pix, 1e-6, 0.0, want_counts=False)
+        dI = l1_grad(img, tgt)
+        z = torch.zeros_like(img)
+        UG.backward(b, pix, dI, z, z, alpha, 1e-6, 0.0, out=grad_bufs)
+        return b
+
+    def plain_step(i):
+        acc = None
+        for f in range(F):
+            k = (i * F + f) % n_pool
+            pix = pixels[k * P1:(k + 1) * P1]
+            tgt = targets[k * P1:(k + 1) * P1]
+            b = UG.bin_gaussians(*params, single_tables[k], 7.815, 1e-4, True)
+            img, alpha, depth, counts = UG.forward(b, pix, 1e-6, 0.0)
+            dI = l1_grad(img, tgt)
+            z = torch.zeros_like(img)
+            g = UG.backward(b, pix, dI, z, z, alpha, 1e-6, 0.0)
+            if acc is None:
+                acc = [x.clone() for x in g]
+            else:
+                for x, y in zip(acc, g):
+                    x.add_(y)
+        return acc
+
+    def timed(fn, steps, warm):
+        for i in range(warm):
+            fn(i)
+        barrier()
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st.record()
+        for i in range(steps):
+            fn(warm + i)
+        en.record()
+        barrier()
+        ms = st.elapsed_time(en)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # -- warm-up + stage selection for the roofline (untimed) --
+    stage_ms = {}
+    for stage in ("ug_bin", "ug_forward", "ug_backward"):
+        _lib.check(L.us3d_profile_stage(stage.encode(), 8), "profile")
+        b = batched_step(0)
+        n = __import__("ctypes").c_int32(0)
+        tot = __import__("ctypes").c_double(0)
+        _lib.check(L.us3d_profile_collect(__import__("ctypes").byref(n), __import__("ctypes").byref(tot)), "collect")
+        stage_ms[stage] = tot.value / max(n.value, 1)
+        inst_per_frame.append(b.total / F)
+    dominant = max(stage_ms, key=stage_ms.get)
+    _lib.check(L.us3d_profile_stage(dominant.encode(), a.steps + 4), "profile")
+
+    launches0 = L.us3d_launch_count()
+    with Clocks(local) as clk:
+        ms_batched = timed(batched_step, a.steps, a.warmup)
+    launches = L.us3d_launch_count() - launches0
+    import ctypes
+
+    n = ctypes.c_int32(0)
+    tot = ctypes.c_double(0)
+    _lib.check(L.us3d_profile_collect(ctypes.byref(n), ctypes.byref(tot)), "collect")
+    _lib.check(L.us3d_profile_stage(None, 0), "profile off")
+    # launches counted include the warm-up steps; keep only the timed ones
+    per_step_launches = launches / (a.steps + a.warmup)
+    gpu_launches = int(round(per_step_launches * a.steps))
+    stage_avg_ms = tot.value / max(n.value, 1)
+    clocks = clk.summary()
+
+    frames_total = a.steps * F * world
+    value = frames_total / (ms_batched / 1e3)
+    I = statistics.mean(inst_per_frame)
+    G = a.gaussians
+    P = P1
+    alg = {
+        "ug_backward": G * (BP + BG) + I * 4 + P * (BO + BD),
+        "ug_forward": I * 4 + P * BO,
+        "ug_bin": G * BP + I * 12,
+    }[dominant] * F
+    peaks = json.load(open(ROOT / "MEASURED_PEAKS.json")) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg / (stage_avg_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
+                "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+                "algorithmic_bytes_per_launch": int(alg)}
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": round(ms_batched / a.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded headline scene (no dataset offline); targets U(0,1)",
+        "config": workload_config(a, world), "instances_per_frame": round(I, 1), "roofline": roofline,
+        "clocks": clocks, "gpu_launches": gpu_launches,
+    }
+
+    if not a.no_plain:
+        steps_p = max(2, a.steps // 2)
+        ms_plain = timed(plain_step, steps_p, 1)
+        plain_value = steps_p * F * world / (ms_plain / 1e3)
+        out["plain"] = {"value": round(plain_value, 3), "unit": UNIT, "ms_per_frame": round(ms_plain / (steps_p * F), 4)}
+        out["batched_over_plain"] = round(value / plain_value, 3)
+
+    if not a.no_e2e:
+        out["e2e"] = run_e2e(a, dev, sc, specs, n_pool, world, rank, timed)
+
+    if rank == 0 and world == 1 and not a.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(a, sc, specs)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed):
+    import torch
+
+    from us3d_b200.batch import UltraGaussBatchRenderer
+    from us3d_b200 import scenes
+
+    F = a.frames_per_step
+    P1 = a.size * a.size
+    host = [sc.means.pin_memory(), sc.precision_tril.contiguous().pin_memory(), sc.opacities.pin_memory(),
+            sc.intensities.pin_memory()]
+    sweep_pix = torch.cat([scenes.slice_pixels(s.origin, s.axis_lat, s.axis_ax, s.height, s.width, s.lateral_spacing,
+                                               s.axial_spacing, s.axial_near, s.lateral_col_offset)
+                           for s in specs]).pin_memory()
+    g = torch.Generator().manual_seed(99 + rank)
+    tgt_host = torch.rand((n_pool * P1,), generator=g).pin_memory()
+    renderers = [UltraGaussBatchRenderer(specs[s:s + F], dev) for s in range(0, n_pool, F)]
+    grad_host = [torch.empty_like(x).pin_memory() for x in host]
+    loss_host = torch.empty((), dtype=torch.float32).pin_memory()
+
+    def step(i):
+        k = i % len(renderers)
+        s = k * F
+        ps = [x.to(dev, non_blocking=True).requires_grad_(True) for x in host]
+        pix = sweep_pix[s * P1:(s + F) * P1].to(dev, non_blocking=True)
+        tgt = tgt_host[s * P1:(s + F) * P1].to(dev, non_blocking=True)
+        img, alpha, depth = renderers[k](*ps, pix)
+        loss = (img - tgt).abs().mean()
+        loss.backward()
+        loss_host.copy_(loss.detach(), non_blocking=True)
+        for gh, p in zip(grad_host, ps):
+            gh.copy_(p.grad, non_blocking=True)
+
+    ms = timed(step, a.steps, a.warmup)
+    h2d = sum(x.numel() * x.element_size() for x in host) + F * P1 * 3 * 4 + F * P1 * 4
+    d2h = 4 + sum(x.numel() * x.element_size() for x in host)
+    return {"value": round(a.steps * F * world / (ms / 1e3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "api": "us3d_b200.batch.UltraGaussBatchRenderer (autograd)"}
+
+
+def cpu_baseline(a, sc, specs, frames: int = 1):
+    """The C oracle (restatement of the reference algorithm) on the host cores, on a bounded
+    sample: `frames` full frames of the same workload (mapper + forward + backward)."""
+    import numpy as np
+
+    from oracle import ultragauss_oracle as O
+
+    nt = os.cpu_count() or 1
+    O.set_threads(nt)
+    means, tril = sc.means.numpy(), sc.precision_tril.numpy()
+    op, it = sc.opacities.numpy(), sc.intensities.numpy()
+    t0 = time.perf_counter()
+    for f in range(frames):
+        s = specs[f]
+        from us3d_b200 import scenes
+
+        pix = scenes.slice_pixels(s.origin, s.axis_lat, s.axis_ax, s.height, s.width, s.lateral_spacing,
+                                  s.axial_spacing, s.axial_near, s.lateral_col_offset).numpy()
+        geo = O.geometry(s.origin, s.axis_lat, s.axis_ax, s.axis_ele, s.lateral_spacing, s.axial_spacing,
+                         s.axial_near, s.lateral_col_offset)
+        st = O.render(means, tril, op, it, pix, geo, s.height, s.width, 7.815, 1e-4, True, 1e-6, 0.0,
+                      want_ambiguous=False)
+        rng = np.random.default_rng(f)
+        dI = np.sign(st["image"] - rng.random(st["image"].shape[0]).astype(np.float32)) / st["image"].shape[0]
+        z = np.zeros_like(dI)
+        O.backward(st, dI, z, z)
+    dt = time.perf_counter() - t0
+    return {"value": round(frames / dt, 5), "unit": UNIT, "cores": nt, "kind": "port",
+            "sample": f"{frames} full frame(s) of the workload ({a.gaussians} Gaussians, {a.size}^2 px): "
+                      f"C oracle mapper + per-pixel candidate lists + forward + backward, {dt:.1f} s"}
+
+
+def run_reference(a):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import torch  # noqa: F401
+
+    from us3d_b200 import scenes
+    from us3d_b200 import ultragauss as UG
+
+    sc = scenes.make_scene(a.gaussians, seed=0)
+    sweep = scenes.linear_sweep(max(a.steps + a.warmup, 1), a.size, a.size, a.spacing, seed=0)
+    specs = [UG.SliceSpec(f.height, f.width, f.lateral_spacing, f.axial_spacing, f.axial_near, f.lateral_col_offset,
+                          f.origin, f.axis_lat, f.axis_ax, f.axis_ele) for f in sweep]
+    for _ in range(a.warmup):
+        pass  # the oracle has no warm-up state; one untimed frame is enough to page code in
+    if a.warmup:
+        cpu_baseline(a, sc, specs[:1], frames=1)
+    times = []
+    for i in range(a.steps):
+        r = cpu_baseline(a, sc, [specs[i % len(specs)]], frames=1)
+        times.append(1.0 / r["value"])
+    value = a.steps / sum(times)
+    cb = {"value": round(value, 5), "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+          "sample": f"{a.steps} step(s) of 1 full frame each ({a.gaussians} Gaussians, {a.size}^2 px): C restatement "
+                    "of the reference UltraGauss mapper + forward + backward on all host threads"}
+    out = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": round(1e3 * sum(times) / a.steps, 2), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded headline scene",
+           "config": workload_config(a, 1), "impl": "reference", "cpu_baseline": cb,
+           "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

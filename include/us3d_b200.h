@@ -1,0 +1,188 @@
+/*
+ * us3d_b200 — C ABI of the B200-native Gaussian rasterisation library for freehand 3D
+ * ultrasound (sm_100a). Plain pointers and sizes only: every pointer argument named
+ * `*_dev` or documented as "device" is CUDA device memory owned by the caller; `stream`
+ * is a cudaStream_t passed as void*. No entry point allocates device memory or
+ * synchronises `stream` unless its comment says so.
+ *
+ * Status codes: every function returns US3D_OK (0) or an error code; the message of the
+ * last error on the calling thread is available from us3d_last_error().
+ *
+ * Reference interfaces replaced (paths inside the reference project
+ * KevinWCCC/ultrasound-3d-reconstruction):
+ *   UltraGauss:  ops/ultragauss_renderer/src/bindings.cpp:6-10
+ *                (MapperForwardCUDA  -> src/mapper/wrapper_mapper.cu:35-206,
+ *                 ShaderForwardCUDA  -> src/shader/wrapper_shader.cu:17-66,
+ *                 ShaderBackwardCUDA -> src/shader/wrapper_shader.cu:68-122)
+ */
+#ifndef US3D_B200_H
+#define US3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define US3D_API __attribute__((visibility("default")))
+#else
+#define US3D_API
+#endif
+
+#define US3D_OK 0
+#define US3D_INVALID_ARG 1
+#define US3D_CAPACITY_OVERFLOW 2
+#define US3D_CUDA_ERROR 3
+#define US3D_TIMEOUT 4
+
+/* Message of the last failed call on this thread ("" if none). */
+US3D_API const char* us3d_last_error(void);
+/* Library ABI version (major*10000 + minor*100 + patch). */
+US3D_API int us3d_version(void);
+/* Makes `device` current for this library's calls on the calling thread (cudaSetDevice). */
+US3D_API int us3d_set_device(int device);
+
+/* Benchmark instrumentation. us3d_launch_count: number of kernels this library has
+ * launched in this process. us3d_profile_stage: from now on, bracket up to max_launches
+ * executions of the named stage ("ug_bin", "ug_forward", "ug_backward") with CUDA events
+ * on the launching stream (NULL or 0 disables); us3d_profile_collect waits for them and
+ * returns how many ran and their summed duration, then resets the count. */
+US3D_API long long us3d_launch_count(void);
+US3D_API int us3d_profile_stage(const char* stage, int max_launches);
+US3D_API int us3d_profile_collect(int* n_launches, double* total_ms);
+
+/*
+ * One planar probe slice ("frame"). The library reads an array of these from DEVICE
+ * memory, so one launch can render many frames of different sizes. Pixel (row y, col x)
+ * of frame f is pixel index `pixel_offset + y*width + x` of the concatenated pixel arrays;
+ * its 16x16 tile (tx, ty) is tile `tile_offset + ty*tiles_x + tx` of the concatenated tile
+ * numbering. tiles_x = ceil(width/16), tiles_y = ceil(height/16).
+ * Axes and spacings have the meaning of the reference's UltraGaussRenderConfig /
+ * SliceGeometry (ops/ultragauss_renderer/ultragauss_renderer/types.py:6-40).
+ */
+typedef struct us3d_slice_frame {
+    float origin[3];
+    float axis_lat[3];
+    float axis_ax[3];
+    float axis_ele[3];
+    float lateral_spacing;    /* mm per pixel (lateral)          */
+    float axial_spacing;      /* mm per pixel (axial / depth)    */
+    float axial_near;         /* depth of pixel row 0, mm        */
+    float lateral_col_offset; /* column of lateral coordinate 0  */
+    int32_t height;
+    int32_t width;
+    int32_t tiles_x;
+    int32_t tiles_y;
+    int32_t pixel_offset;
+    int32_t tile_offset;
+    int32_t reserved0;
+    int32_t reserved1;
+} us3d_slice_frame; /* 96 bytes */
+
+/* ------------------------------------------------------------------------------------
+ * UltraGauss probe-plane slice splatting.
+ *
+ * Gaussian parameters (device, fp32, contiguous): means (G,3) world mm; precision_tril
+ * (G,6) raw lower-Cholesky factor of the precision in the order l11,l12,l13,l22,l23,l33
+ * with diagonal entries raw^2 + diag_beta; opacities (G); intensities (G).
+ * Pixels (device, fp32): pixel_positions (n_pixels,3) world mm, frames concatenated.
+ *
+ * Workspace: one caller-allocated device buffer of us3d_ug_workspace_bytes() bytes,
+ * which holds the binning of the last us3d_ug_bin() call; keep it alive (unchanged)
+ * between us3d_ug_bin, us3d_ug_forward and us3d_ug_backward of the same frames, and pass
+ * every call the same sizes and instance_capacity (they locate the arrays inside it).
+ * ---------------------------------------------------------------------------------- */
+
+/* Bytes of workspace for G Gaussians, n_frames frames with n_tiles tiles and n_pixels
+ * pixels in total, and room for `instance_capacity` (tile, Gaussian) instances. */
+US3D_API size_t us3d_ug_workspace_bytes(int64_t n_gauss, int32_t n_frames, int64_t n_tiles,
+                               int64_t n_pixels, int64_t instance_capacity);
+
+/* Bytes of the backward scratch buffer (per-instance partial gradients). */
+US3D_API size_t us3d_ug_backward_scratch_bytes(int64_t instance_capacity);
+
+/*
+ * Mapper: per-Gaussian probe-frame projection, chi-square window radii, elevational cull,
+ * 16x16 tile rectangles, (tile, depth) keys, per-tile stable ordering and tile ranges.
+ * Replaces MapperForwardCUDA (ops/ultragauss_renderer/src/mapper/wrapper_mapper.cu:35-206)
+ * up to the tile ranges; the per-pixel candidate lists are produced by us3d_ug_forward
+ * (counts) and us3d_ug_pixel_csr (indices). Never synchronises: the instance total and
+ * an overflow flag stay on the device (read them with us3d_ug_read_status).
+ */
+US3D_API int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames_dev,
+                int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
+                const float* means, const float* precision_tril, const float* opacities,
+                const float* intensities, float chi2_threshold, float diag_beta,
+                int32_t sort_by_depth, int64_t instance_capacity, void* stream);
+
+/* Copies the instance total and overflow flag of the last us3d_ug_bin to the host.
+ * SYNCHRONISES `stream`. */
+US3D_API int us3d_ug_read_status(const void* workspace, int64_t* total_instances, int32_t* overflow,
+                        void* stream);
+
+/*
+ * Forward shading: per pixel, the candidates that pass the reference's lateral/axial
+ * window test, then q <= chi2, alpha_hat = o*exp(-q/2) (skipped if <= 1e-8);
+ * image = clamp01((sum a*c + bg_a*bg_i) / max(sum a + bg_a, 1e-8)), alpha = sum a + bg_a,
+ * depth = sum a*((mean-origin).ele) / max(sum a, 1e-8). Also writes the per-pixel
+ * candidate count (the reference's pixel_gauss_counts) and the no-skip sums that the
+ * backward needs. Replaces ShaderForwardCUDA (src/shader/wrapper_shader.cu:17-66,
+ * kernel src/shader/forward.cu:17-76). out_counts may be NULL.
+ */
+US3D_API int us3d_ug_forward(void* workspace, const us3d_slice_frame* frames_dev, int32_t n_frames,
+                    int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
+                    int64_t instance_capacity, const float* pixel_positions, float chi2_threshold, float diag_beta,
+                    float bg_alpha, float bg_intensity, float* out_image, float* out_alpha,
+                    float* out_depth, int32_t* out_counts, void* stream);
+
+/*
+ * Backward (adjoint): gradients of (image, alpha, depth) w.r.t. means (G,3),
+ * precision_tril (G,6), opacities (G) and intensities (G), summed over all frames of the
+ * last bin. Deterministic: per (tile, Gaussian) partials are reduced per Gaussian in a
+ * fixed order (no float atomics). Overwrites the four gradient arrays. Replaces
+ * ShaderBackwardCUDA (src/shader/wrapper_shader.cu:68-122, kernel
+ * src/shader/backward.cu:17-131).
+ */
+US3D_API int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames_dev, int32_t n_frames,
+                     int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
+                     int64_t instance_capacity, const float* pixel_positions, const float* d_image,
+                     const float* d_alpha, const float* d_depth, const float* saved_alpha,
+                     float chi2_threshold, float diag_beta, float bg_alpha,
+                     float bg_intensity, void* scratch, size_t scratch_bytes,
+                     float* d_means, float* d_precision_tril, float* d_opacities,
+                     float* d_intensities, void* stream);
+
+/*
+ * Per-pixel candidate lists in the reference's CSR layout (pixel_gauss_indices of
+ * MapperForwardCUDA, src/mapper/core.cu:237-287): for each pixel, in tile-list order,
+ * the Gaussians passing the window test. `offsets` is the exclusive scan of the counts
+ * written by us3d_ug_forward (n_pixels entries); `out_indices` must hold the total.
+ */
+US3D_API int us3d_ug_pixel_csr(void* workspace, const us3d_slice_frame* frames_dev, int32_t n_frames,
+                      int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
+                      int64_t instance_capacity, const float* pixel_positions, float chi2_threshold, float diag_beta,
+                      const int32_t* offsets, int32_t* out_indices, void* stream);
+
+/*
+ * Sorted keys, values and tile ranges of one frame in the reference's format
+ * (key = (tile << 32) | depth_key, value = Gaussian index; empty tiles have start = end
+ * = -1; src/mapper/core.cu:118-164). out_keys/out_values hold the frame's instances
+ * (in tile order); out_range_start/out_range_end hold tiles_x*tiles_y entries.
+ */
+US3D_API int us3d_ug_export_bins(const void* workspace, int64_t n_tiles, int32_t frame_tile_offset,
+                        int32_t frame_n_tiles, int64_t* out_keys, int32_t* out_values,
+                        int32_t* out_range_start, int32_t* out_range_end, void* stream);
+
+/* Instance offset of a frame's first tile and its instance count (device -> host copy;
+ * SYNCHRONISES `stream`). */
+US3D_API int us3d_ug_frame_instances(const void* workspace, int64_t n_tiles, int32_t frame_tile_offset,
+                            int32_t frame_n_tiles, int64_t* first, int64_t* count,
+                            void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* US3D_B200_H */

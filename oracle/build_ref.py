@@ -1,0 +1,106 @@
+"""TEST INFRASTRUCTURE: compiles the reference's own UltraGauss CUDA extension, unmodified,
+from the reference tree for sm_100a, into ``oracle/_ref/`` (git-ignored; it travels to the
+GPU machine with the repository snapshot and is used only by tests as the parity checker).
+
+Recipe: nvcc on the reference's .cu files and g++ on its bindings.cpp, with the reference's
+own nvcc flags (ops/ultragauss_renderer/setup.py:29-41: -O3 --use_fast_math -lineinfo
+-DTHRUST_IGNORE_CUB_VERSION_CHECK), plus ``oracle/ref_shim`` for the helper header that the
+reference tree does not contain. The reference's setup.py is not run.
+
+Usage: python oracle/build_ref.py [--reference /path/to/reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sysconfig
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT_DIR = HERE / "_ref"
+SHIM = HERE / "ref_shim"
+DEFAULT_REFERENCE = Path("/root/reference")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+# module name -> (renderer directory, sources relative to it, extra nvcc flags)
+MODULES = {
+    "ultragauss_ref_C": (
+        "ops/ultragauss_renderer",
+        ["src/mapper/wrapper_mapper.cu", "src/mapper/core.cu", "src/shader/wrapper_shader.cu",
+         "src/shader/forward.cu", "src/shader/backward.cu", "src/bindings.cpp"],
+        ["-O3", "--use_fast_math", "-lineinfo", "-DTHRUST_IGNORE_CUB_VERSION_CHECK"],
+    ),
+    # The reference's mapper kernels plus oracle/ref_harness/ultragauss_keys.cu, which runs
+    # them the way MapperForwardCUDA does and returns its private sorted keys and ranges.
+    "ultragauss_ref_keys": (
+        "ops/ultragauss_renderer",
+        ["src/mapper/core.cu", "HARNESS:ultragauss_keys.cu"],
+        ["-O3", "--use_fast_math", "-lineinfo", "-DTHRUST_IGNORE_CUB_VERSION_CHECK"],
+    ),
+}
+
+
+def _torch_flags():
+    import torch
+    from torch.utils import cpp_extension as ce
+
+    inc = ce.include_paths(device_type="cuda") + [sysconfig.get_paths()["include"]]
+    libdirs = ce.library_paths(device_type="cuda")
+    abi = int(torch._C._GLIBCXX_USE_CXX11_ABI)
+    return inc, libdirs, abi
+
+
+def build_module(name: str, reference: Path, force: bool = False) -> Path:
+    rdir, srcs, nvflags = MODULES[name]
+    root = reference / rdir
+    suffix = sysconfig.get_config_var("EXT_SUFFIX")
+    out = OUT_DIR / f"{name}{suffix}"
+    if out.exists() and not force:
+        return out
+    OUT_DIR.mkdir(parents=True, exist_ok=True)
+    obj_dir = OUT_DIR / f"obj_{name}"
+    obj_dir.mkdir(parents=True, exist_ok=True)
+    inc, libdirs, abi = _torch_flags()
+    defs = [f"-DTORCH_EXTENSION_NAME={name}", "-DTORCH_API_INCLUDE_EXTENSION_H", f"-D_GLIBCXX_USE_CXX11_ABI={abi}"]
+    incs = ["-I", str(root / "include"), "-I", str(SHIM)] + [x for p in inc for x in ("-I", p)]
+    objs = []
+    for s in srcs:
+        src = (HERE / "ref_harness" / s.split(":", 1)[1]) if s.startswith("HARNESS:") else root / s
+        obj = obj_dir / (s.replace("/", "_").replace(":", "_") + ".o")
+        if s.endswith(".cu") and not s.startswith("HARNESS:"):
+            cmd = ["nvcc", "-c", str(src), "-o", str(obj), *ARCH, *nvflags, "-std=c++17", "-Xcompiler", "-fPIC",
+                   "--expt-relaxed-constexpr", *defs, *incs]
+        elif s.endswith(".cu"):
+            cmd = ["nvcc", "-c", str(src), "-o", str(obj), *ARCH, *nvflags, "-std=c++17", "-Xcompiler", "-fPIC",
+                   "--expt-relaxed-constexpr", *defs, *incs]
+        else:
+            cmd = ["g++", "-c", str(src), "-o", str(obj), "-O3", "-std=c++17", "-fPIC", *defs, *incs]
+        subprocess.run(cmd, check=True)
+        objs.append(str(obj))
+    link = ["g++", "-shared", "-o", str(out), *objs]
+    for d in libdirs:
+        link += ["-L", d, f"-Wl,-rpath,{d}"]
+    link += ["-lc10", "-lc10_cuda", "-ltorch", "-ltorch_cpu", "-ltorch_cuda", "-ltorch_python", "-lcudart"]
+    subprocess.run(link, check=True)
+    for o in objs:
+        os.remove(o)
+    obj_dir.rmdir()
+    return out
+
+
+def build_all(reference: Path = DEFAULT_REFERENCE, force: bool = False) -> list[Path]:
+    if not reference.exists():
+        return []
+    return [build_module(n, reference, force) for n in MODULES]
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", type=Path, default=DEFAULT_REFERENCE)
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    for p in build_all(a.reference, a.force):
+        print(p)

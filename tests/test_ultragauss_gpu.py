@@ -1,0 +1,284 @@
+"""UltraGauss parity on the GPU, through the C ABI (ctypes) of libus3d_b200.so.
+
+Checks against (1) golden fixtures produced by the reference's own CUDA build,
+(2) the reference build run live (oracle/_ref, when present), (3) the C oracle, and
+(4) FP64 central finite differences. Tolerances (from the workload specification):
+sort keys, tile ranges and per-pixel candidate counts/lists bit-exact; images <= 1e-5
+relative L2; gradients <= 1e-4 relative L2 against the reference backward.
+"""
+
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from ug_helpers import golden_names, load_golden, rel_l2, run_b200
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parents[1]
+IMG_TOL = 1e-5
+GRAD_TOL = 1e-4
+
+
+def _assert_case(out, fx, prefix="ref_"):
+    np.testing.assert_array_equal(out["keys"], fx[prefix + "keys"].astype(np.int64), err_msg="sorted keys")
+    np.testing.assert_array_equal(out["values"], fx[prefix + "values"], err_msg="sorted values")
+    np.testing.assert_array_equal(out["range_start"], fx[prefix + "range_start"], err_msg="range start")
+    np.testing.assert_array_equal(out["range_end"], fx[prefix + "range_end"], err_msg="range end")
+    np.testing.assert_array_equal(out["counts"], fx[prefix + "counts"], err_msg="pixel candidate counts")
+    np.testing.assert_array_equal(out["offsets"], fx[prefix + "offsets"], err_msg="pixel offsets")
+    np.testing.assert_array_equal(out["indices"], fx[prefix + "indices"], err_msg="pixel candidate indices")
+    for k in ("image", "alpha", "depth"):
+        assert rel_l2(out[k], fx[prefix + k]) <= IMG_TOL, (k, rel_l2(out[k], fx[prefix + k]))
+    for k in ("d_means", "d_tril", "d_opacity", "d_intensity"):
+        assert rel_l2(out[k], fx[prefix + k]) <= GRAD_TOL, (k, rel_l2(out[k], fx[prefix + k]))
+
+
+@pytest.mark.parametrize("name", golden_names() or ["c1"])
+def test_golden_reference_parity(name, cuda_device):
+    fx = load_golden(name)
+    out = run_b200(fx, cuda_device)
+    _assert_case(out, fx)
+
+
+def _reference_modules():
+    p = ROOT / "oracle" / "_ref"
+    if not any(p.glob("ultragauss_ref_C*.so")):
+        pytest.skip("reference build oracle/_ref not present")
+    sys.path.insert(0, str(p))
+    import ultragauss_ref_C
+    import ultragauss_ref_keys
+
+    return ultragauss_ref_C, ultragauss_ref_keys
+
+
+def _reference_run(REF, REFK, fx, device):
+    dev = device
+    t = lambda k: torch.as_tensor(fx[k]).to(dev).contiguous()  # noqa: E731
+    pad = lambda x: torch.nn.functional.pad(x, (0, 1)).contiguous()  # noqa: E731
+    geo = torch.as_tensor(fx["geo"]).to(dev)
+    o, l, a, e = geo[0:3].contiguous(), geo[3:6].contiguous(), geo[6:9].contiguous(), geo[9:12].contiguous()
+    H, W = int(fx["H"]), int(fx["W"])
+    dlat, dax, near, coloff = (float(x) for x in fx["geo"][12:16])
+    chi2, beta, sort = float(fx["chi2"]), float(fx["beta"]), bool(fx["sort_by_depth"])
+    mp, pp, tril = pad(t("means")), pad(t("pixels")), t("precision_tril")
+    counts, offsets, indices = REF.MapperForwardCUDA(pp, mp, tril, o, l, a, e, H, W, dlat, dax, near, coloff, chi2,
+                                                     sort, beta)
+    attr = torch.stack([t("opacities"), t("intensities")], 1).contiguous()
+    image, alpha, depth, sic = REF.ShaderForwardCUDA(attr, mp, tril, pp, o, e, offsets, counts, indices,
+                                                     float(fx["bg_alpha"]), float(fx["bg_intensity"]), chi2, beta)
+    dm, dt, da = REF.ShaderBackwardCUDA(t("d_image"), t("d_alpha"), t("d_depth"), attr, mp, tril, pp, o, e, offsets,
+                                        counts, indices, sic, alpha, float(fx["bg_alpha"]), float(fx["bg_intensity"]),
+                                        chi2, beta)
+    _, _, _, keys, vals, rs, re = REFK.RefBinning(mp, tril, o, l, a, e, H, W, dlat, dax, near, coloff, chi2, sort, beta)
+    torch.cuda.synchronize()
+    c = lambda x: x.detach().cpu().numpy()  # noqa: E731
+    return dict(ref_keys=c(keys), ref_values=c(vals), ref_range_start=c(rs), ref_range_end=c(re), ref_counts=c(counts),
+                ref_offsets=c(offsets), ref_indices=c(indices), ref_image=c(image), ref_alpha=c(alpha),
+                ref_depth=c(depth), ref_d_means=c(dm)[:, :3], ref_d_tril=c(dt), ref_d_opacity=c(da)[:, 0],
+                ref_d_intensity=c(da)[:, 1])
+
+
+def _scene_case(G, H, W, spacing, seed, frame=0, n_frames=4, sort=True, bg_a=1e-6, bg_i=0.0, chi2=7.815, **kw):
+    from us3d_b200 import scenes
+
+    sc = scenes.make_scene(G, seed=seed, **kw)
+    fr = scenes.linear_sweep(n_frames, H, W, spacing, seed=seed, cube_mm=kw.get("cube_mm", 64.0))[frame]
+    g = torch.Generator().manual_seed(seed + 7)
+    P = H * W
+    geo = np.concatenate([fr.origin.numpy(), fr.axis_lat.numpy(), fr.axis_ax.numpy(), fr.axis_ele.numpy(),
+                          np.array([spacing, spacing, 0.0, fr.lateral_col_offset], np.float32)]).astype(np.float32)
+    return dict(means=sc.means.numpy(), precision_tril=sc.precision_tril.numpy(), opacities=sc.opacities.numpy(),
+                intensities=sc.intensities.numpy(), pixels=fr.pixels.numpy(), geo=geo, H=H, W=W,
+                chi2=np.float32(chi2), beta=np.float32(1e-4), sort_by_depth=int(sort), bg_alpha=np.float32(bg_a),
+                bg_intensity=np.float32(bg_i), d_image=torch.randn(P, generator=g).numpy(),
+                d_alpha=(0.3 * torch.randn(P, generator=g)).numpy(), d_depth=(0.05 * torch.randn(P, generator=g)).numpy())
+
+
+@pytest.mark.parametrize(
+    "G,H,W,spacing,seed,sort",
+    [(4096, 128, 128, 0.3, 0, True), (20000, 256, 256, 0.25, 1, True), (3000, 100, 60, 0.5, 2, False),
+     (60000, 192, 320, 0.2, 3, True)],
+)
+def test_live_reference_parity(G, H, W, spacing, seed, sort, cuda_device):
+    REF, REFK = _reference_modules()
+    fx = _scene_case(G, H, W, spacing, seed, frame=1, sort=sort)
+    fx.update(_reference_run(REF, REFK, fx, cuda_device))
+    out = run_b200(fx, cuda_device)
+    _assert_case(out, fx)
+
+
+def test_oracle_agreement(cuda_device):
+    """GPU vs the C oracle (IEEE CPU arithmetic): counts differ at most by the oracle's
+    near-threshold window tests; image and gradients within tolerance."""
+    from oracle import ultragauss_oracle as O
+
+    fx = _scene_case(8192, 128, 160, 0.3, 5, frame=2)
+    out = run_b200(fx, cuda_device)
+    st = O.render(fx["means"], fx["precision_tril"], fx["opacities"], fx["intensities"], fx["pixels"], fx["geo"],
+                  int(fx["H"]), int(fx["W"]), float(fx["chi2"]), float(fx["beta"]), True, float(fx["bg_alpha"]),
+                  float(fx["bg_intensity"]))
+    assert np.all(np.abs(out["counts"] - st["counts"]) <= st["ambiguous"])
+    assert rel_l2(out["image"], st["image"]) <= IMG_TOL
+    g = O.backward(st, fx["d_image"], fx["d_alpha"], fx["d_depth"])
+    for k in ("d_means", "d_tril", "d_opacity", "d_intensity"):
+        assert rel_l2(out[k], g[k]) <= GRAD_TOL, (k, rel_l2(out[k], g[k]))
+
+
+def test_fd_gradients_fp64(cuda_device):
+    """Central finite differences (step 1e-4) of the FP64 oracle forward vs the GPU
+    adjoint, on a small scene with a wide chi-square window so no pair crosses a cut."""
+    from oracle import ultragauss_oracle as O
+
+    fx = _scene_case(48, 32, 32, 0.6, 11, frame=1, n_frames=3, chi2=400.0, cube_mm=19.2, log_scale_mean=0.7,
+                     bg_a=1e-3)
+    fx["intensities"] = (0.1 + 0.8 * fx["intensities"]).astype(np.float32)
+    out = run_b200(fx, cuda_device)
+    wI, wA, wD = fx["d_image"].astype(np.float64), fx["d_alpha"].astype(np.float64), fx["d_depth"].astype(np.float64)
+
+    def loss(means, tril, op, it):
+        st = O.render(means, tril, op, it, fx["pixels"].astype(np.float64), fx["geo"].astype(np.float64),
+                      int(fx["H"]), int(fx["W"]), float(fx["chi2"]), float(fx["beta"]), True, float(fx["bg_alpha"]),
+                      float(fx["bg_intensity"]), precision="f64", want_indices=True, want_ambiguous=False)
+        return float(np.dot(wI, st["image"]) + np.dot(wA, st["alpha"]) + np.dot(wD, st["depth"]))
+
+    base = [fx[k].astype(np.float64).copy() for k in ("means", "precision_tril", "opacities", "intensities")]
+    rng = np.random.default_rng(0)
+    h = 1e-4
+    fd, an = [], []
+    for which, key in enumerate(("d_means", "d_tril", "d_opacity", "d_intensity")):
+        arr = base[which]
+        flat_idx = rng.choice(arr.size, size=min(24, arr.size), replace=False)
+        for fi in flat_idx:
+            plus = [b.copy() for b in base]
+            minus = [b.copy() for b in base]
+            plus[which].reshape(-1)[fi] += h
+            minus[which].reshape(-1)[fi] -= h
+            fd.append((loss(*plus) - loss(*minus)) / (2 * h))
+            an.append(out[key].reshape(-1)[fi])
+    err = rel_l2(an, fd)
+    print(f"FD gradient check (FP64 oracle, h=1e-4): rel-L2 {err:.3e} over {len(fd)} entries")
+    assert err <= 2e-3, err
+
+
+def test_batched_frames_match_single(cuda_device):
+    """Many frames of different sizes binned and shaded in one launch sequence give each
+    frame's single-frame result; gradients are the sum over frames."""
+    from us3d_b200 import scenes
+    from us3d_b200 import ultragauss as UG
+
+    dev = cuda_device
+    sc = scenes.make_scene(30000, seed=4).to(dev)
+    sizes = [(128, 128, 0.5), (96, 200, 0.32), (256, 256, 0.25), (50, 70, 0.9)]
+    specs, pix, grads = [], [], []
+    g = torch.Generator().manual_seed(3)
+    for i, (H, W, s) in enumerate(sizes):
+        fr = scenes.linear_sweep(len(sizes), H, W, s, seed=4)[i]
+        specs.append(UG.SliceSpec(H, W, s, s, 0.0, fr.lateral_col_offset, fr.origin, fr.axis_lat, fr.axis_ax,
+                                  fr.axis_ele))
+        pix.append(fr.pixels)
+        grads.append(torch.randn(3, H * W, generator=g))
+    args = (sc.means, sc.precision_tril.contiguous(), sc.opacities, sc.intensities)
+    ft = UG.build_frame_table(specs, dev)
+    allpix = torch.cat(pix).to(dev)
+    b = UG.bin_gaussians(*args, ft, 7.815, 1e-4, True)
+    img, alp, dep, cnt = UG.forward(b, allpix, 1e-6, 0.0)
+    gg = torch.cat(grads, dim=1).to(dev)
+    dsum = UG.backward(b, allpix, gg[0].contiguous(), gg[1].contiguous(), gg[2].contiguous(), alp, 1e-6, 0.0)
+    acc = [torch.zeros_like(x) for x in dsum]
+    off = 0
+    for i, sp in enumerate(specs):
+        n = sp.height * sp.width
+        f1 = UG.build_frame_table([sp], dev)
+        b1 = UG.bin_gaussians(*args, f1, 7.815, 1e-4, True)
+        i1, a1, d1, c1 = UG.forward(b1, pix[i].to(dev), 1e-6, 0.0)
+        assert torch.equal(i1, img[off:off + n]) and torch.equal(c1, cnt[off:off + n])
+        assert torch.equal(a1, alp[off:off + n]) and torch.equal(d1, dep[off:off + n])
+        gi = grads[i].to(dev)
+        d = UG.backward(b1, pix[i].to(dev), gi[0].contiguous(), gi[1].contiguous(), gi[2].contiguous(), a1, 1e-6, 0.0)
+        for a_, d_ in zip(acc, d):
+            a_ += d_
+        off += n
+    for a_, d_ in zip(acc, dsum):
+        assert rel_l2(d_.cpu().numpy(), a_.cpu().numpy()) <= 1e-5
+
+
+def test_backward_deterministic(cuda_device):
+    fx = _scene_case(20000, 128, 128, 0.4, 6)
+    a = run_b200(fx, cuda_device)
+    b = run_b200(fx, cuda_device)
+    for k in ("d_means", "d_tril", "d_opacity", "d_intensity", "image"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_capacity_retry_and_oversized_tile(cuda_device):
+    """A capacity far below the instance count is grown and re-binned; a tile holding more
+    instances than the in-shared-memory sort takes the global-memory path, same result."""
+    from oracle import ultragauss_oracle as O
+
+    from us3d_b200 import scenes
+
+    fx = _scene_case(12000, 16, 16, 0.05, 8, log_scale_mean=-1.0)
+    geo = np.array([0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0.05, 0.05, 0.0, 0.0], np.float32)
+    fx["geo"] = geo
+    fx["pixels"] = scenes.slice_pixels(torch.zeros(3), torch.tensor([1.0, 0, 0]), torch.tensor([0, 1.0, 0]), 16, 16,
+                                       0.05, 0.05, 0.0, 0.0).numpy()
+    rng = np.random.default_rng(0)
+    fx["means"] = (np.array([0.4, 0.4, 0.0]) + rng.normal(0, 0.05, (12000, 3))).astype(np.float32)
+    out = run_b200(fx, cuda_device, capacity=16)
+    st = O.render(fx["means"], fx["precision_tril"], fx["opacities"], fx["intensities"], fx["pixels"], fx["geo"],
+                  16, 16, float(fx["chi2"]), float(fx["beta"]), True, float(fx["bg_alpha"]), 0.0)
+    assert out["keys"].shape[0] > 8192
+    same = np.mean(out["keys"] == st["keys"].astype(np.int64))
+    assert same > 0.999, same
+    assert rel_l2(out["image"], st["image"]) <= IMG_TOL
+
+
+def test_empty_and_invalid_inputs(cuda_device):
+    from ultragauss_renderer import SliceGeometry, UltraGaussRenderConfig, UltraGaussRenderer
+
+    dev = cuda_device
+    cfg = UltraGaussRenderConfig(H=20, W=33, lateral_spacing_mm_per_pix=0.5, axial_spacing_mm_per_pix=0.5,
+                                 axial_near_mm=0.0, fixed_bg_alpha=0.2, fixed_bg_intensity=0.4)
+    geom = SliceGeometry(torch.zeros(3, device=dev), torch.tensor([1.0, 0, 0], device=dev),
+                         torch.tensor([0, 1.0, 0], device=dev), torch.tensor([0, 0, 1.0], device=dev))
+    pix = torch.rand(20 * 33, 3, device=dev)
+    z = torch.zeros((0, 3), device=dev)
+    img, alpha, depth, inter = UltraGaussRenderer(cfg)(z, torch.zeros((0, 6), device=dev), torch.zeros(0, device=dev),
+                                                       torch.zeros(0, device=dev), pix, geom, True)
+    assert torch.allclose(img, torch.full_like(img, 0.4)) and torch.allclose(alpha, torch.full_like(alpha, 0.2))
+    assert int(inter["pixel_gauss_counts"].sum()) == 0 and inter["pixel_gauss_indices"].numel() == 0
+    with pytest.raises(RuntimeError, match="n_pixels must equal H\\*W"):
+        UltraGaussRenderer(cfg)(z, torch.zeros((0, 6), device=dev), torch.zeros(0, device=dev),
+                                torch.zeros(0, device=dev), pix[:-1], geom)
+
+
+def test_dropin_autograd_matches_lowlevel(cuda_device):
+    from ultragauss_renderer import SliceGeometry, UltraGaussRenderConfig, UltraGaussRenderer
+
+    fx = _scene_case(5000, 96, 128, 0.4, 9, bg_a=1e-6)
+    low = run_b200(fx, cuda_device)
+    dev = cuda_device
+    geo = fx["geo"]
+    cfg = UltraGaussRenderConfig(H=96, W=128, lateral_spacing_mm_per_pix=0.4, axial_spacing_mm_per_pix=0.4,
+                                 axial_near_mm=0.0, lateral_col_offset=float(geo[15]), fixed_bg_alpha=1e-6)
+    T = lambda k: torch.as_tensor(fx[k]).to(dev).requires_grad_(True)  # noqa: E731
+    means, tril, op, it = T("means"), T("precision_tril"), T("opacities"), T("intensities")
+    g = lambda a, b: torch.as_tensor(geo[a:b]).to(dev)  # noqa: E731
+    img, alpha, depth, inter = UltraGaussRenderer(cfg)(means, tril, op, it, torch.as_tensor(fx["pixels"]).to(dev),
+                                                       SliceGeometry(g(0, 3), g(3, 6), g(6, 9), g(9, 12)), True)
+    assert not inter.is_materialized("pixel_gauss_indices")
+    loss = ((img.reshape(-1) * torch.as_tensor(fx["d_image"]).to(dev)).sum()
+            + (alpha.reshape(-1) * torch.as_tensor(fx["d_alpha"]).to(dev)).sum()
+            + (depth.reshape(-1) * torch.as_tensor(fx["d_depth"]).to(dev)).sum())
+    loss.backward()
+    assert np.array_equal(img.detach().cpu().numpy().reshape(-1), low["image"])
+    assert np.array_equal(inter["pixel_gauss_indices"].cpu().numpy(), low["indices"])
+    assert np.array_equal(inter["pixel_gauss_offsets"].cpu().numpy(), low["offsets"])
+    for p, k in ((means, "d_means"), (tril, "d_tril"), (op, "d_opacity"), (it, "d_intensity")):
+        assert rel_l2(p.grad.cpu().numpy(), low[k]) <= 1e-6, k

@@ -1,0 +1,925 @@
+// UltraGauss probe-plane slice splatting: binning, forward shading, backward adjoint.
+//
+// Reference behaviour restated here (paths inside KevinWCCC/ultrasound-3d-reconstruction):
+//   ops/ultragauss_renderer/src/mapper/core.cu:9-164    projection, window radii, cull,
+//                                                       tile rectangles, keys, ranges
+//   ops/ultragauss_renderer/src/mapper/core.cu:166-287  per-pixel window test (candidates)
+//   ops/ultragauss_renderer/src/shader/forward.cu:17-76 per-pixel normalised compositing
+//   ops/ultragauss_renderer/src/shader/backward.cu:17-131 adjoint
+//   ops/ultragauss_renderer/include/shader/shared.cuh:4-52 precision from the raw factor
+//
+// B200 design (not the reference's): one launch sequence bins any number of frames at
+// once; instances are bucketed straight into their tile (atomic cursor) and each tile's
+// bucket is put into the reference's (depth key, Gaussian index) order by an in-shared-
+// memory bitonic sort, so no global 64-bit radix sort and no host synchronisation is
+// needed. The forward stages each tile's Gaussians in shared memory (one pixel per
+// thread, reference summation order); the backward gives each thread one (tile, Gaussian)
+// instance, walks the tile's pixels from shared memory and accumulates that instance's
+// gradient in registers, so there are no float atomics and no warp reductions. Partials
+// are reduced per Gaussian in a fixed order (deterministic gradients).
+//
+// Arithmetic that decides integer outputs (window radii, culling, tile rectangles, depth
+// keys, the window test) is written with the same operations in the same order as the
+// reference so that, compiled with the same fast-math flags, keys, ranges and candidate
+// counts agree bit for bit.
+#include "us3d_common.cuh"
+#include "scan.cuh"
+
+namespace us3d {
+namespace ug {
+
+constexpr int TILE = 16;           // reference SLICE_TILE_SIZE (include/mapper/core.cuh:5)
+constexpr int TILE_PIX = TILE * TILE;
+constexpr int SORT_THREADS = 512;
+constexpr int SORT_SMEM_CAP = 8192;  // keys sorted in shared memory per tile (96 KB)
+constexpr int FWD_BATCH = 256;       // Gaussians staged per shared-memory batch
+
+// Header words at the start of the workspace.
+enum { H_TOTAL = 0, H_FLAGS = 1, H_SCAN_G = 2, H_SCAN_T = 3, H_CAP = 4, H_G = 5, H_T = 6, H_P = 7, H_WORDS = 8 };
+enum { FLAG_OVERFLOW = 1, FLAG_TABLE = 2 };
+
+struct Workspace {
+    long long* header;
+    float4* pack;            // G x 3 float4: (m.xyz, o) (t0..t3) (t4, t5, c, 0)
+    int* touched;            // G
+    int* inst_offset;        // G + 1
+    long long* bs_g;         // scan block sums over G
+    int* tile_count;         // T
+    int* tile_start;         // T + 1
+    int* tile_cursor;        // T
+    long long* bs_t;         // scan block sums over T
+    int* tile_frame;         // T
+    unsigned long long* keys;  // cap: (depth_key << 32) | g, sorted in place per tile
+    int* slot_inst;          // cap: instance index of each bucket slot (unsorted)
+    int* sorted_gid;         // cap
+    int* sorted_inst;        // cap
+    float2* pixel_aux;       // P: no-skip sums (sum a*c, sum a*depth) for the backward
+    size_t bytes;
+};
+
+static Workspace carve(void* base, int64_t G, int64_t T, int64_t P, int64_t cap) {
+    Carver c(base);
+    Workspace w;
+    w.header = c.take<long long>(H_WORDS);
+    w.pack = c.take<float4>((size_t)G * 3);
+    w.touched = c.take<int>((size_t)G);
+    w.inst_offset = c.take<int>((size_t)G + 1);
+    w.bs_g = c.take<long long>((size_t)scan_num_blocks(G) + 1);
+    w.tile_count = c.take<int>((size_t)T);
+    w.tile_start = c.take<int>((size_t)T + 1);
+    w.tile_cursor = c.take<int>((size_t)T);
+    w.bs_t = c.take<long long>((size_t)scan_num_blocks(T) + 1);
+    w.tile_frame = c.take<int>((size_t)T);
+    w.keys = c.take<unsigned long long>((size_t)cap);
+    w.slot_inst = c.take<int>((size_t)cap);
+    w.sorted_gid = c.take<int>((size_t)cap);
+    w.sorted_inst = c.take<int>((size_t)cap);
+    w.pixel_aux = c.take<float2>((size_t)P);
+    w.bytes = align_up(c.off, 256);
+    return w;
+}
+
+struct Geo {
+    float3 o, lat, ax, ele;
+    float dlat, dax, near, coloff;
+    int H, W, tx, ty, pix_off, tile_off;
+};
+
+__device__ __forceinline__ Geo load_geo(const us3d_slice_frame* __restrict__ fr) {
+    Geo g;
+    g.o = make_float3(fr->origin[0], fr->origin[1], fr->origin[2]);
+    g.lat = make_float3(fr->axis_lat[0], fr->axis_lat[1], fr->axis_lat[2]);
+    g.ax = make_float3(fr->axis_ax[0], fr->axis_ax[1], fr->axis_ax[2]);
+    g.ele = make_float3(fr->axis_ele[0], fr->axis_ele[1], fr->axis_ele[2]);
+    g.dlat = fr->lateral_spacing;
+    g.dax = fr->axial_spacing;
+    g.near = fr->axial_near;
+    g.coloff = fr->lateral_col_offset;
+    g.H = fr->height;
+    g.W = fr->width;
+    g.tx = fr->tiles_x;
+    g.ty = fr->tiles_y;
+    g.pix_off = fr->pixel_offset;
+    g.tile_off = fr->tile_offset;
+    return g;
+}
+
+// Lateral / axial / elevational half-widths of the chi-square ellipsoid: for the
+// precision Lambda = L L^T, the standard deviation along unit axis a is ||L^-1 a||,
+// obtained by forward substitution (reference: src/mapper/core.cu:9-44).
+__device__ __forceinline__ void window_radii(float t0, float t1, float t2, float t3, float t4,
+                                             float t5, float chi2, float beta, float3 a_lat,
+                                             float3 a_ax, float3 a_ele, float& r_lat,
+                                             float& r_ax, float& r_ele) {
+    const float d1 = t0 * t0 + beta;
+    const float d2 = t3 * t3 + beta;
+    const float d3 = t5 * t5 + beta;
+    const float inv1 = fmaxf(d1, 1e-10f), inv2 = fmaxf(d2, 1e-10f), inv3 = fmaxf(d3, 1e-10f);
+    const float la0 = a_lat.x / inv1;
+    const float la1 = (a_lat.y - t1 * la0) / inv2;
+    const float la2 = (a_lat.z - t2 * la0 - t4 * la1) / inv3;
+    const float v_lat = fmaxf(la0 * la0 + la1 * la1 + la2 * la2, 1e-12f);
+    const float xa0 = a_ax.x / inv1;
+    const float xa1 = (a_ax.y - t1 * xa0) / inv2;
+    const float xa2 = (a_ax.z - t2 * xa0 - t4 * xa1) / inv3;
+    const float v_ax = fmaxf(xa0 * xa0 + xa1 * xa1 + xa2 * xa2, 1e-12f);
+    const float ea0 = a_ele.x / inv1;
+    const float ea1 = (a_ele.y - t1 * ea0) / inv2;
+    const float ea2 = (a_ele.z - t2 * ea0 - t4 * ea1) / inv3;
+    const float v_ele = fmaxf(ea0 * ea0 + ea1 * ea1 + ea2 * ea2, 1e-12f);
+    const float k = sqrtf(chi2);
+    r_lat = fmaxf(1e-3f, k * sqrtf(v_lat));
+    r_ax = fmaxf(1e-3f, k * sqrtf(v_ax));
+    r_ele = fmaxf(1e-3f, k * sqrtf(v_ele));
+}
+
+// Probe-frame projection, elevational cull and 16x16 tile rectangle of one Gaussian in
+// one frame (reference: src/mapper/core.cu:46-116). Returns false when culled.
+__device__ __forceinline__ bool project_rect(const float4 a, const float4 b, const float4 c,
+                                             const Geo& F, float chi2, float beta, int4& rect,
+                                             float& v_pix) {
+    const float3 m = make_float3(a.x, a.y, a.z);
+    const float3 v = f3_sub(m, F.o);
+    const float lat = f3_dot(v, F.lat);
+    const float ele = f3_dot(v, F.ele);
+    const float ax = f3_dot(v, F.ax);
+    float r_lat, r_ax, r_ele;
+    window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, F.lat, F.ax, F.ele, r_lat, r_ax, r_ele);
+    if (fabsf(ele) > r_ele) return false;
+    const float u_pix = lat / F.dlat + F.coloff;
+    v_pix = (ax - F.near) / F.dax;
+    const float r_u = fmaxf(1.0f, r_lat / F.dlat);
+    const float r_v = fmaxf(1.0f, r_ax / F.dax);
+    int x0 = (int)floorf((u_pix - r_u) / TILE);
+    int y0 = (int)floorf((v_pix - r_v) / TILE);
+    int x1 = (int)ceilf((u_pix + r_u) / TILE);
+    int y1 = (int)ceilf((v_pix + r_v) / TILE);
+    x0 = max(0, x0);
+    y0 = max(0, y0);
+    x1 = min(min((F.W + TILE - 1) / TILE, F.tx), x1);
+    y1 = min(min((F.H + TILE - 1) / TILE, F.ty), y1);
+    if (x0 >= x1 || y0 >= y1) return false;
+    rect = make_int4(x0, y0, x1, y1);
+    return true;
+}
+
+// Depth key of the reference (src/mapper/core.cu:134): truncation of (v + 500) * 1000 to
+// uint32 with the saturating float->u32 conversion of the GPU.
+__device__ __forceinline__ uint32_t depth_key(float v_pix, int sort_by_depth) {
+    return sort_by_depth ? f32_to_u32_sat((v_pix + 500.0f) * 1000.0f) : 0u;
+}
+
+// ------------------------------------------------------------------------------------
+// Binning kernels
+// ------------------------------------------------------------------------------------
+
+__device__ __forceinline__ bool frame_ok(const us3d_slice_frame* __restrict__ frp, int64_t T, int64_t P) {
+    const us3d_slice_frame& fr = *frp;
+    return fr.height >= 0 && fr.width >= 0 && fr.tiles_x == (fr.width + TILE - 1) / TILE &&
+           fr.tiles_y == (fr.height + TILE - 1) / TILE && fr.tile_offset >= 0 && fr.pixel_offset >= 0 &&
+           (int64_t)fr.tile_offset + (int64_t)fr.tiles_x * fr.tiles_y <= T &&
+           (int64_t)fr.pixel_offset + (int64_t)fr.width * fr.height <= P;
+}
+
+// Clears the per-tile counters, marks every tile as belonging to no frame and records the
+// sizes the workspace was carved with.
+__global__ void init_tiles_kernel(int64_t T, int* __restrict__ tile_count, int* __restrict__ tile_cursor,
+                                  int* __restrict__ tile_frame, long long* __restrict__ header, int64_t cap,
+                                  int64_t G, int64_t P) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x < H_WORDS) {
+        long long v = 0;
+        if (threadIdx.x == H_CAP) v = cap;
+        if (threadIdx.x == H_G) v = G;
+        if (threadIdx.x == H_T) v = T;
+        if (threadIdx.x == H_P) v = P;
+        header[threadIdx.x] = v;
+    }
+    if (t >= T) return;
+    tile_count[t] = 0;
+    tile_cursor[t] = 0;
+    tile_frame[t] = -1;
+}
+
+// Assigns each frame's tiles to it and validates the frame table against the sizes.
+__global__ void setup_kernel(const us3d_slice_frame* __restrict__ frames, int F, int64_t T, int64_t P,
+                             int* __restrict__ tile_frame, long long* __restrict__ header) {
+    const int f = blockIdx.x;
+    if (f >= F) return;
+    const us3d_slice_frame fr = frames[f];
+    if (!frame_ok(frames + f, T, P)) {
+        if (threadIdx.x == 0) atomicOr(reinterpret_cast<unsigned long long*>(header + H_FLAGS), (unsigned long long)FLAG_TABLE);
+        return;
+    }
+    const int n = fr.tiles_x * fr.tiles_y;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tile_frame[fr.tile_offset + i] = f;
+}
+
+__global__ void pack_kernel(int64_t G, const float* __restrict__ means, const float* __restrict__ tril,
+                            const float* __restrict__ opac, const float* __restrict__ inten,
+                            float4* __restrict__ pack) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    const float* m = means + 3 * g;
+    const float2* t = reinterpret_cast<const float2*>(tril + 6 * g);  // 8-byte aligned rows
+    const float2 t01 = t[0], t23 = t[1], t45 = t[2];
+    pack[3 * g + 0] = make_float4(m[0], m[1], m[2], opac[g]);
+    pack[3 * g + 1] = make_float4(t01.x, t01.y, t23.x, t23.y);
+    pack[3 * g + 2] = make_float4(t45.x, t45.y, inten[g], 0.0f);
+}
+
+__global__ void __launch_bounds__(256)
+count_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, int F,
+             const float4* __restrict__ pack, float chi2, float beta, int* __restrict__ touched,
+             int* __restrict__ tile_count) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+    int total = 0;
+    for (int f = 0; f < F; ++f) {
+        if (!frame_ok(frames + f, T, P)) continue;
+        const Geo geo = load_geo(frames + f);
+        int4 r;
+        float v_pix;
+        if (!project_rect(a, b, c, geo, chi2, beta, r, v_pix)) continue;
+        total += (r.z - r.x) * (r.w - r.y);
+        for (int y = r.y; y < r.w; ++y)
+            for (int x = r.x; x < r.z; ++x) atomicAdd(&tile_count[geo.tile_off + y * geo.tx + x], 1);
+    }
+    touched[g] = total;
+}
+
+__global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
+    const long long tg = header[H_SCAN_G], tt = header[H_SCAN_T];
+    long long flags = header[H_FLAGS];
+    if (tg != tt) flags |= FLAG_TABLE;
+    if (tg > cap || tg > 0x7fffffffLL) flags |= FLAG_OVERFLOW;
+    header[H_TOTAL] = tg;
+    header[H_FLAGS] = flags;
+}
+
+__global__ void __launch_bounds__(256)
+scatter_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, int F,
+               const float4* __restrict__ pack, float chi2, float beta, int sort_by_depth,
+               const int* __restrict__ inst_offset, const int* __restrict__ tile_start,
+               int* __restrict__ tile_cursor, const long long* __restrict__ header,
+               unsigned long long* __restrict__ keys, int* __restrict__ slot_inst) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G || header[H_FLAGS] != 0) return;
+    const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+    int inst = inst_offset[g];
+    for (int f = 0; f < F; ++f) {
+        if (!frame_ok(frames + f, T, P)) continue;
+        const Geo geo = load_geo(frames + f);
+        int4 r;
+        float v_pix;
+        if (!project_rect(a, b, c, geo, chi2, beta, r, v_pix)) continue;
+        const unsigned long long key =
+            ((unsigned long long)depth_key(v_pix, sort_by_depth) << 32) | (unsigned long long)(uint32_t)g;
+        for (int y = r.y; y < r.w; ++y) {
+            for (int x = r.x; x < r.z; ++x) {
+                const int t = geo.tile_off + y * geo.tx + x;
+                const int slot = tile_start[t] + atomicAdd(&tile_cursor[t], 1);
+                keys[slot] = key;
+                slot_inst[slot] = inst++;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void cswap(unsigned long long* k, int* v, int a, int b) {
+    const unsigned long long ka = k[a], kb = k[b];
+    if (kb < ka) {
+        k[a] = kb;
+        k[b] = ka;
+        const int t = v[a];
+        v[a] = v[b];
+        v[b] = t;
+    }
+}
+
+// Ascending bitonic sort of n (not necessarily a power of two) keys with payload, in the
+// "mirror" formulation where every compare-exchange puts the smaller key at the lower
+// index; positions >= n act as +infinity and are never touched.
+__device__ void bitonic_sort(unsigned long long* k, int* v, int n) {
+    int npow = 1;
+    while (npow < n) npow <<= 1;
+    const int half_n = npow >> 1;
+    for (int size = 2; size <= npow; size <<= 1) {
+        const int hs = size >> 1;
+        for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
+            const int blk = i / hs, off = i - blk * hs;
+            const int a = blk * size + off, b = blk * size + size - 1 - off;
+            if (b < n) cswap(k, v, a, b);
+        }
+        __syncthreads();
+        for (int h = hs >> 1; h >= 1; h >>= 1) {
+            for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
+                const int blk = i / h, off = i - blk * h;
+                const int a = blk * 2 * h + off, b = a + h;
+                if (b < n) cswap(k, v, a, b);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// One block per tile: order the tile's bucket by (depth key, Gaussian index), which is the
+// order the reference's stable radix sort of (tile << 32 | depth key) over instances
+// enumerated Gaussian by Gaussian produces (src/mapper/wrapper_mapper.cu:134-146).
+__global__ void __launch_bounds__(SORT_THREADS)
+tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
+                 unsigned long long* __restrict__ keys, int* __restrict__ slot_inst,
+                 int* __restrict__ sorted_gid, int* __restrict__ sorted_inst) {
+    extern __shared__ unsigned long long s_keys[];
+    int* s_idx = reinterpret_cast<int*>(s_keys + SORT_SMEM_CAP);
+    const int64_t t = blockIdx.x;
+    if (t >= T || header[H_FLAGS] != 0) return;
+    const int s0 = tile_start[t];
+    const int n = tile_start[t + 1] - s0;
+    if (n <= 0) return;
+    if (n <= SORT_SMEM_CAP) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            s_keys[i] = keys[s0 + i];
+            s_idx[i] = i;
+        }
+        __syncthreads();
+        bitonic_sort(s_keys, s_idx, n);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned long long k = s_keys[i];
+            sorted_gid[s0 + i] = (int)(uint32_t)(k & 0xffffffffull);
+            sorted_inst[s0 + i] = slot_inst[s0 + s_idx[i]];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) keys[s0 + i] = s_keys[i];
+    } else {
+        // Oversized bucket: same network directly on global memory (one block owns it).
+        bitonic_sort(keys + s0, slot_inst + s0, n);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            sorted_gid[s0 + i] = (int)(uint32_t)(keys[s0 + i] & 0xffffffffull);
+            sorted_inst[s0 + i] = slot_inst[s0 + i];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Shading
+// ------------------------------------------------------------------------------------
+
+// Per-Gaussian data staged in shared memory for one frame.
+struct Staged {
+    float4 q0;  // mean.xyz, opacity
+    float4 q1;  // s00 s01 s02 s11 (precision)
+    float4 q2;  // s12 s22 intensity depth_term
+    float4 q3;  // r_lat r_ax
+};
+
+// Precision Lambda = L L^T from the raw factor (reference include/shader/shared.cuh:4-25).
+__device__ __forceinline__ void precision_from_raw(float t0, float t1, float t2, float t3, float t4,
+                                                   float t5, float beta, float4& q1, float& s12,
+                                                   float& s22) {
+    const float l11 = t0 * t0 + beta;
+    const float l12 = t1;
+    const float l13 = t2;
+    const float l22 = t3 * t3 + beta;
+    const float l23 = t4;
+    const float l33 = t5 * t5 + beta;
+    q1.x = l11 * l11;
+    q1.y = l11 * l12;
+    q1.z = l11 * l13;
+    q1.w = l12 * l12 + l22 * l22;
+    s12 = l12 * l13 + l22 * l23;
+    s22 = l13 * l13 + l23 * l23 + l33 * l33;
+}
+
+__device__ __forceinline__ Staged stage_gaussian(const float4* __restrict__ pack, int g, const Geo& F,
+                                                 float chi2, float beta) {
+    const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+    Staged s;
+    s.q0 = a;
+    float s12, s22;
+    precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, s.q1, s12, s22);
+    const float3 m = make_float3(a.x, a.y, a.z);
+    const float dterm = f3_dot(f3_sub(m, F.o), F.ele);
+    s.q2 = make_float4(s12, s22, c.z, dterm);
+    float r_lat, r_ax, r_ele;
+    window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, F.lat, F.ax, F.ele, r_lat, r_ax, r_ele);
+    s.q3 = make_float4(r_lat, r_ax, 0.0f, 0.0f);
+    return s;
+}
+
+// Reference window test (src/mapper/core.cu:166-182): |(p-m).lat| <= r_lat && |(p-m).ax| <= r_ax.
+__device__ __forceinline__ bool window_hit(const float3 d, const float3 lat, const float3 ax, float r_lat,
+                                           float r_ax) {
+    const float dl = fabsf(f3_dot(d, lat));
+    const float da = fabsf(f3_dot(d, ax));
+    return dl <= r_lat && da <= r_ax;
+}
+
+// Quadratic form d^T Lambda d in the reference's term order (include/shader/shared.cuh:41-52).
+__device__ __forceinline__ float quad_form(const float3 d, const float4 q1, const float s12, const float s22) {
+    return (q1.x * d.x + q1.y * d.y + q1.z * d.z) * d.x + (q1.y * d.x + q1.w * d.y + s12 * d.z) * d.y +
+           (q1.z * d.x + s12 * d.y + s22 * d.z) * d.z;
+}
+
+__device__ __forceinline__ int find_tile_coords(const Geo& geo, int64_t t, int& tx, int& ty) {
+    const int lt = (int)(t - geo.tile_off);
+    tx = lt % geo.tx;
+    ty = lt / geo.tx;
+    return lt;
+}
+
+__global__ void __launch_bounds__(TILE_PIX)
+forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
+               const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
+               const long long* __restrict__ header, const float4* __restrict__ pack,
+               const float* __restrict__ pixels, float chi2, float beta, float bg_alpha,
+               float bg_intensity, float* __restrict__ out_image, float* __restrict__ out_alpha,
+               float* __restrict__ out_depth, int* __restrict__ out_counts,
+               float2* __restrict__ pixel_aux) {
+    __shared__ Staged sg[FWD_BATCH];
+    const int64_t t = blockIdx.x;
+    if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
+    const Geo geo = load_geo(frames + tile_frame[t]);
+    int tx, ty;
+    find_tile_coords(geo, t, tx, ty);
+    const int px = tx * TILE + (threadIdx.x & (TILE - 1));
+    const int py = ty * TILE + (threadIdx.x / TILE);
+    const int64_t p = (int64_t)geo.pix_off + (int64_t)py * geo.W + px;
+    const bool valid = px < geo.W && py < geo.H && p < P;
+    float3 pv = make_float3(0.f, 0.f, 0.f);
+    if (valid) pv = make_float3(pixels[3 * p], pixels[3 * p + 1], pixels[3 * p + 2]);
+    const int s0 = tile_start[t];
+    const int n = tile_start[t + 1] - s0;
+
+    int cnt = 0;
+    float sa = 0.f, sc = 0.f, sd = 0.f, sc_ns = 0.f, sd_ns = 0.f;
+    for (int b0 = 0; b0 < n; b0 += FWD_BATCH) {
+        const int nb = min(FWD_BATCH, n - b0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nb; j += blockDim.x)
+            sg[j] = stage_gaussian(pack, sorted_gid[s0 + b0 + j], geo, chi2, beta);
+        __syncthreads();
+        if (valid) {
+            for (int j = 0; j < nb; ++j) {
+                const float4 q0 = sg[j].q0;
+                const float4 q3 = sg[j].q3;
+                const float3 d = make_float3(pv.x - q0.x, pv.y - q0.y, pv.z - q0.z);
+                if (!window_hit(d, geo.lat, geo.ax, q3.x, q3.y)) continue;
+                ++cnt;
+                const float4 q1 = sg[j].q1;
+                const float4 q2 = sg[j].q2;
+                const float q = quad_form(d, q1, q2.x, q2.y);
+                if (q > chi2) continue;
+                const float w = __expf(-0.5f * q);
+                const float ah = q0.w * w;
+                sc_ns += ah * q2.z;
+                sd_ns += ah * q2.w;
+                if (ah <= 1e-8f) continue;
+                sa += ah;
+                sc += ah * q2.z;
+                sd += ah * q2.w;
+            }
+        }
+    }
+    if (!valid) return;
+    const float alpha_total = sa + bg_alpha;
+    const float num = sc + bg_alpha * bg_intensity;
+    const float img = num / fmaxf(alpha_total, 1e-8f);
+    out_alpha[p] = alpha_total;
+    out_image[p] = fmaxf(0.0f, fminf(1.0f, img));
+    out_depth[p] = sd / fmaxf(sa, 1e-8f);
+    if (out_counts) out_counts[p] = cnt;
+    pixel_aux[p] = make_float2(sc_ns, sd_ns);
+}
+
+// One block per tile; thread k owns instance k of the tile list (strided by the block) and
+// sweeps the tile's pixels, which sit in shared memory with their upstream coefficients.
+__global__ void __launch_bounds__(TILE_PIX)
+backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
+                const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
+                const int* __restrict__ sorted_inst, const long long* __restrict__ header,
+                const float4* __restrict__ pack, const float* __restrict__ pixels,
+                const float* __restrict__ d_image, const float* __restrict__ d_alpha,
+                const float* __restrict__ d_depth, const float* __restrict__ saved_alpha,
+                const float2* __restrict__ pixel_aux, float chi2, float beta, float bg_alpha,
+                float bg_intensity, float4* __restrict__ partial) {
+    __shared__ float4 s_pa[TILE_PIX];  // pixel position, dL/dnum
+    __shared__ float4 s_pb[TILE_PIX];  // dL/dalpha_total + dL/dsum_alpha (depth), dL/ddepth_weighted
+    const int64_t t = blockIdx.x;
+    if (t >= T || header[H_FLAGS] != 0) return;
+    const int s0 = tile_start[t];
+    const int n = tile_start[t + 1] - s0;
+    if (n <= 0 || tile_frame[t] < 0) return;
+    const Geo geo = load_geo(frames + tile_frame[t]);
+    int tx, ty;
+    find_tile_coords(geo, t, tx, ty);
+    const int rows = min(TILE, geo.H - ty * TILE);
+    const int cols = min(TILE, geo.W - tx * TILE);
+    const int nv = rows * cols;
+    if (threadIdx.x < nv) {
+        const int r = threadIdx.x / cols, c = threadIdx.x - (threadIdx.x / cols) * cols;
+        const int64_t p = (int64_t)geo.pix_off + (int64_t)(ty * TILE + r) * geo.W + (tx * TILE + c);
+        // Per-pixel adjoint coefficients (reference src/shader/backward.cu:175-197).
+        const float sum_alpha = saved_alpha[p] - bg_alpha;
+        const float2 aux = pixel_aux[p];
+        const float alpha_total = sum_alpha + bg_alpha;
+        const float inv_alpha = 1.0f / fmaxf(alpha_total, 1e-8f);
+        const float num = aux.x + bg_alpha * bg_intensity;
+        const float gI = d_image[p], gA = d_alpha[p], gD = d_depth[p];
+        const float dnum = gI * inv_alpha;
+        const float dtot = gA - gI * num * inv_alpha * inv_alpha;
+        const float inv_sa = 1.0f / fmaxf(sum_alpha, 1e-8f);
+        const float ddw = gD * inv_sa;
+        const float dsad = -gD * aux.y * inv_sa * inv_sa;
+        s_pa[threadIdx.x] = make_float4(pixels[3 * p], pixels[3 * p + 1], pixels[3 * p + 2], dnum);
+        s_pb[threadIdx.x] = make_float4(dtot + dsad, ddw, 0.f, 0.f);
+    }
+    __syncthreads();
+
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int g = sorted_gid[s0 + k];
+        const int inst = sorted_inst[s0 + k];
+        const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+        float4 q1;
+        float s12, s22;
+        precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
+        const float3 m = make_float3(a.x, a.y, a.z);
+        const float dterm = f3_dot(f3_sub(m, geo.o), geo.ele);
+        float r_lat, r_ax, r_ele;
+        window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax, r_ele);
+        const float o = a.w, ci = c.z;
+        float acc_c = 0.f, acc_o = 0.f, acc_e = 0.f;
+        float sdx = 0.f, sdy = 0.f, sdz = 0.f;
+        float sxx = 0.f, sxy = 0.f, sxz = 0.f, syy = 0.f, syz = 0.f, szz = 0.f;
+        for (int j = 0; j < nv; ++j) {
+            const float4 pa = s_pa[j];
+            const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
+            if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
+            const float q = quad_form(d, q1, s12, s22);
+            if (q > chi2) continue;
+            const float4 pb = s_pb[j];
+            const float w = __expf(-0.5f * q);
+            const float ah = o * w;
+            const float dah = pa.w * ci + pb.x + pb.y * dterm;
+            acc_c += pa.w * ah;
+            acc_o += dah * w;
+            acc_e += pb.y * ah;
+            const float dq = -0.5f * dah * ah;
+            const float ux = dq * d.x, uy = dq * d.y, uz = dq * d.z;
+            sdx += ux;
+            sdy += uy;
+            sdz += uz;
+            sxx += ux * d.x;
+            sxy += ux * d.y;
+            sxz += ux * d.z;
+            syy += uy * d.y;
+            syz += uy * d.z;
+            szz += uz * d.z;
+        }
+        // d/dmean = -2 Lambda sum(dq d) + sum(ddw * ah) * ele (reference backward.cu:218-228).
+        const float vx = q1.x * sdx + q1.y * sdy + q1.z * sdz;
+        const float vy = q1.y * sdx + q1.w * sdy + s12 * sdz;
+        const float vz = q1.z * sdx + s12 * sdy + s22 * sdz;
+        // dL/dL (lower triangle) from dL/dLambda = sum(dq d d^T) (reference backward.cu:230-255).
+        const float l11 = b.x * b.x + beta, l12 = b.y, l13 = b.z;
+        const float l22 = b.w * b.w + beta, l23 = c.x, l33 = c.y * c.y + beta;
+        const float dl11 = 2.0f * (sxx * l11 + sxy * l12 + sxz * l13);
+        const float dl12 = 2.0f * (sxy * l11 + syy * l12 + syz * l13);
+        const float dl13 = 2.0f * (sxz * l11 + syz * l12 + szz * l13);
+        const float dl22 = 2.0f * (syy * l22 + syz * l23);
+        const float dl23 = 2.0f * (syz * l22 + szz * l23);
+        const float dl33 = 2.0f * (szz * l33);
+        float4* out = partial + 3 * (int64_t)inst;
+        out[0] = make_float4(-2.0f * vx + acc_e * geo.ele.x, -2.0f * vy + acc_e * geo.ele.y,
+                             -2.0f * vz + acc_e * geo.ele.z, acc_o);
+        out[1] = make_float4(dl11 * (2.0f * b.x), dl12, dl13, dl22 * (2.0f * b.w));
+        out[2] = make_float4(dl23, dl33 * (2.0f * c.y), acc_c, 0.f);
+    }
+}
+
+__global__ void __launch_bounds__(256)
+reduce_kernel(int64_t G, const int* __restrict__ inst_offset, const long long* __restrict__ header,
+              const float4* __restrict__ partial, float* __restrict__ d_means, float* __restrict__ d_tril,
+              float* __restrict__ d_opac, float* __restrict__ d_inten) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, c = a;
+    if (header[H_FLAGS] == 0) {
+        const int i0 = inst_offset[g], i1 = inst_offset[g + 1];
+        for (int i = i0; i < i1; ++i) {
+            const float4 x = partial[3 * (int64_t)i], y = partial[3 * (int64_t)i + 1], z = partial[3 * (int64_t)i + 2];
+            a.x += x.x; a.y += x.y; a.z += x.z; a.w += x.w;
+            b.x += y.x; b.y += y.y; b.z += y.z; b.w += y.w;
+            c.x += z.x; c.y += z.y; c.z += z.z;
+        }
+    }
+    d_means[3 * g + 0] = a.x;
+    d_means[3 * g + 1] = a.y;
+    d_means[3 * g + 2] = a.z;
+    d_opac[g] = a.w;
+    d_tril[6 * g + 0] = b.x;
+    d_tril[6 * g + 1] = b.y;
+    d_tril[6 * g + 2] = b.z;
+    d_tril[6 * g + 3] = b.w;
+    d_tril[6 * g + 4] = c.x;
+    d_tril[6 * g + 5] = c.y;
+    d_inten[g] = c.z;
+}
+
+// Per-pixel candidate indices in tile-list order (reference src/mapper/core.cu:237-287).
+__global__ void __launch_bounds__(TILE_PIX)
+pixel_csr_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
+                 const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
+                 const long long* __restrict__ header, const float4* __restrict__ pack,
+                 const float* __restrict__ pixels, float chi2, float beta, const int* __restrict__ offsets,
+                 int* __restrict__ out_indices) {
+    __shared__ float4 s_m[FWD_BATCH];   // mean, gaussian index (as float bits)
+    __shared__ float2 s_r[FWD_BATCH];   // r_lat, r_ax
+    const int64_t t = blockIdx.x;
+    if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
+    const Geo geo = load_geo(frames + tile_frame[t]);
+    int tx, ty;
+    find_tile_coords(geo, t, tx, ty);
+    const int px = tx * TILE + (threadIdx.x & (TILE - 1));
+    const int py = ty * TILE + (threadIdx.x / TILE);
+    const int64_t p = (int64_t)geo.pix_off + (int64_t)py * geo.W + px;
+    const bool valid = px < geo.W && py < geo.H && p < P;
+    float3 pv = make_float3(0.f, 0.f, 0.f);
+    int wp = 0;
+    if (valid) {
+        pv = make_float3(pixels[3 * p], pixels[3 * p + 1], pixels[3 * p + 2]);
+        wp = offsets[p];
+    }
+    const int s0 = tile_start[t];
+    const int n = tile_start[t + 1] - s0;
+    for (int b0 = 0; b0 < n; b0 += FWD_BATCH) {
+        const int nb = min(FWD_BATCH, n - b0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+            const int g = sorted_gid[s0 + b0 + j];
+            const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+            float r_lat, r_ax, r_ele;
+            window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax, r_ele);
+            s_m[j] = make_float4(a.x, a.y, a.z, __int_as_float(g));
+            s_r[j] = make_float2(r_lat, r_ax);
+        }
+        __syncthreads();
+        if (valid) {
+            for (int j = 0; j < nb; ++j) {
+                const float4 m = s_m[j];
+                const float2 r = s_r[j];
+                const float3 d = make_float3(pv.x - m.x, pv.y - m.y, pv.z - m.z);
+                if (window_hit(d, geo.lat, geo.ax, r.x, r.y)) out_indices[wp++] = __float_as_int(m.w);
+            }
+        }
+    }
+}
+
+__global__ void export_kernel(int tile_off, int n_tiles_frame, const int* __restrict__ tile_start,
+                              const unsigned long long* __restrict__ keys, const int* __restrict__ sorted_gid,
+                              int64_t* __restrict__ out_keys, int* __restrict__ out_values,
+                              int* __restrict__ rs, int* __restrict__ re) {
+    const int lt = blockIdx.x;
+    if (lt >= n_tiles_frame) return;
+    const int base = tile_start[tile_off];
+    const int s0 = tile_start[tile_off + lt];
+    const int s1 = tile_start[tile_off + lt + 1];
+    if (threadIdx.x == 0) {
+        rs[lt] = (s1 > s0) ? s0 - base : -1;
+        re[lt] = (s1 > s0) ? s1 - base : -1;
+    }
+    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        out_keys[s - base] = (int64_t)(((unsigned long long)(uint32_t)lt << 32) | (keys[s] >> 32));
+        out_values[s - base] = sorted_gid[s];
+    }
+}
+
+}  // namespace ug
+}  // namespace us3d
+
+using namespace us3d;
+using namespace us3d::ug;
+
+// Per-device flag: the sort kernel's dynamic shared-memory limit has been raised.
+static bool g_sort_attr_done[128];
+
+static int ensure_sort_attr() {
+    int dev = 0;
+    US3D_CHECK_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 128 && g_sort_attr_done[dev]) return US3D_OK;
+    US3D_CHECK_CUDA(cudaFuncSetAttribute(tile_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         SORT_SMEM_CAP * (int)(sizeof(unsigned long long) + sizeof(int))));
+    if (dev >= 0 && dev < 128) g_sort_attr_done[dev] = true;
+    return US3D_OK;
+}
+
+extern "C" size_t us3d_ug_workspace_bytes(int64_t n_gauss, int32_t n_frames, int64_t n_tiles,
+                                          int64_t n_pixels, int64_t instance_capacity) {
+    (void)n_frames;
+    if (n_gauss < 0 || n_tiles < 0 || n_pixels < 0 || instance_capacity < 0) return 0;
+    return carve(nullptr, n_gauss, n_tiles, n_pixels, instance_capacity).bytes;
+}
+
+extern "C" size_t us3d_ug_backward_scratch_bytes(int64_t instance_capacity) {
+    if (instance_capacity < 0) return 0;
+    return (size_t)instance_capacity * 3 * sizeof(float4);
+}
+
+static int check_common(const us3d_slice_frame* frames, int32_t n_frames, int64_t n_tiles, int64_t n_pixels,
+                        int64_t n_gauss) {
+    US3D_CHECK_ARG(frames != nullptr || n_frames == 0, "frames table is NULL");
+    US3D_CHECK_ARG(n_frames >= 0 && n_tiles >= 0 && n_pixels >= 0 && n_gauss >= 0, "negative size");
+    US3D_CHECK_ARG(n_gauss <= 0x7fffffffLL, "n_gauss must fit in int32");
+    US3D_CHECK_ARG(n_pixels <= 0x7fffffffLL && n_tiles <= 0x7fffffffLL, "pixel/tile count must fit in int32");
+    return US3D_OK;
+}
+
+// Reads the header of a binned workspace (synchronises the stream).
+static int read_header(const void* workspace, long long hdr[H_WORDS], cudaStream_t stream) {
+    US3D_CHECK_ARG(workspace != nullptr, "workspace is NULL");
+    US3D_CHECK_CUDA(cudaMemcpyAsync(hdr, workspace, sizeof(long long) * H_WORDS, cudaMemcpyDeviceToHost, stream));
+    US3D_CHECK_CUDA(cudaStreamSynchronize(stream));
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames,
+                           int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
+                           const float* means, const float* tril, const float* opac, const float* inten,
+                           float chi2, float beta, int32_t sort_by_depth, int64_t cap, void* stream_) {
+    int st = check_common(frames, n_frames, n_tiles, n_pixels, n_gauss);
+    if (st != US3D_OK) return st;
+    US3D_CHECK_ARG(workspace != nullptr, "workspace is NULL");
+    US3D_CHECK_ARG(cap >= 0 && cap <= 0x7fffffffLL, "instance capacity must be in [0, 2^31)");
+    US3D_CHECK_ARG(n_gauss == 0 || (means && tril && opac && inten), "Gaussian parameter pointer is NULL");
+    US3D_CHECK_ARG((reinterpret_cast<uintptr_t>(tril) & 7) == 0, "precision_tril must be 8-byte aligned");
+    US3D_CHECK_ARG(chi2 > 0.f && beta > 0.f, "chi2_threshold and diag_beta must be > 0");
+    const Workspace w = carve(workspace, n_gauss, n_tiles, n_pixels, cap);
+    US3D_CHECK_ARG(workspace_bytes >= w.bytes, "workspace too small: %zu < %zu bytes", workspace_bytes, w.bytes);
+    cudaStream_t stream = (cudaStream_t)stream_;
+
+    const int prof = prof_begin("ug_bin", stream);
+    init_tiles_kernel<<<(unsigned)((n_tiles + 255) / 256 > 0 ? (n_tiles + 255) / 256 : 1), 256, 0, stream>>>(
+        n_tiles, w.tile_count, w.tile_cursor, w.tile_frame, w.header, cap, n_gauss, n_pixels);
+    if (n_frames > 0)
+        setup_kernel<<<n_frames, 256, 0, stream>>>(frames, n_frames, n_tiles, n_pixels, w.tile_frame, w.header);
+    US3D_CHECK_LAUNCH("ug setup");
+    const int gb = (int)((n_gauss + 255) / 256);
+    if (n_gauss > 0) {
+        pack_kernel<<<gb, 256, 0, stream>>>(n_gauss, means, tril, opac, inten, w.pack);
+        count_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, w.touched,
+                                             w.tile_count);
+        US3D_CHECK_LAUNCH("ug count");
+    }
+    US3D_CHECK_CUDA(exclusive_scan(w.touched, n_gauss, w.inst_offset, w.bs_g, w.header + H_SCAN_G, stream));
+    US3D_CHECK_CUDA(exclusive_scan(w.tile_count, n_tiles, w.tile_start, w.bs_t, w.header + H_SCAN_T, stream));
+    check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
+    if (n_gauss > 0) {
+        scatter_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, sort_by_depth,
+                                               w.inst_offset, w.tile_start, w.tile_cursor, w.header, w.keys,
+                                               w.slot_inst);
+        US3D_CHECK_LAUNCH("ug scatter");
+    }
+    if (n_tiles > 0) {
+        st = ensure_sort_attr();
+        if (st != US3D_OK) return st;
+        tile_sort_kernel<<<(unsigned)n_tiles, SORT_THREADS,
+                           SORT_SMEM_CAP * (sizeof(unsigned long long) + sizeof(int)), stream>>>(
+            n_tiles, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst);
+        US3D_CHECK_LAUNCH("ug tile sort");
+    }
+    prof_end(prof, stream);
+    count_launches(1 + (n_frames > 0) + 2 * (n_gauss > 0) + 6 + 1 + (n_gauss > 0) + (n_tiles > 0));
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_read_status(const void* workspace, int64_t* total, int32_t* overflow, void* stream_) {
+    long long hdr[H_WORDS];
+    int st = read_header(workspace, hdr, (cudaStream_t)stream_);
+    if (st != US3D_OK) return st;
+    if (total) *total = hdr[H_TOTAL];
+    if (overflow) *overflow = (int32_t)hdr[H_FLAGS];
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_forward(void* workspace, const us3d_slice_frame* frames, int32_t n_frames, int64_t n_tiles,
+                               int64_t n_pixels, int64_t n_gauss, int64_t cap, const float* pixels, float chi2,
+                               float beta, float bg_alpha, float bg_intensity, float* out_image, float* out_alpha,
+                               float* out_depth, int32_t* out_counts, void* stream_) {
+    int st = check_common(frames, n_frames, n_tiles, n_pixels, n_gauss);
+    if (st != US3D_OK) return st;
+    US3D_CHECK_ARG(workspace != nullptr, "workspace is NULL");
+    US3D_CHECK_ARG(cap >= 0 && cap <= 0x7fffffffLL, "instance capacity must be in [0, 2^31)");
+    US3D_CHECK_ARG(n_pixels == 0 || (pixels && out_image && out_alpha && out_depth), "output pointer is NULL");
+    const Workspace w = carve(workspace, n_gauss, n_tiles, n_pixels, cap);
+    if (n_tiles == 0) return US3D_OK;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    const int prof = prof_begin("ug_forward", stream);
+    forward_kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(
+        n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.header, w.pack, pixels, chi2, beta,
+        bg_alpha, bg_intensity, out_image, out_alpha, out_depth, out_counts, w.pixel_aux);
+    US3D_CHECK_LAUNCH("ug forward");
+    prof_end(prof, stream);
+    count_launches(1);
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames, int32_t n_frames, int64_t n_tiles,
+                                int64_t n_pixels, int64_t n_gauss, int64_t cap, const float* pixels,
+                                const float* d_image, const float* d_alpha, const float* d_depth,
+                                const float* saved_alpha, float chi2, float beta, float bg_alpha,
+                                float bg_intensity, void* scratch, size_t scratch_bytes, float* d_means,
+                                float* d_tril, float* d_opac, float* d_inten, void* stream_) {
+    int st = check_common(frames, n_frames, n_tiles, n_pixels, n_gauss);
+    if (st != US3D_OK) return st;
+    US3D_CHECK_ARG(workspace != nullptr, "workspace is NULL");
+    US3D_CHECK_ARG(cap >= 0 && cap <= 0x7fffffffLL, "instance capacity must be in [0, 2^31)");
+    US3D_CHECK_ARG(scratch != nullptr || cap == 0, "backward scratch is NULL");
+    US3D_CHECK_ARG(scratch_bytes >= us3d_ug_backward_scratch_bytes(cap), "backward scratch too small: %zu < %zu",
+                   scratch_bytes, us3d_ug_backward_scratch_bytes(cap));
+    US3D_CHECK_ARG(n_gauss == 0 || (d_means && d_tril && d_opac && d_inten), "gradient pointer is NULL");
+    US3D_CHECK_ARG(n_pixels == 0 || (pixels && d_image && d_alpha && d_depth && saved_alpha),
+                   "input pointer is NULL");
+    const Workspace w = carve(workspace, n_gauss, n_tiles, n_pixels, cap);
+    cudaStream_t stream = (cudaStream_t)stream_;
+    float4* partial = reinterpret_cast<float4*>(scratch);
+    const int prof = prof_begin("ug_backward", stream);
+    if (n_tiles > 0) {
+        backward_kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(
+            n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_inst, w.header, w.pack,
+            pixels, d_image, d_alpha, d_depth, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha, bg_intensity, partial);
+        US3D_CHECK_LAUNCH("ug backward");
+    }
+    if (n_gauss > 0) {
+        reduce_kernel<<<(unsigned)((n_gauss + 255) / 256), 256, 0, stream>>>(n_gauss, w.inst_offset, w.header,
+                                                                               partial, d_means, d_tril, d_opac,
+                                                                               d_inten);
+        US3D_CHECK_LAUNCH("ug reduce");
+    }
+    prof_end(prof, stream);
+    count_launches((n_tiles > 0) + (n_gauss > 0));
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_pixel_csr(void* workspace, const us3d_slice_frame* frames, int32_t n_frames, int64_t n_tiles,
+                                 int64_t n_pixels, int64_t n_gauss, int64_t cap, const float* pixels, float chi2,
+                                 float beta, const int32_t* offsets, int32_t* out_indices, void* stream_) {
+    int st = check_common(frames, n_frames, n_tiles, n_pixels, n_gauss);
+    if (st != US3D_OK) return st;
+    US3D_CHECK_ARG(workspace != nullptr, "workspace is NULL");
+    US3D_CHECK_ARG(cap >= 0 && cap <= 0x7fffffffLL, "instance capacity must be in [0, 2^31)");
+    US3D_CHECK_ARG(n_pixels == 0 || (pixels && offsets), "input pointer is NULL");
+    const Workspace w = carve(workspace, n_gauss, n_tiles, n_pixels, cap);
+    if (n_tiles == 0) return US3D_OK;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    pixel_csr_kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(n_tiles, n_pixels, frames, w.tile_frame,
+                                                                  w.tile_start, w.sorted_gid, w.header, w.pack,
+                                                                  pixels, chi2, beta, offsets, out_indices);
+    US3D_CHECK_LAUNCH("ug pixel csr");
+    count_launches(1);
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_export_bins(const void* workspace, int64_t n_tiles, int32_t frame_tile_offset,
+                                   int32_t frame_n_tiles, int64_t* out_keys, int32_t* out_values,
+                                   int32_t* out_range_start, int32_t* out_range_end, void* stream_) {
+    cudaStream_t stream = (cudaStream_t)stream_;
+    long long hdr[H_WORDS];
+    int st = read_header(workspace, hdr, stream);
+    if (st != US3D_OK) return st;
+    US3D_CHECK_ARG(hdr[H_T] == n_tiles, "n_tiles does not match the binned workspace");
+    US3D_CHECK_ARG(frame_tile_offset >= 0 && frame_n_tiles >= 0 && frame_tile_offset + (int64_t)frame_n_tiles <= n_tiles,
+                   "frame tile range out of bounds");
+    if (hdr[H_FLAGS] != 0) {
+        us3d::set_error("workspace binning overflowed (flags=%lld)", hdr[H_FLAGS]);
+        return US3D_CAPACITY_OVERFLOW;
+    }
+    const Workspace w = carve(const_cast<void*>(workspace), hdr[H_G], hdr[H_T], hdr[H_P], hdr[H_CAP]);
+    if (frame_n_tiles == 0) return US3D_OK;
+    export_kernel<<<frame_n_tiles, 256, 0, stream>>>(frame_tile_offset, frame_n_tiles, w.tile_start, w.keys,
+                                                     w.sorted_gid, out_keys, out_values, out_range_start,
+                                                     out_range_end);
+    US3D_CHECK_LAUNCH("ug export");
+    count_launches(1);
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_frame_instances(const void* workspace, int64_t n_tiles, int32_t frame_tile_offset,
+                                       int32_t frame_n_tiles, int64_t* first, int64_t* count, void* stream_) {
+    cudaStream_t stream = (cudaStream_t)stream_;
+    long long hdr[H_WORDS];
+    int st = read_header(workspace, hdr, stream);
+    if (st != US3D_OK) return st;
+    US3D_CHECK_ARG(hdr[H_T] == n_tiles, "n_tiles does not match the binned workspace");
+    US3D_CHECK_ARG(frame_tile_offset >= 0 && frame_n_tiles >= 0 && frame_tile_offset + (int64_t)frame_n_tiles <= n_tiles,
+                   "frame tile range out of bounds");
+    const Workspace w = carve(const_cast<void*>(workspace), hdr[H_G], hdr[H_T], hdr[H_P], hdr[H_CAP]);
+    int se[2];
+    US3D_CHECK_CUDA(cudaMemcpyAsync(&se[0], w.tile_start + frame_tile_offset, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    US3D_CHECK_CUDA(cudaMemcpyAsync(&se[1], w.tile_start + frame_tile_offset + frame_n_tiles, sizeof(int),
+                                    cudaMemcpyDeviceToHost, stream));
+    US3D_CHECK_CUDA(cudaStreamSynchronize(stream));
+    if (first) *first = se[0];
+    if (count) *count = se[1] - se[0];
+    return US3D_OK;
+}

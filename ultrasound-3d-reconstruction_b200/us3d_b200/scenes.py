@@ -1,0 +1,135 @@
+"""Seeded synthetic scenes and probe sweeps (the real ultrasound datasets are not available
+offline; these stand in with the distributions the workloads are specified by).
+
+Headline scene: G anisotropic Gaussians in a 64 mm cube, means uniform, per-axis
+log-scales N(log 1.0 mm, 0.3), uniformly random unit quaternions, intensity U(0,1),
+opacity sigmoid(N(0,1)). Frames: planar B-mode slices from a linear sweep (probe moved
+along the elevational axis, tilt N(0, 2 deg) about the lateral axis). All draws come from
+one ``torch.Generator`` in a fixed order.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import List
+
+import torch
+
+
+@dataclass
+class GaussianScene:
+    means: torch.Tensor  # (G,3)
+    scales: torch.Tensor  # (G,3)
+    quats: torch.Tensor  # (G,4) wxyz, unit
+    opacities: torch.Tensor  # (G,)
+    intensities: torch.Tensor  # (G,)
+    precision_tril: torch.Tensor  # (G,6) raw factor, l11,l12,l13,l22,l23,l33
+
+    def to(self, device) -> "GaussianScene":
+        return GaussianScene(*(getattr(self, f).to(device) for f in
+                               ("means", "scales", "quats", "opacities", "intensities", "precision_tril")))
+
+
+@dataclass
+class Slice:
+    height: int
+    width: int
+    lateral_spacing: float
+    axial_spacing: float
+    axial_near: float
+    lateral_col_offset: float
+    origin: torch.Tensor
+    axis_lat: torch.Tensor
+    axis_ax: torch.Tensor
+    axis_ele: torch.Tensor
+    pixels: torch.Tensor  # (H*W, 3) world positions of pixel centres
+
+    def to(self, device) -> "Slice":
+        return Slice(self.height, self.width, self.lateral_spacing, self.axial_spacing, self.axial_near,
+                     self.lateral_col_offset, *(getattr(self, f).to(device) for f in
+                                                ("origin", "axis_lat", "axis_ax", "axis_ele", "pixels")))
+
+
+def quat_to_rot(q: torch.Tensor) -> torch.Tensor:
+    """Rotation matrices of unit (w,x,y,z) quaternions."""
+    w, x, y, z = q.unbind(-1)
+    return torch.stack(
+        [
+            1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+            2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+            2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y),
+        ],
+        dim=-1,
+    ).reshape(*q.shape[:-1], 3, 3)
+
+
+def precision_tril_from_scales_quats(scales: torch.Tensor, quats: torch.Tensor, beta: float = 1e-4) -> torch.Tensor:
+    """Raw lower-Cholesky factor of Lambda = R diag(1/s^2) R^T with diagonal raw^2 + beta
+    (the parameterisation UltraGauss learns); computed in float64."""
+    s = scales.double().clamp_min(beta)
+    R = quat_to_rot(quats.double())
+    lam = R @ torch.diag_embed(1.0 / (s * s)) @ R.transpose(-1, -2)
+    L = torch.linalg.cholesky(lam)
+    diag = torch.diagonal(L, dim1=-2, dim2=-1)
+    raw = (diag - beta).clamp_min(1e-8).sqrt()
+    return torch.stack([raw[:, 0], L[:, 1, 0], L[:, 2, 0], raw[:, 1], L[:, 2, 1], raw[:, 2]], dim=1).float()
+
+
+def make_scene(n: int, seed: int = 0, cube_mm: float = 64.0, log_scale_mean: float = 0.0,
+               log_scale_std: float = 0.3, opacity_mu: float = 0.0, opacity_std: float = 1.0,
+               beta: float = 1e-4) -> GaussianScene:
+    g = torch.Generator().manual_seed(seed)
+    means = torch.rand((n, 3), generator=g) * cube_mm
+    scales = torch.exp(log_scale_mean + log_scale_std * torch.randn((n, 3), generator=g))
+    quats = torch.nn.functional.normalize(torch.randn((n, 4), generator=g), dim=-1)
+    intensities = torch.rand((n,), generator=g)
+    opacities = torch.sigmoid(opacity_mu + opacity_std * torch.randn((n,), generator=g))
+    tril = precision_tril_from_scales_quats(scales, quats, beta)
+    return GaussianScene(means, scales, quats, opacities, intensities, tril)
+
+
+def slice_pixels(origin, lat, ax, H, W, lateral_spacing, axial_spacing, axial_near, col_offset) -> torch.Tensor:
+    """Pixel-centre world positions, row-major (row = axial), as the reference pipeline
+    builds them (pipeline_god_file.py:299-306)."""
+    u = torch.arange(W, dtype=torch.float32)
+    v = torch.arange(H, dtype=torch.float32)
+    lateral_mm = (u - col_offset) * lateral_spacing
+    axial_mm = axial_near + v * axial_spacing
+    yy, xx = torch.meshgrid(axial_mm, lateral_mm, indexing="ij")
+    pix = origin.view(1, 1, 3) + xx[..., None] * lat.view(1, 1, 3) + yy[..., None] * ax.view(1, 1, 3)
+    return pix.reshape(-1, 3).contiguous()
+
+
+def _rot_about(axis: torch.Tensor, angle: float) -> torch.Tensor:
+    axis = axis / axis.norm()
+    x, y, z = axis.tolist()
+    c, s = math.cos(angle), math.sin(angle)
+    C = 1 - c
+    return torch.tensor([[c + x * x * C, x * y * C - z * s, x * z * C + y * s],
+                         [y * x * C + z * s, c + y * y * C, y * z * C - x * s],
+                         [z * x * C - y * s, z * y * C + x * s, c + z * z * C]], dtype=torch.float32)
+
+
+def linear_sweep(n_frames: int, H: int, W: int, spacing_mm: float, seed: int = 0, cube_mm: float = 64.0,
+                 step_mm: float = 2.0, tilt_deg: float = 2.0) -> List[Slice]:
+    """Probe translated ``step_mm`` per frame along elevation through the cube centre,
+    each frame tilted about its lateral axis by N(0, tilt_deg)."""
+    g = torch.Generator().manual_seed(seed + 1_000_003)
+    tilts = torch.randn((n_frames,), generator=g) * math.radians(tilt_deg)
+    out = []
+    col_off = (W - 1) * 0.5
+    depth_mm = H * spacing_mm
+    for f in range(n_frames):
+        z = cube_mm * 0.5 + (f - (n_frames - 1) * 0.5) * step_mm
+        lat0 = torch.tensor([1.0, 0.0, 0.0])
+        ax0 = torch.tensor([0.0, 1.0, 0.0])
+        ele0 = torch.tensor([0.0, 0.0, 1.0])
+        R = _rot_about(lat0, float(tilts[f]))
+        ax = R @ ax0
+        ele = R @ ele0
+        centre = torch.tensor([cube_mm * 0.5, cube_mm * 0.5, z])
+        origin = centre - ax * (depth_mm * 0.5)
+        pix = slice_pixels(origin, lat0, ax, H, W, spacing_mm, spacing_mm, 0.0, col_off)
+        out.append(Slice(H, W, spacing_mm, spacing_mm, 0.0, col_off, origin, lat0.clone(), ax, ele, pix))
+    return out
