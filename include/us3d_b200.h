@@ -181,6 +181,28 @@ US3D_API int us3d_ug_frame_instances(const void* workspace, int64_t n_tiles, int
                             int32_t frame_n_tiles, int64_t* first, int64_t* count,
                             void* stream);
 
+/*
+ * UltraGauss forward render without any device allocation. No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc (an application that owns
+ * the device memory pool, or a real-time pipeline that must not allocate or stall while
+ * it runs). Does us3d_ug_bin + us3d_ug_forward with the workspace taken from one
+ * file-scope device array of US3D_UG_NOALLOC_BYTES bytes that every GPU loading this
+ * library holds until exit. Sizes whose workspace does not fit are rejected
+ * (US3D_INVALID_ARG); an instance total beyond what fits returns US3D_CAPACITY_OVERFLOW.
+ * SYNCHRONISES `stream` once (to read the instance total, also returned in
+ * *out_instances if not NULL). The first call on a device resolves the array's address
+ * and should come before any stream capture on that device. All calls on a device share
+ * the array and keep the last call's contents there: calls that overlap on one GPU race.
+ */
+#define US3D_UG_NOALLOC_BYTES (32 * 1024 * 1024)
+US3D_API int us3d_ug_render_noalloc(const us3d_slice_frame* frames_dev, int32_t n_frames, int64_t n_tiles,
+                                    int64_t n_pixels, int64_t n_gauss, const float* means,
+                                    const float* precision_tril, const float* opacities,
+                                    const float* intensities, const float* pixel_positions,
+                                    float chi2_threshold, float diag_beta, int32_t sort_by_depth,
+                                    float bg_alpha, float bg_intensity, float* out_image, float* out_alpha,
+                                    float* out_depth, int32_t* out_counts, int64_t* out_instances, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -89,6 +89,11 @@ _SIGNATURES = {
     "us3d_ug_frame_instances": (
         c_int32, [c_void_p, c_int64, c_int32, c_int32, POINTER(c_int64), POINTER(c_int64), c_void_p]
     ),
+    "us3d_ug_render_noalloc": (
+        c_int32,
+        [c_void_p, c_int32, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
+         c_float, c_int32, c_float, c_float, c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_int64), c_void_p],
+    ),
 }
 
 _lock = threading.Lock()
