@@ -36,6 +36,12 @@ METRIC = "fwd+bwd frames/s @1M Gaussians 512² (batched vs plain, 1 B200); % HBM
 UNIT = "frames/s"
 BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (params, grads, outputs, upstream)
 
+# DRAM bytes (read + write) per frame of each stage's dominant kernel, from one ncu capture
+# of a 4-frame launch of the same scene, scaled linearly to the frames of a launch.
+NCU_TRAFFIC_PER_FRAME = {
+    "ug_backward": (119.58e6 + 212.23e6) / 4,  # backward_kernel, profiles/ultragauss_backward_kernel_4frames.md
+}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -150,7 +156,7 @@ def run_b200(a):
 
     from us3d_b200 import _lib
     from us3d_b200 import ultragauss as UG
-    from us3d_b200.batch import UltraGaussBatchRenderer
+    from us3d_b200.dist import max_over_ranks
 
     rank, world, local = dist_env()
     if world > 1:
@@ -215,12 +221,7 @@ def run_b200(a):
             fn(warm + i)
         en.record()
         barrier()
-        ms = st.elapsed_time(en)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(st.elapsed_time(en), device=dev)
 
     # -- warm-up + stage selection for the roofline (untimed) --
     stage_ms = {}
@@ -264,8 +265,10 @@ def run_b200(a):
     peaks = json.load(open(ROOT / "MEASURED_PEAKS.json")) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg / (stage_avg_ms / 1e3) / 1e9
+    traffic = NCU_TRAFFIC_PER_FRAME.get(dominant)
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
+                "frac": round(achieved / peak, 4), "traffic": int(traffic * F) if traffic else None,
+                "traffic_source": "ncu dram bytes of a 4-frame launch scaled to the launch's frames" if traffic else None,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
                 "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
                 "algorithmic_bytes_per_launch": int(alg)}

@@ -1,0 +1,91 @@
+"""Host-side logic that needs no GPU: lazy intermediates, frame tables, scenes, config
+validation, loud failure without CUDA, frame sharding."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+
+def test_lazy_dict_resolves_once_and_only_on_access():
+    from us3d_b200.lazy import LazyDict
+
+    calls = []
+    d = LazyDict({"b": lambda: calls.append("b") or 2}, a=1)
+    assert "b" in d and len(d) == 2 and sorted(d.keys()) == ["a", "b"]
+    assert calls == []
+    assert d["b"] == 2 and d["b"] == 2 and calls == ["b"]
+    d["c"] = 3
+    assert dict(d.items()) == {"a": 1, "b": 2, "c": 3}
+    e = LazyDict({"x": lambda: 5})
+    assert {**e} == {"x": 5} and e.get("x") == 5 and e.pop("x") == 5 and "x" not in e
+
+
+def test_frame_table_layout():
+    from us3d_b200 import scenes
+    from us3d_b200 import ultragauss as UG
+
+    frs = [scenes.linear_sweep(3, h, w, 0.5)[i] for i, (h, w) in enumerate([(16, 16), (40, 70), (7, 33)])]
+    specs = [UG.SliceSpec(f.height, f.width, 0.5, 0.5, 0.0, f.lateral_col_offset, f.origin, f.axis_lat, f.axis_ax,
+                          f.axis_ele) for f in frs]
+    ft = UG.build_frame_table(specs, torch.device("cpu"))
+    assert ft.table.shape == (3, 24) and ft.table.dtype == torch.float32
+    ints = ft.table[:, 16:].contiguous().view(torch.int32)
+    assert ints[:, 0].tolist() == [16, 40, 7] and ints[:, 1].tolist() == [16, 70, 33]
+    assert ints[:, 2].tolist() == [1, 5, 3] and ints[:, 3].tolist() == [1, 3, 1]
+    assert ints[:, 4].tolist() == [0, 256, 256 + 2800] and ints[:, 5].tolist() == [0, 1, 16]
+    assert ft.n_tiles == 19 and ft.n_pixels == 256 + 2800 + 231
+    assert torch.allclose(ft.table[1, 3:6], frs[1].axis_lat)
+
+
+def test_scene_is_seeded_and_precision_matches_scales():
+    from us3d_b200 import scenes
+
+    a = scenes.make_scene(500, seed=7)
+    b = scenes.make_scene(500, seed=7)
+    assert torch.equal(a.means, b.means) and torch.equal(a.precision_tril, b.precision_tril)
+    t = a.precision_tril.double()
+    L = torch.zeros(500, 3, 3, dtype=torch.float64)
+    L[:, 0, 0] = t[:, 0] ** 2 + 1e-4
+    L[:, 1, 0], L[:, 2, 0] = t[:, 1], t[:, 2]
+    L[:, 1, 1] = t[:, 3] ** 2 + 1e-4
+    L[:, 2, 1] = t[:, 4]
+    L[:, 2, 2] = t[:, 5] ** 2 + 1e-4
+    R = scenes.quat_to_rot(a.quats.double())
+    lam = R @ torch.diag_embed(1 / a.scales.double() ** 2) @ R.transpose(1, 2)
+    assert torch.allclose(L @ L.transpose(1, 2), lam, rtol=1e-5, atol=1e-6)
+
+
+def test_config_validation_messages():
+    from ultragauss_renderer import UltraGaussRenderConfig
+
+    with pytest.raises(ValueError, match="H/W must be positive"):
+        UltraGaussRenderConfig(H=0, W=4, lateral_spacing_mm_per_pix=1, axial_spacing_mm_per_pix=1, axial_near_mm=0)
+    with pytest.raises(ValueError, match="chi2_threshold must be > 0"):
+        UltraGaussRenderConfig(H=4, W=4, lateral_spacing_mm_per_pix=1, axial_spacing_mm_per_pix=1, axial_near_mm=0,
+                               chi2_threshold=0)
+    c = UltraGaussRenderConfig(H=4, W=9, lateral_spacing_mm_per_pix=1, axial_spacing_mm_per_pix=1, axial_near_mm=0)
+    assert c.lateral_col_offset == 4.0
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU behaviour")
+def test_renderer_fails_loudly_without_cuda():
+    from ultragauss_renderer import SliceGeometry, UltraGaussRenderConfig, UltraGaussRenderer
+
+    cfg = UltraGaussRenderConfig(H=4, W=4, lateral_spacing_mm_per_pix=1, axial_spacing_mm_per_pix=1, axial_near_mm=0)
+    g = SliceGeometry(torch.zeros(3), torch.tensor([1.0, 0, 0]), torch.tensor([0, 1.0, 0]), torch.tensor([0, 0, 1.0]))
+    with pytest.raises(RuntimeError, match="requires CUDA"):
+        UltraGaussRenderer(cfg)(torch.zeros(1, 3), torch.ones(1, 6), torch.ones(1), torch.ones(1), torch.zeros(16, 3), g)
+
+
+def test_shard_frames_partition():
+    from us3d_b200.dist import shard_frames
+
+    for n in (0, 1, 7, 16, 33):
+        for w in (1, 2, 3, 8):
+            parts = [shard_frames(n, r, w) for r in range(w)]
+            assert sum(parts, []) == list(range(n))
+            assert max(map(len, parts)) - min(map(len, parts)) <= 1
+    with pytest.raises(ValueError):
+        shard_frames(4, 2, 2)
