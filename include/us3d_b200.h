@@ -10,6 +10,10 @@
  *
  * Reference interfaces replaced (paths inside the reference project
  * KevinWCCC/ultrasound-3d-reconstruction):
+ *   GaussianPile: ops/gaussianplie_renderer/src/bindings.cpp:5-8
+ *                (ProjectedSliceForwardCUDA, ProjectedSliceBackwardCUDA)
+ *   slice-adapted 3DGS: ops/slice_adapted_3dgs_renderer/src/bindings.cpp:46-91
+ *                (forward, backward, bounded_forward, bounded_backward)
  *   UltraGauss:  ops/ultragauss_renderer/src/bindings.cpp:6-10
  *                (MapperForwardCUDA  -> src/mapper/wrapper_mapper.cu:35-206,
  *                 ShaderForwardCUDA  -> src/shader/wrapper_shader.cu:17-66,
@@ -180,6 +184,105 @@ US3D_API int us3d_ug_export_bins(const void* workspace, int64_t n_tiles, int32_t
 US3D_API int us3d_ug_frame_instances(const void* workspace, int64_t n_tiles, int32_t frame_tile_offset,
                             int32_t frame_n_tiles, int64_t* first, int64_t* count,
                             void* stream);
+
+/* ------------------------------------------------------------------------------------
+ * GaussianPile projected-slice ("us_focus") additive splatting, one slice per call.
+ *
+ * Gaussians (device, fp32): means (G,3), scales (G,3), quats (G,4) as (w,x,y,z),
+ * opacities (G), intensities (G). pose (16 floats, row-major 4x4; probe axes are its
+ * normalised columns 0..2 and the origin its column 3), grid_pack (16 floats, the
+ * reference's slice grid layout), focus_params (14 floats, the reference's us_focus
+ * parameter layout) are device arrays. The reference passes the same values as these
+ * scalar arguments and as the pack; both are taken here so that each computation reads
+ * the one the reference reads.
+ * ---------------------------------------------------------------------------------- */
+
+US3D_API size_t us3d_gp_workspace_bytes(int64_t n_gauss, int32_t height, int32_t width, int32_t tile_size,
+                                        int64_t instance_capacity);
+US3D_API size_t us3d_gp_backward_scratch_bytes(int64_t n_gauss, int64_t instance_capacity);
+
+/* Mapper + forward: footprints, tile rectangles, keys, per-tile order, ranges and the
+ * additive image (H,W). Replaces ProjectedSliceForwardCUDA
+ * (ops/gaussianplie_renderer/src/shader/wrapper_shader.cu:49-217) for the us_focus shader
+ * with the tile mapper and additive compositing. Never synchronises. */
+US3D_API int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t n_gauss, const float* means,
+                             const float* scales, const float* quats, const float* opacities,
+                             const float* intensities, const float* pose, const float* grid_pack,
+                             const float* focus_params, int32_t height, int32_t width, float lateral_spacing,
+                             float axial_spacing, float axial_near, int32_t tile_size, float k_sigma,
+                             int32_t sort_by_v, int64_t instance_capacity, float* out_image, void* stream);
+
+/* Instance total and flags of the last us3d_gp_forward (SYNCHRONISES `stream`). */
+US3D_API int us3d_gp_read_status(const void* workspace, int64_t* total_instances, int32_t* overflow,
+                                 void* stream);
+
+/* Backward: gradients w.r.t. means (G,3), scales (G,3), quats (G,4), opacities,
+ * intensities and, if pose_grad, the pose (4x4). Scale and quaternion gradients are the
+ * reference's central differences (step 1e-3) of the footprint/adjoint dot product;
+ * gradients are NaN-sanitised and clamped to +-1e3 as in the reference. Deterministic.
+ * Replaces ProjectedSliceBackwardCUDA (wrapper_shader.cu:218-416; kernels
+ * src/shader/us_focus.cu:479-966). */
+US3D_API int us3d_gp_backward(void* workspace, int64_t n_gauss, const float* means, const float* scales,
+                              const float* quats, const float* opacities, const float* intensities,
+                              const float* pose, const float* grid_pack, const float* focus_params,
+                              int32_t height, int32_t width, int32_t tile_size, float k_sigma,
+                              int64_t instance_capacity, const float* grad_image, int32_t pose_grad,
+                              void* scratch, size_t scratch_bytes, float* d_means, float* d_scales,
+                              float* d_quats, float* d_opacities, float* d_intensities, float* d_pose,
+                              void* stream);
+
+/* Sorted Gaussian ids (instance total entries), tile ranges (-1 for empty tiles) and
+ * per-Gaussian tile rectangles (G x int4, may be NULL) in the reference's format
+ * (OursTileGaussMapperCUDA, src/mapper/core_tile.cu:238-379). */
+US3D_API int us3d_gp_export_bins(const void* workspace, int64_t n_gauss, int32_t height, int32_t width,
+                                 int32_t tile_size, int64_t instance_capacity, int32_t* out_sorted_ids,
+                                 int32_t* out_range_start, int32_t* out_range_end, int32_t* out_rects,
+                                 void* stream);
+
+/* ------------------------------------------------------------------------------------
+ * slice-adapted 3DGS: bounded additive splatting of projected 2D Gaussians.
+ *
+ * Inputs (device, fp32): means2d (N,2) in slice-plane mm, inv2d (N,2,2) inverse 2D
+ * covariances, weights (N), colors (N,3). Pixel (x, y) sits at
+ * (-half_width + 2 half_width x/(W-1), -half_height + 2 half_height y/(H-1)).
+ * Outputs: image (H*W, 3) RGB and alpha (H*W) weight sums, as the reference returns them.
+ * ---------------------------------------------------------------------------------- */
+
+US3D_API size_t us3d_sa_workspace_bytes(int64_t n, int32_t height, int32_t width, int64_t instance_capacity);
+US3D_API size_t us3d_sa_backward_scratch_bytes(int64_t instance_capacity);
+
+/* Replaces bounded_forward (ops/slice_adapted_3dgs_renderer/src/render.cu:836-921) for
+ * every N (the reference scatters with atomics below 16384 Gaussians and bins above;
+ * results agree up to summation order). Never synchronises. */
+US3D_API int us3d_sa_bounded_forward(void* workspace, size_t workspace_bytes, int64_t n, int32_t height,
+                                     int32_t width, float half_width, float half_height, const float* means2d,
+                                     const float* inv2d, const float* weights, const float* colors,
+                                     float radius_sigma, int64_t instance_capacity, float* out_image,
+                                     float* out_alpha, void* stream);
+US3D_API int us3d_sa_read_status(const void* workspace, int64_t* total_instances, int32_t* overflow,
+                                 void* stream);
+/* Replaces bounded_backward (render.cu:923-1013): gradients w.r.t. means2d (N,2),
+ * inv2d (N,2,2), weights (N) and colors (N,3). Deterministic. */
+US3D_API int us3d_sa_bounded_backward(void* workspace, int64_t n, int32_t height, int32_t width, float half_width,
+                                      float half_height, const float* means2d, const float* inv2d,
+                                      const float* weights, const float* colors, const float* grad_image,
+                                      const float* grad_alpha, float radius_sigma, int64_t instance_capacity,
+                                      void* scratch, size_t scratch_bytes, float* d_means2d, float* d_inv2d,
+                                      float* d_weights, float* d_colors, void* stream);
+/* Sorted Gaussian ids and tile ranges (-1 for empty tiles) of the 16x16 binning
+ * (reference build_tile_binning, render.cu:673-760). */
+US3D_API int us3d_sa_export_bins(const void* workspace, int64_t n, int32_t height, int32_t width,
+                                 int64_t instance_capacity, int32_t* out_sorted_ids, int32_t* out_range_start,
+                                 int32_t* out_range_end, void* stream);
+/* Unbounded splat over arbitrary pixel coordinates (P,2): replaces forward / backward
+ * (render.cu:41-153, the package's additive_splat). */
+US3D_API int us3d_sa_dense_forward(int64_t n_pixels, int64_t n, const float* pixels, const float* means2d,
+                                   const float* inv2d, const float* weights, const float* colors,
+                                   float* out_image, float* out_alpha, void* stream);
+US3D_API int us3d_sa_dense_backward(int64_t n_pixels, int64_t n, const float* pixels, const float* means2d,
+                                    const float* inv2d, const float* weights, const float* colors,
+                                    const float* grad_image, const float* grad_alpha, float* d_means2d,
+                                    float* d_inv2d, float* d_weights, float* d_colors, void* stream);
 
 /*
  * UltraGauss forward render without any device allocation. No counterpart in the

@@ -33,6 +33,25 @@ MODULES = {
          "src/shader/forward.cu", "src/shader/backward.cu", "src/bindings.cpp"],
         ["-O3", "--use_fast_math", "-lineinfo", "-DTHRUST_IGNORE_CUB_VERSION_CHECK"],
     ),
+    "gaussianplie_ref_C": (
+        "ops/gaussianplie_renderer",
+        ["src/bindings.cpp", "src/mapper/core_tile.cu", "src/mapper/core_pixel.cu", "src/shader/forward.cu",
+         "src/shader/backward.cu", "src/shader/plane_cond2d.cu", "src/shader/us_focus.cu",
+         "src/shader/wrapper_shader.cu"],
+        ["-O3", "--use_fast_math", "-lineinfo", "-DTHRUST_IGNORE_CUB_VERSION_CHECK"],
+    ),
+    "slice_adapted_ref_C": (
+        "ops/slice_adapted_3dgs_renderer",
+        ["src/bindings.cpp", "src/render.cu"],
+        ["-O3", "--use_fast_math", "-lineinfo"],
+    ),
+    # The reference's render.cu included by oracle/ref_harness/slice_adapted_bins.cu, which
+    # exposes its internal tile binning.
+    "slice_adapted_ref_bins": (
+        "ops/slice_adapted_3dgs_renderer",
+        ["HARNESS:slice_adapted_bins.cu"],
+        ["-O3", "--use_fast_math", "-lineinfo"],
+    ),
     # The reference's mapper kernels plus oracle/ref_harness/ultragauss_keys.cu, which runs
     # them the way MapperForwardCUDA does and returns its private sorted keys and ranges.
     "ultragauss_ref_keys": (
@@ -65,7 +84,7 @@ def build_module(name: str, reference: Path, force: bool = False) -> Path:
     obj_dir.mkdir(parents=True, exist_ok=True)
     inc, libdirs, abi = _torch_flags()
     defs = [f"-DTORCH_EXTENSION_NAME={name}", "-DTORCH_API_INCLUDE_EXTENSION_H", f"-D_GLIBCXX_USE_CXX11_ABI={abi}"]
-    incs = ["-I", str(root / "include"), "-I", str(SHIM)] + [x for p in inc for x in ("-I", p)]
+    incs = ["-I", str(root / "include"), "-I", str(root / "src"), "-I", str(SHIM)] + [x for p in inc for x in ("-I", p)]
     objs = []
     for s in srcs:
         src = (HERE / "ref_harness" / s.split(":", 1)[1]) if s.startswith("HARNESS:") else root / s

@@ -1,0 +1,107 @@
+"""GaussianPile parity on the GPU through the C ABI: against golden fixtures from the
+reference's own CUDA build, the live reference build, and the C oracle.
+
+Tolerances: tile rectangles, sorted ids and tile ranges bit-exact; images <= 1e-5
+relative L2; mean / opacity / intensity / pose gradients <= 1e-4 relative L2 against the
+reference backward. Scale and quaternion gradients are, as in the reference, central
+differences (step 1e-3) of an adjoint-weighted footprint in fp32; they are compared at
+<= 1e-3 relative L2, because the reference's own float-atomic accumulation order changes
+the adjoint in its last bits and the finite difference amplifies that.
+"""
+
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from gp_helpers import gp_golden_names, load_gp, run_b200_gp
+from ug_helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _check(out, fx):
+    vis = fx["ref_rects"][:, 0] < fx["ref_rects"][:, 2]
+    np.testing.assert_array_equal(out["rects"][vis], fx["ref_rects"][vis], err_msg="tile rectangles")
+    np.testing.assert_array_equal(out["sorted_ids"], fx["ref_sorted_ids"], err_msg="sorted ids")
+    np.testing.assert_array_equal(out["range_start"], fx["ref_range_start"], err_msg="range start")
+    np.testing.assert_array_equal(out["range_end"], fx["ref_range_end"], err_msg="range end")
+    assert rel_l2(out["image"], fx["ref_image"]) <= 1e-5, rel_l2(out["image"], fx["ref_image"])
+    for k in ("d_means", "d_opacity", "d_intensity"):
+        assert rel_l2(out[k], fx["ref_" + k]) <= 1e-4, (k, rel_l2(out[k], fx["ref_" + k]))
+    if int(fx["pose_grad"]):
+        assert rel_l2(out["d_pose"], fx["ref_d_pose"]) <= 1e-4, rel_l2(out["d_pose"], fx["ref_d_pose"])
+    for k in ("d_scales", "d_quats"):
+        assert rel_l2(out[k], fx["ref_" + k]) <= 1e-3, (k, rel_l2(out[k], fx["ref_" + k]))
+
+
+@pytest.mark.parametrize("name", gp_golden_names() or ["c1"])
+def test_gaussianpile_golden_parity(name, cuda_device):
+    fx = load_gp(name)
+    _check(run_b200_gp(fx, cuda_device), fx)
+
+
+def test_gaussianpile_live_reference(cuda_device):
+    p = ROOT / "oracle" / "_ref"
+    if not any(p.glob("gaussianplie_ref_C*.so")):
+        pytest.skip("reference build not present")
+    sys.path.insert(0, str(p))
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    import make_gaussianpile_golden as MG
+
+    from us3d_b200 import scenes
+
+    sc = scenes.make_scene(20000, seed=9, cube_mm=60.0, opacity_mu=-1.0)
+    fx = MG.run("live", sc, MG.pose_matrix(3.0, (0.2, 1, 0), (30.0, 5.0, 30.0)),
+                dict(H=256, W=256, lat=0.2, ax=0.2, near=0.0, centre=True, sigma_z=1.0, pose_grad=True))
+    _check(run_b200_gp(fx, cuda_device), fx)
+
+
+def test_gaussianpile_oracle_agreement(cuda_device):
+    from oracle import gaussianpile_oracle as GO
+
+    fx = load_gp("c1")
+    out = run_b200_gp(fx, cuda_device)
+    m = fx["meta"].tolist()
+    st = GO.render(fx["means"], fx["scales"], fx["quats"], fx["opacities"], fx["intensities"], fx["pose"], fx["grid"],
+                   fx["params"], int(fx["H"]), int(fx["W"]), m[2], m[3], m[4], int(m[5]), m[8])
+    np.testing.assert_array_equal(st["sorted_ids"], out["sorted_ids"])
+    assert rel_l2(out["image"], st["image"]) <= 1e-5
+    g = GO.backward(st, fx["grad_image"], pose_grad=True)
+    for k in ("d_means", "d_opacity"):
+        assert rel_l2(out[k], g[k]) <= 1e-4, (k, rel_l2(out[k], g[k]))
+    # The pose gradient is a sum over all Gaussians with heavy cancellation; the CPU
+    # restatement (IEEE division/exp, no FMA) and the fast-math GPU build differ by a few
+    # 1e-4 there. Against the reference's own GPU build it agrees to 1e-4 (golden tests).
+    assert rel_l2(out["d_pose"], g["d_pose"]) <= 2e-3
+
+
+def test_gaussianpile_dropin_api(cuda_device):
+    """GaussianPlieRenderer through autograd equals the low-level path; pose gradient only
+    when the pose requires grad."""
+    from types import SimpleNamespace
+
+    from gaussianplie_renderer import GaussianPlieRenderConfig, GaussianPlieRenderer, build_slice_grid_pack
+
+    fx = load_gp("c1")
+    dev = cuda_device
+    cfg = GaussianPlieRenderConfig(H=int(fx["H"]), W=int(fx["W"]), lateral_spacing_mm_per_pix=0.3,
+                                   axial_spacing_mm_per_pix=0.3, axial_near_mm=0.0, sigma_z_mm=1.0)
+    r = GaussianPlieRenderer(cfg)
+    r.set_slice_grid_geometry(build_slice_grid_pack(SimpleNamespace(H=cfg.H, W=cfg.W, delta_lateral_mm=0.3,
+                                                                    delta_axial_mm=0.3, near_mm=0.0,
+                                                                    center_lateral=True), dev))
+    T = lambda k: torch.as_tensor(fx[k]).to(dev).requires_grad_(True)  # noqa: E731
+    means, scales, quats, alphas = T("means"), T("scales"), T("quats"), T("opacities")
+    pose = torch.as_tensor(fx["pose"]).to(dev).requires_grad_(True)
+    img = r(means, scales, quats, alphas, pose)
+    assert img.shape == (cfg.H, cfg.W)
+    (img * torch.as_tensor(fx["grad_image"]).to(dev)).sum().backward()
+    assert rel_l2(img.detach().cpu().numpy(), fx["ref_image"]) <= 1e-5
+    assert rel_l2(means.grad.cpu().numpy(), fx["ref_d_means"]) <= 1e-4
+    assert rel_l2(pose.grad.cpu().numpy(), fx["ref_d_pose"]) <= 1e-4

@@ -19,7 +19,7 @@ constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 static inline int scan_num_blocks(int64_t n) { return (int)((n + SCAN_TILE - 1) / SCAN_TILE); }
 
 // Inclusive warp scan of a 64-bit value.
-__device__ __forceinline__ long long warp_inclusive_scan(long long v) {
+static __device__ __forceinline__ long long warp_inclusive_scan(long long v) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -30,7 +30,7 @@ __device__ __forceinline__ long long warp_inclusive_scan(long long v) {
 }
 
 // Block-wide exclusive scan (blockDim.x == SCAN_THREADS); returns the block total in *total.
-__device__ __forceinline__ long long block_exclusive_scan(long long v, long long* total) {
+static __device__ __forceinline__ long long block_exclusive_scan(long long v, long long* total) {
     __shared__ long long warp_sums[SCAN_THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     long long inc = warp_inclusive_scan(v);
@@ -51,7 +51,7 @@ __device__ __forceinline__ long long block_exclusive_scan(long long v, long long
     return excl;
 }
 
-__device__ __forceinline__ void load_items(const int* in, int64_t n, int64_t base, int (&x)[SCAN_ITEMS]) {
+static __device__ __forceinline__ void load_items(const int* in, int64_t n, int64_t base, int (&x)[SCAN_ITEMS]) {
     if (base + SCAN_ITEMS <= n && ((reinterpret_cast<uintptr_t>(in + base) & 15) == 0)) {
         const int4* p = reinterpret_cast<const int4*>(in + base);
 #pragma unroll
@@ -65,7 +65,7 @@ __device__ __forceinline__ void load_items(const int* in, int64_t n, int64_t bas
     }
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS)
+static __global__ void __launch_bounds__(SCAN_THREADS)
 scan_reduce_kernel(const int* __restrict__ in, int64_t n, long long* __restrict__ block_sums) {
     const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
     int x[SCAN_ITEMS];
@@ -78,7 +78,7 @@ scan_reduce_kernel(const int* __restrict__ in, int64_t n, long long* __restrict_
     if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS)
+static __global__ void __launch_bounds__(SCAN_THREADS)
 scan_blocksums_kernel(long long* __restrict__ block_sums, int nb, long long* __restrict__ total_out) {
     long long carry = 0;
     for (int base = 0; base < nb; base += SCAN_THREADS) {
@@ -93,7 +93,7 @@ scan_blocksums_kernel(long long* __restrict__ block_sums, int nb, long long* __r
     if (threadIdx.x == 0) *total_out = carry;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS)
+static __global__ void __launch_bounds__(SCAN_THREADS)
 scan_downsweep_kernel(const int* __restrict__ in, int64_t n, const long long* __restrict__ block_sums,
                       const long long* __restrict__ total, int* __restrict__ out) {
     const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;

@@ -89,6 +89,49 @@ _SIGNATURES = {
     "us3d_ug_frame_instances": (
         c_int32, [c_void_p, c_int64, c_int32, c_int32, POINTER(c_int64), POINTER(c_int64), c_void_p]
     ),
+    "us3d_gp_workspace_bytes": (c_size_t, [c_int64, c_int32, c_int32, c_int32, c_int64]),
+    "us3d_gp_backward_scratch_bytes": (c_size_t, [c_int64, c_int64]),
+    "us3d_gp_forward": (
+        c_int32,
+        [c_void_p, c_size_t, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_void_p, c_int32, c_int32, c_float, c_float, c_float, c_int32, c_float, c_int32, c_int64, c_void_p,
+         c_void_p],
+    ),
+    "us3d_gp_read_status": (c_int32, [c_void_p, POINTER(c_int64), POINTER(c_int32), c_void_p]),
+    "us3d_gp_backward": (
+        c_int32,
+        [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_int32, c_int32, c_int32, c_float, c_int64, c_void_p, c_int32, c_void_p, c_size_t, c_void_p, c_void_p,
+         c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
+    ),
+    "us3d_gp_export_bins": (
+        c_int32, [c_void_p, c_int64, c_int32, c_int32, c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                  c_void_p]
+    ),
+    "us3d_sa_workspace_bytes": (c_size_t, [c_int64, c_int32, c_int32, c_int64]),
+    "us3d_sa_backward_scratch_bytes": (c_size_t, [c_int64]),
+    "us3d_sa_bounded_forward": (
+        c_int32,
+        [c_void_p, c_size_t, c_int64, c_int32, c_int32, c_float, c_float, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_float, c_int64, c_void_p, c_void_p, c_void_p],
+    ),
+    "us3d_sa_read_status": (c_int32, [c_void_p, POINTER(c_int64), POINTER(c_int32), c_void_p]),
+    "us3d_sa_bounded_backward": (
+        c_int32,
+        [c_void_p, c_int64, c_int32, c_int32, c_float, c_float, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_void_p, c_float, c_int64, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
+    ),
+    "us3d_sa_export_bins": (
+        c_int32, [c_void_p, c_int64, c_int32, c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]
+    ),
+    "us3d_sa_dense_forward": (
+        c_int32, [c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    ),
+    "us3d_sa_dense_backward": (
+        c_int32,
+        [c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_void_p, c_void_p, c_void_p],
+    ),
     "us3d_ug_render_noalloc": (
         c_int32,
         [c_void_p, c_int32, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
