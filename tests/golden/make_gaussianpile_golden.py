@@ -45,8 +45,10 @@ def cases():
     yield "c1", sc, pose_matrix(5.0, (1, 0.2, 0), (20.0, 1.0, 20.0)), dict(H=128, W=128, lat=0.3, ax=0.3, near=0.0,
                                                                           centre=True, sigma_z=1.0, pose_grad=True)
     sc2 = scenes.make_scene(1500, seed=1, cube_mm=30.0, log_scale_mean=0.3)
-    # the pipeline passes a world->probe pose where the API expects probe->world
-    P = pose_matrix(-8.0, (0.3, 1, 0.1), (12.0, -2.0, 15.0))
+    # the pipeline passes a world->probe pose where the API expects probe->world; build the
+    # probe->world pose so that its inverse still places the slice inside the cloud
+    P = pose_matrix(-8.0, (0.3, 1, 0.1), (0.0, 0.0, 0.0))
+    P[:3, 3] = -(P[:3, :3] @ torch.tensor([15.0, 2.0, 15.0]))
     yield "inverse_pose", sc2, torch.linalg.inv(P), dict(H=64, W=96, lat=0.4, ax=0.35, near=0.0, centre=True,
                                                          sigma_z=0.8, pose_grad=True)
     sc3 = scenes.make_scene(800, seed=3, cube_mm=24.0)

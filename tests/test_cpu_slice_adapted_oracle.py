@@ -1,0 +1,26 @@
+"""The slice-adapted 3DGS C oracle against golden vectors from the reference's own CUDA build."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from sa_helpers import load_sa, sa_golden_names
+from ug_helpers import rel_l2
+
+
+@pytest.mark.parametrize("name", sa_golden_names())
+def test_slice_adapted_oracle_matches_reference_golden(name):
+    from oracle import slice_adapted_oracle as SO
+
+    fx = load_sa(name)
+    st = SO.render(int(fx["H"]), int(fx["W"]), float(fx["half_width"]), float(fx["half_height"]), fx["means2d"],
+                   fx["inv2d"], fx["weights"], fx["colors"], float(fx["radius_sigma"]))
+    np.testing.assert_array_equal(st["sorted_ids"], fx["ref_sorted_ids"])
+    np.testing.assert_array_equal(st["range_start"], fx["ref_range_start"])
+    np.testing.assert_array_equal(st["range_end"], fx["ref_range_end"])
+    assert rel_l2(st["image"], fx["ref_image"]) <= 1e-5
+    assert rel_l2(st["alpha"], fx["ref_alpha"]) <= 1e-5
+    g = SO.backward(st, fx["grad_image"], fx["grad_alpha"])
+    for k in ("d_means", "d_inv", "d_weights", "d_colors"):
+        assert rel_l2(g[k], fx["ref_" + k]) <= 1e-4, (k, rel_l2(g[k], fx["ref_" + k]))
