@@ -284,6 +284,57 @@ US3D_API int us3d_sa_dense_backward(int64_t n_pixels, int64_t n, const float* pi
                                     const float* grad_image, const float* grad_alpha, float* d_means2d,
                                     float* d_inv2d, float* d_weights, float* d_colors, void* stream);
 
+/* ------------------------------------------------------------------------------------
+ * UltraGray: scanline B-mode rendering by ray-Gaussian attenuation integrals.
+ *
+ * Inputs (device, fp32, contiguous): means (G,3), scales (G,3), quats (G,4) (w,x,y,z),
+ * attenuations (G) (raw, sigmoid applied inside), sh_coeffs (G,4) degree-1 echo terms,
+ * pixel_positions (W,H,3), ray_origins (W,3), ray_dirs (W,3), probe origin and axes (3
+ * each), ray_perturbations (W) elevational offsets in mm. W rays (image columns), H
+ * samples per ray. Output image (H,W). The workspace keeps the ray binning and, per
+ * pixel, the forward's (transmission, echo numerator, echo denominator, weight sum) so
+ * the backward needs no recompute pass.
+ * ---------------------------------------------------------------------------------- */
+
+US3D_API size_t us3d_ugr_workspace_bytes(int64_t n_gauss, int32_t width, int32_t height,
+                                         int64_t instance_capacity);
+US3D_API size_t us3d_ugr_backward_scratch_bytes(int64_t instance_capacity);
+
+/* Replaces MapperForwardCUDA followed by ShaderForwardCUDA
+ * (ops/ultragray_renderer/src/mapper/wrapper_mapper.cu:7-128,
+ * src/shader/wrapper_shader.cu:7-58). Never synchronises; an instance total above
+ * instance_capacity sets the overflow flag read by us3d_ugr_read_status and leaves the
+ * image unwritten. */
+US3D_API int us3d_ugr_forward(void* workspace, size_t workspace_bytes, int64_t n_gauss, const float* means,
+                              const float* scales, const float* quats, const float* attenuations,
+                              const float* sh_coeffs, const float* pixel_positions, const float* ray_origins,
+                              const float* ray_dirs, const float* origin, const float* axis_lateral,
+                              const float* axis_elevational, const float* axis_axial,
+                              const float* ray_perturbations, int32_t width, int32_t height, float width_mm,
+                              float near_mm, float lateral_col_offset, float elev_cutoff_mm, float k_sigma,
+                              float quadrature_window_radius_mm, int32_t local_transmission_window_only,
+                              float local_transmission_max_window_mm, int64_t instance_capacity,
+                              float* out_image, void* stream);
+/* Synchronises `stream`: instance total and overflow flags of the last us3d_ugr_forward. */
+US3D_API int us3d_ugr_read_status(const void* workspace, int64_t* total_instances, int32_t* overflow,
+                                  void* stream);
+/* Replaces ShaderBackwardCUDA (src/shader/wrapper_shader.cu:60-123): gradients w.r.t.
+ * means (G,3), scales (G,3), quats (G,4), attenuations (G) and sh_coeffs (G,4), every
+ * entry written. Deterministic (fixed-order per-Gaussian reduction). */
+US3D_API int us3d_ugr_backward(void* workspace, int64_t n_gauss, const float* quats, const float* pixel_positions,
+                               const float* ray_origins, const float* ray_dirs, const float* axis_elevational,
+                               const float* ray_perturbations, int32_t width, int32_t height, float k_sigma,
+                               float quadrature_window_radius_mm, int32_t local_transmission_window_only,
+                               float local_transmission_max_window_mm, int64_t instance_capacity,
+                               const float* grad_image, void* scratch, size_t scratch_bytes, float* d_means,
+                               float* d_scales, float* d_quats, float* d_attenuations, float* d_sh_coeffs,
+                               void* stream);
+/* The ray binning in MapperForwardCUDA's output format: ray_counts (W), ray_offsets (W,
+ * 0 for empty rays), ray_indices and sorted_depths (instance total entries). */
+US3D_API int us3d_ugr_export_csr(const void* workspace, int64_t n_gauss, int32_t width, int32_t height,
+                                 int64_t instance_capacity, int32_t* out_ray_counts, int32_t* out_ray_offsets,
+                                 int32_t* out_ray_indices, float* out_sorted_depths, void* stream);
+
 /*
  * UltraGauss forward render without any device allocation. No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc (an application that owns

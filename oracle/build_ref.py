@@ -40,6 +40,12 @@ MODULES = {
          "src/shader/wrapper_shader.cu"],
         ["-O3", "--use_fast_math", "-lineinfo", "-DTHRUST_IGNORE_CUB_VERSION_CHECK"],
     ),
+    "ultragray_ref_C": (
+        "ops/ultragray_renderer",
+        ["src/bindings.cpp", "src/mapper/wrapper_mapper.cu", "src/mapper/core.cu", "src/shader/wrapper_shader.cu",
+         "src/shader/forward.cu", "src/shader/backward.cu"],
+        ["-O3", "--use_fast_math", "-lineinfo", "-DTHRUST_IGNORE_CUB_VERSION_CHECK"],
+    ),
     "slice_adapted_ref_C": (
         "ops/slice_adapted_3dgs_renderer",
         ["src/bindings.cpp", "src/render.cu"],

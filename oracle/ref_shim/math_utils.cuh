@@ -18,3 +18,12 @@ __device__ __forceinline__ void vec3_copy(const float* src, float* dst) {
     dst[1] = src[1];
     dst[2] = src[2];
 }
+
+// float3 arithmetic used by the reference's UltraGray shader sources.
+__device__ __forceinline__ float3 operator+(const float3 a, const float3 b) {
+    return make_float3(a.x + b.x, a.y + b.y, a.z + b.z);
+}
+
+__device__ __forceinline__ float3 operator*(const float3 a, const float b) {
+    return make_float3(a.x * b, a.y * b, a.z * b);
+}

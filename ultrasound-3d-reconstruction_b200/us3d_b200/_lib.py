@@ -132,6 +132,24 @@ _SIGNATURES = {
         [c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
          c_void_p, c_void_p, c_void_p],
     ),
+    "us3d_ugr_workspace_bytes": (c_size_t, [c_int64, c_int32, c_int32, c_int64]),
+    "us3d_ugr_backward_scratch_bytes": (c_size_t, [c_int64]),
+    "us3d_ugr_forward": (
+        c_int32,
+        [c_void_p, c_size_t, c_int64] + [c_void_p] * 15
+        + [c_int32, c_int32, c_float, c_float, c_float, c_float, c_float, c_float, c_int32, c_float, c_int64,
+           c_void_p, c_void_p],
+    ),
+    "us3d_ugr_read_status": (c_int32, [c_void_p, POINTER(c_int64), POINTER(c_int32), c_void_p]),
+    "us3d_ugr_backward": (
+        c_int32,
+        [c_void_p, c_int64] + [c_void_p] * 6
+        + [c_int32, c_int32, c_float, c_float, c_int32, c_float, c_int64, c_void_p, c_void_p, c_size_t]
+        + [c_void_p] * 6,
+    ),
+    "us3d_ugr_export_csr": (
+        c_int32, [c_void_p, c_int64, c_int32, c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    ),
     "us3d_ug_render_noalloc": (
         c_int32,
         [c_void_p, c_int32, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
