@@ -29,6 +29,39 @@ def test_header_symbols_exported():
     assert sorted(_lib.exported_symbols()) == names
 
 
+def _declared_parameter_lists():
+    text = (ROOT / "include" / "us3d_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"US3D_API\s+([\w\s\*]+?)\b(us3d_\w+)\s*\(([^)]*)\)\s*;", text):
+        params = " ".join(m.group(3).split())
+        out[m.group(2)] = (m.group(1).strip(), [] if params in ("", "void") else params.split(","))
+    return out
+
+
+_CTYPE_OF = {"int32_t": "c_int", "int": "c_int", "int64_t": "c_long", "size_t": "c_ulong", "float": "c_float",
+             "double": "c_double"}
+
+
+def test_binding_signatures_match_header():
+    """Every ctypes signature has the header's arity and, for scalar parameters, its type
+    (pointers of any kind bind as c_void_p or POINTER(...))."""
+    from us3d_b200 import _lib
+
+    decl = _declared_parameter_lists()
+    for name, (res, args) in _lib._SIGNATURES.items():
+        ret, params = decl[name]
+        assert len(args) == len(params), (name, len(args), len(params))
+        for a, p in zip(args, params):
+            p = p.strip()
+            if "*" in p:
+                assert a is ctypes.c_void_p or a is ctypes.c_char_p or hasattr(a, "_type_") and a.__name__.startswith(
+                    "LP_"), (name, p, a)
+            else:
+                ctype = p.replace("const ", "").split()[0]
+                assert a.__name__ == _CTYPE_OF[ctype], (name, p, a.__name__)
+
+
 def test_slice_frame_layout():
     from us3d_b200 import _lib
 

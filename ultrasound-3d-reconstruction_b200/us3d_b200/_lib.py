@@ -136,7 +136,7 @@ _SIGNATURES = {
     "us3d_ugr_backward_scratch_bytes": (c_size_t, [c_int64]),
     "us3d_ugr_forward": (
         c_int32,
-        [c_void_p, c_size_t, c_int64] + [c_void_p] * 15
+        [c_void_p, c_size_t, c_int64] + [c_void_p] * 13
         + [c_int32, c_int32, c_float, c_float, c_float, c_float, c_float, c_float, c_int32, c_float, c_int64,
            c_void_p, c_void_p],
     ),
