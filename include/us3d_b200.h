@@ -335,6 +335,61 @@ US3D_API int us3d_ugr_export_csr(const void* workspace, int64_t n_gauss, int32_t
                                  int64_t instance_capacity, int32_t* out_ray_counts, int32_t* out_ray_offsets,
                                  int32_t* out_ray_indices, float* out_sorted_depths, void* stream);
 
+/* ------------------------------------------------------------------------------------
+ * UltraGS baseline: 2D-Gaussian-surfel rasterisation with auxiliary maps.
+ *
+ * Inputs (device, fp32, contiguous): means3D (P,3); exactly one of shs (P,M,3) with
+ * sh_degree/sh_coeffs or colors_precomp (P,3); opacities (P); exactly one of scales (P,2)
+ * + rotations (P,4) (w,x,y,z) or transmat_precomp (P,9); viewmatrix, projmatrix (4,4) in
+ * the reference's row-vector layout; campos (3) (SH only); background (3). NULL stands for
+ * an absent optional input. Outputs: color (3,H,W), others (7,H,W: depth, alpha, normal x3,
+ * median depth, distortion) and radii (P). The workspace keeps the binning, the records and
+ * the per-pixel compositing state for the backward.
+ * ---------------------------------------------------------------------------------- */
+
+US3D_API size_t us3d_gs_workspace_bytes(int64_t n_gauss, int32_t width, int32_t height, int64_t instance_capacity);
+US3D_API size_t us3d_gs_backward_scratch_bytes(int64_t instance_capacity);
+
+/* Replaces RasterizeGaussiansCUDA
+ * (ops/ultrags_baseline_renderer/rasterize_points.cu:41-133). Never synchronises; an
+ * instance total above instance_capacity, or a Gaussian failing the near test while
+ * `prefiltered` is set (the reference traps the GPU there), sets a flag read by
+ * us3d_gs_read_status and leaves the outputs unwritten. */
+US3D_API int us3d_gs_forward(void* workspace, size_t workspace_bytes, int64_t n_gauss, int32_t sh_degree,
+                             int32_t sh_coeffs, const float* background, int32_t width, int32_t height,
+                             const float* means3D, const float* shs, const float* colors_precomp,
+                             const float* opacities, const float* scales, float scale_modifier,
+                             const float* rotations, const float* transmat_precomp, const float* viewmatrix,
+                             const float* projmatrix, const float* campos, int32_t prefiltered,
+                             int64_t instance_capacity, float* out_color, float* out_others, int32_t* out_radii,
+                             void* stream);
+/* Synchronises `stream`: instance total and flags (1 overflow, 2 table, 4 prefiltered). */
+US3D_API int us3d_gs_read_status(const void* workspace, int64_t* total_instances, int32_t* flags, void* stream);
+/* Replaces RasterizeGaussiansBackwardCUDA (rasterize_points.cu:135-233). Gradient outputs
+ * (every entry written): means2D (P,3), colors (P,3), opacity (P), means3D (P,3),
+ * transmat (P,9), sh (P,M,3) when shs is given, scales (P,2) and rotations (P,4) when
+ * given (may be NULL otherwise). Deterministic. */
+US3D_API int us3d_gs_backward(void* workspace, int64_t n_gauss, int32_t sh_degree, int32_t sh_coeffs,
+                              const float* background, int32_t width, int32_t height, const float* means3D,
+                              const float* shs, const float* colors_precomp, const float* scales,
+                              float scale_modifier, const float* rotations, const float* transmat_precomp,
+                              const float* viewmatrix, const float* projmatrix, const float* campos, float tan_fovx,
+                              float tan_fovy, const int32_t* radii, int64_t instance_capacity,
+                              const float* dL_dcolor, const float* dL_dothers, void* scratch, size_t scratch_bytes,
+                              float* d_means2D, float* d_colors, float* d_opacity, float* d_means3D,
+                              float* d_transmat, float* d_sh, float* d_scales, float* d_rotations, void* stream);
+/* The binning and compositing state in the reference's formats: point_list (instance
+ * total), keys (tile << 32 | depth bits; may be NULL), tile ranges (T,2; 0,0 for empty
+ * tiles), n_contrib (2,H,W), accum (3,H,W: final T, M1, M2) and the 80-byte records (P,20)
+ * (may be NULL). */
+US3D_API int us3d_gs_export(const void* workspace, int64_t n_gauss, int32_t width, int32_t height,
+                            int64_t instance_capacity, uint32_t* out_point_list, uint64_t* out_keys,
+                            uint32_t* out_ranges, uint32_t* out_n_contrib, float* out_accum, float* out_records,
+                            void* stream);
+/* Replaces markVisible (rasterize_points.cu:235-254): view-space depth > 0.2. */
+US3D_API int us3d_gs_mark_visible(int64_t n_gauss, const float* means3D, const float* viewmatrix,
+                                  uint8_t* out_present, void* stream);
+
 /*
  * UltraGauss forward render without any device allocation. No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc (an application that owns

@@ -1,11 +1,15 @@
-"""TEST INFRASTRUCTURE: compiles the reference's own UltraGauss CUDA extension, unmodified,
-from the reference tree for sm_100a, into ``oracle/_ref/`` (git-ignored; it travels to the
-GPU machine with the repository snapshot and is used only by tests as the parity checker).
+"""TEST INFRASTRUCTURE: compiles the reference's own renderer CUDA extensions, unmodified,
+from the reference tree for sm_100a, into ``oracle/_ref/`` (git-ignored; they travel to the
+GPU machine with the repository snapshot and are used only by tests as parity checkers).
 
-Recipe: nvcc on the reference's .cu files and g++ on its bindings.cpp, with the reference's
-own nvcc flags (ops/ultragauss_renderer/setup.py:29-41: -O3 --use_fast_math -lineinfo
--DTHRUST_IGNORE_CUB_VERSION_CHECK), plus ``oracle/ref_shim`` for the helper header that the
-reference tree does not contain. The reference's setup.py is not run.
+Recipe: nvcc on each renderer's .cu files and g++ on its bindings, with the reference's own
+nvcc flags (its setup.py files: -O3 --use_fast_math -lineinfo
+-DTHRUST_IGNORE_CUB_VERSION_CHECK; the UltraGS rasteriser adds its vendored GLM include
+directory and needs ``-include cstdint``), plus ``oracle/ref_shim`` for the helper headers
+the reference tree does not contain (math_utils.cuh, load_utils.cuh, and UltraGray's
+covariance.cuh, whose four functions are defined there from the mathematics their call
+sites imply). Two harnesses in ``oracle/ref_harness`` expose internal binning results.
+The reference's setup.py files are not run.
 
 Usage: python oracle/build_ref.py [--reference /path/to/reference]
 """
@@ -46,6 +50,13 @@ MODULES = {
          "src/shader/forward.cu", "src/shader/backward.cu"],
         ["-O3", "--use_fast_math", "-lineinfo", "-DTHRUST_IGNORE_CUB_VERSION_CHECK"],
     ),
+    "ultrags_ref_C": (
+        "ops/ultrags_baseline_renderer",
+        ["cuda_rasterizer/rasterizer_impl.cu", "cuda_rasterizer/forward.cu", "cuda_rasterizer/backward.cu",
+         "rasterize_points.cu", "ext.cpp"],
+        ["-O3", "--use_fast_math", "-lineinfo", "-DTHRUST_IGNORE_CUB_VERSION_CHECK", "-include", "cstdint",
+         "-I{root}/third_party/glm"],
+    ),
     "slice_adapted_ref_C": (
         "ops/slice_adapted_3dgs_renderer",
         ["src/bindings.cpp", "src/render.cu"],
@@ -81,6 +92,7 @@ def _torch_flags():
 def build_module(name: str, reference: Path, force: bool = False) -> Path:
     rdir, srcs, nvflags = MODULES[name]
     root = reference / rdir
+    nvflags = [f.replace("{root}", str(root)) for f in nvflags]
     suffix = sysconfig.get_config_var("EXT_SUFFIX")
     out = OUT_DIR / f"{name}{suffix}"
     if out.exists() and not force:
@@ -102,7 +114,8 @@ def build_module(name: str, reference: Path, force: bool = False) -> Path:
             cmd = ["nvcc", "-c", str(src), "-o", str(obj), *ARCH, *nvflags, "-std=c++17", "-Xcompiler", "-fPIC",
                    "--expt-relaxed-constexpr", *defs, *incs]
         else:
-            cmd = ["g++", "-c", str(src), "-o", str(obj), "-O3", "-std=c++17", "-fPIC", *defs, *incs]
+            cmd = ["g++", "-c", str(src), "-o", str(obj), "-O3", "-std=c++17", "-fPIC", "-include", "cstdint", *defs,
+                   *incs, *[f for f in nvflags if f.startswith("-I")]]
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
     link = ["g++", "-shared", "-o", str(out), *objs]

@@ -150,6 +150,24 @@ _SIGNATURES = {
     "us3d_ugr_export_csr": (
         c_int32, [c_void_p, c_int64, c_int32, c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
     ),
+    "us3d_gs_workspace_bytes": (c_size_t, [c_int64, c_int32, c_int32, c_int64]),
+    "us3d_gs_backward_scratch_bytes": (c_size_t, [c_int64]),
+    "us3d_gs_forward": (
+        c_int32,
+        [c_void_p, c_size_t, c_int64, c_int32, c_int32, c_void_p, c_int32, c_int32] + [c_void_p] * 5
+        + [c_float] + [c_void_p] * 5 + [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p],
+    ),
+    "us3d_gs_read_status": (c_int32, [c_void_p, POINTER(c_int64), POINTER(c_int32), c_void_p]),
+    "us3d_gs_backward": (
+        c_int32,
+        [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_int32, c_int32] + [c_void_p] * 4 + [c_float]
+        + [c_void_p] * 5 + [c_float, c_float, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_size_t]
+        + [c_void_p] * 9,
+    ),
+    "us3d_gs_export": (
+        c_int32, [c_void_p, c_int64, c_int32, c_int32, c_int64] + [c_void_p] * 7
+    ),
+    "us3d_gs_mark_visible": (c_int32, [c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "us3d_ug_render_noalloc": (
         c_int32,
         [c_void_p, c_int32, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
