@@ -18,6 +18,11 @@
  *                (MapperForwardCUDA  -> src/mapper/wrapper_mapper.cu:35-206,
  *                 ShaderForwardCUDA  -> src/shader/wrapper_shader.cu:17-66,
  *                 ShaderBackwardCUDA -> src/shader/wrapper_shader.cu:68-122)
+ *   UltraGray:   ops/ultragray_renderer/src/bindings.cpp:6-10
+ *                (MapperForwardCUDA, ShaderForwardCUDA, ShaderBackwardCUDA)
+ *   UltraGS baseline: ops/ultrags_baseline_renderer/ext.cpp:14-18
+ *                (rasterize_gaussians, rasterize_gaussians_backward, mark_visible)
+ *   slice-adapted adapter projection: baselines/slice_adapted_3dgs/render.py:66-98,132-163
  */
 #ifndef US3D_B200_H
 #define US3D_B200_H
@@ -283,6 +288,31 @@ US3D_API int us3d_sa_dense_backward(int64_t n_pixels, int64_t n, const float* pi
                                     const float* inv2d, const float* weights, const float* colors,
                                     const float* grad_image, const float* grad_alpha, float* d_means2d,
                                     float* d_inv2d, float* d_weights, float* d_colors, void* stream);
+
+/* Fused slice projection of 3D Gaussians for the bounded splat: replaces the PyTorch
+ * projection of the slice-adapted adapter (baselines/slice_adapted_3dgs/render.py:66-98,
+ * 132-163). Inputs: means (G,3), scales (G,3), quats (G,4) (w,x,y,z), opacities (G),
+ * colors (G,3), viewmatrix (4,4 row-major, points as row vectors). Writes the kept
+ * Gaussians, in index order, to the first n_kept rows of means2d (G,2), inv2d (G,2,2),
+ * weights (G), colors (G,3) and keep_idx (G); keep_mask (G, may be NULL) flags every
+ * Gaussian. If out_kept is not NULL, synchronises `stream` and returns the count there. */
+US3D_API size_t us3d_sa_project_workspace_bytes(int64_t n_gauss);
+US3D_API int us3d_sa_project(void* workspace, size_t workspace_bytes, int64_t n_gauss, const float* means,
+                             const float* scales, const float* quats, const float* opacities, const float* colors,
+                             const float* viewmatrix, float focal_depth, float slice_thickness, float cull_std,
+                             float thickness_scale, float min_covariance, int32_t normalize_by_footprint,
+                             float* out_means2d, float* out_inv2d, float* out_weights, float* out_colors,
+                             int32_t* out_keep_idx, uint8_t* out_keep_mask, int64_t* out_kept, void* stream);
+/* Vector-Jacobian product of us3d_sa_project: gradients of the kept rows in, gradients of
+ * means, scales, quats, opacities and colors (all G rows written; zero for culled) out. */
+US3D_API int us3d_sa_project_backward(int64_t n_gauss, int64_t n_kept, const int32_t* keep_idx, const float* means,
+                                      const float* scales, const float* quats, const float* opacities,
+                                      const float* viewmatrix, float focal_depth, float slice_thickness,
+                                      float cull_std, float thickness_scale, float min_covariance,
+                                      int32_t normalize_by_footprint, const float* d_means2d, const float* d_inv2d,
+                                      const float* d_weights, const float* d_colors_kept, float* d_means,
+                                      float* d_scales, float* d_quats, float* d_opacities, float* d_colors,
+                                      void* stream);
 
 /* ------------------------------------------------------------------------------------
  * UltraGray: scanline B-mode rendering by ray-Gaussian attenuation integrals.

@@ -132,6 +132,16 @@ _SIGNATURES = {
         [c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
          c_void_p, c_void_p, c_void_p],
     ),
+    "us3d_sa_project_workspace_bytes": (c_size_t, [c_int64]),
+    "us3d_sa_project": (
+        c_int32,
+        [c_void_p, c_size_t, c_int64] + [c_void_p] * 6 + [c_float] * 5 + [c_int32] + [c_void_p] * 6
+        + [POINTER(c_int64), c_void_p],
+    ),
+    "us3d_sa_project_backward": (
+        c_int32,
+        [c_int64, c_int64] + [c_void_p] * 6 + [c_float] * 5 + [c_int32] + [c_void_p] * 9 + [c_void_p],
+    ),
     "us3d_ugr_workspace_bytes": (c_size_t, [c_int64, c_int32, c_int32, c_int64]),
     "us3d_ugr_backward_scratch_bytes": (c_size_t, [c_int64]),
     "us3d_ugr_forward": (

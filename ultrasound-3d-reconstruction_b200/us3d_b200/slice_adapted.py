@@ -111,3 +111,56 @@ def dense_backward(pixels, means2d, inv2d, weights, colors, grad_image, grad_alp
                          weights.data_ptr(), colors.data_ptr(), gi.data_ptr(), ga.data_ptr(), dm.data_ptr(),
                          di.data_ptr(), dw.data_ptr(), dc.data_ptr(), _stream()), "us3d_sa_dense_backward")
     return dm, di, dw, dc
+
+
+@dataclass
+class ProjectionSettings:
+    focal_depth: float
+    slice_thickness: float
+    cull_std: float
+    thickness_scale: float
+    min_covariance: float
+    normalize_by_footprint: bool
+
+
+def project(means, scales, quats, opacities, colors, viewmatrix, s: ProjectionSettings):
+    """Fused slice projection. Returns (means2d (N,2), inv2d (N,2,2), weights (N,1),
+    colors (N,3), keep_idx (N,), keep_mask (G,)) for the N kept Gaussians, in index order."""
+    G = int(means.shape[0])
+    dev = means.device
+    _lib.check(_lib.call("us3d_set_device", dev.index if dev.index is not None else torch.cuda.current_device()),
+               "us3d_set_device")
+    nbytes = int(_lib.call("us3d_sa_project_workspace_bytes", G))
+    ws = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
+    m2 = torch.empty((G, 2), dtype=torch.float32, device=dev)
+    inv = torch.empty((G, 2, 2), dtype=torch.float32, device=dev)
+    w = torch.empty((G, 1), dtype=torch.float32, device=dev)
+    col = torch.empty((G, 3), dtype=torch.float32, device=dev)
+    idx = torch.empty((G,), dtype=torch.int32, device=dev)
+    mask = torch.zeros((G,), dtype=torch.uint8, device=dev)
+    kept = ctypes.c_int64(0)
+    _lib.check(_lib.call("us3d_sa_project", ws.data_ptr(), ws.numel(), G, means.data_ptr(), scales.data_ptr(),
+                         quats.data_ptr(), opacities.data_ptr(), colors.data_ptr(), viewmatrix.data_ptr(),
+                         float(s.focal_depth), float(s.slice_thickness), float(s.cull_std), float(s.thickness_scale),
+                         float(s.min_covariance), 1 if s.normalize_by_footprint else 0, m2.data_ptr(), inv.data_ptr(),
+                         w.data_ptr(), col.data_ptr(), idx.data_ptr(), mask.data_ptr(), ctypes.byref(kept),
+                         _stream()), "us3d_sa_project")
+    n = int(kept.value)
+    return m2[:n], inv[:n], w[:n], col[:n], idx[:n], mask.bool()
+
+
+def project_backward(keep_idx, means, scales, quats, opacities, viewmatrix, s: ProjectionSettings, d_means2d,
+                     d_inv2d, d_weights, d_colors_kept):
+    G, N = int(means.shape[0]), int(keep_idx.shape[0])
+    dev = means.device
+    z = lambda *sh: torch.empty(sh, dtype=torch.float32, device=dev)  # noqa: E731
+    dm, ds, dq, dop, dc = z(G, 3), z(G, 3), z(G, 4), z(G), z(G, 3)
+    c = lambda t: t.to(dtype=torch.float32).contiguous()  # noqa: E731
+    g = [c(d_means2d), c(d_inv2d), c(d_weights), c(d_colors_kept)]
+    _lib.check(_lib.call("us3d_sa_project_backward", G, N, keep_idx.data_ptr(), means.data_ptr(), scales.data_ptr(),
+                         quats.data_ptr(), opacities.data_ptr(), viewmatrix.data_ptr(), float(s.focal_depth),
+                         float(s.slice_thickness), float(s.cull_std), float(s.thickness_scale),
+                         float(s.min_covariance), 1 if s.normalize_by_footprint else 0, g[0].data_ptr(),
+                         g[1].data_ptr(), g[2].data_ptr(), g[3].data_ptr(), dm.data_ptr(), ds.data_ptr(),
+                         dq.data_ptr(), dop.data_ptr(), dc.data_ptr(), _stream()), "us3d_sa_project_backward")
+    return dm, ds, dq, dop, dc
