@@ -84,10 +84,12 @@ def test_slice_adapted_oracle_and_api(cuda_device):
     st = SO.render(H, W, float(fx["half_width"]), float(fx["half_height"]), fx["means2d"], fx["inv2d"],
                    fx["weights"], fx["colors"], float(fx["radius_sigma"]))
     np.testing.assert_array_equal(st["sorted_ids"], out["sorted_ids"])
-    assert rel_l2(out["image"], st["image"]) <= 1e-5
+    # the oracle evaluates e^power with IEEE expf, the GPU build (like the reference's) with
+    # the fast __expf: the same bounds as the oracle-vs-reference test on the CPU
+    assert rel_l2(out["image"], st["image"]) <= 3e-5
     g = SO.backward(st, fx["grad_image"], fx["grad_alpha"])
     for k in ("d_means", "d_inv", "d_weights", "d_colors"):
-        assert rel_l2(out[k], g[k]) <= 1e-4, k
+        assert rel_l2(out[k], g[k]) <= 5e-4, k
     dev = cuda_device
     ps = [torch.as_tensor(fx[k]).to(dev).requires_grad_(True) for k in ("means2d", "inv2d", "weights", "colors")]
     img, alpha = additive_splat_bounded(H, W, float(fx["half_width"]), float(fx["half_height"]), *ps,
