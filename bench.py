@@ -186,7 +186,7 @@ def run_b200(a):
 
     def batched_step(i):
         ft, pix, tgt = batches[i % len(batches)]
-        b = UG.bin_gaussians(*params, ft, 7.815, 1e-4, True)
+        b = UG.bin_gaussians(*params, ft, 7.815, 1e-4, True, slice_cull_pixels=pix)
         img, alpha, depth, _ = UG.forward(b, pix, 1e-6, 0.0, want_counts=False)
         dI = l1_grad(img, tgt)
         z = torch.zeros_like(img)

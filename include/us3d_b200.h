@@ -126,6 +126,27 @@ US3D_API int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_sli
                 const float* intensities, float chi2_threshold, float diag_beta,
                 int32_t sort_by_depth, int64_t instance_capacity, void* stream);
 
+/*
+ * us3d_ug_bin with options. flags = US3D_UG_BIN_SLICE_CULL keeps a (tile, Gaussian)
+ * instance only if the Gaussian's chi-square quadratic, restricted to the frame's pixel grid,
+ * can reach chi2_threshold inside the tile (exact test in double precision with margins for
+ * the pixels' distance from the grid, measured from pixel_positions (n_pixels,3), and for
+ * float rounding). Images, alpha, depth and gradients are identical to those of a full
+ * binning (the kept lists are order-preserving subsequences and the dropped instances have no
+ * contributing pixel); the per-pixel window-test counts, the candidate lists
+ * (us3d_ug_pixel_csr) and us3d_ug_export_bins describe the reference's full binning only,
+ * so after a culled binning us3d_ug_forward leaves out_counts unwritten and
+ * us3d_ug_pixel_csr writes nothing. No counterpart in the reference (its mapper always bins
+ * the full window rectangle).
+ */
+#define US3D_UG_BIN_SLICE_CULL 1
+US3D_API int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames_dev,
+                            int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
+                            const float* means, const float* precision_tril, const float* opacities,
+                            const float* intensities, float chi2_threshold, float diag_beta,
+                            int32_t sort_by_depth, int64_t instance_capacity, const float* pixel_positions,
+                            int32_t flags, void* stream);
+
 /* Copies the instance total and overflow flag of the last us3d_ug_bin to the host.
  * SYNCHRONISES `stream`. */
 US3D_API int us3d_ug_read_status(const void* workspace, int64_t* total_instances, int32_t* overflow,

@@ -282,3 +282,65 @@ def test_dropin_autograd_matches_lowlevel(cuda_device):
     assert np.array_equal(inter["pixel_gauss_offsets"].cpu().numpy(), low["offsets"])
     for p, k in ((means, "d_means"), (tril, "d_tril"), (op, "d_opacity"), (it, "d_intensity")):
         assert rel_l2(p.grad.cpu().numpy(), low[k]) <= 1e-6, k
+
+
+def _cull_case(dev, G=120000, sizes=((256, 256, 0.125), (200, 330, 0.2), (128, 96, 0.4)), jitter=0.0, seed=8,
+               scale_mm=1.0):
+    from us3d_b200 import scenes
+    from us3d_b200 import ultragauss as UG
+
+    sc = scenes.make_scene(G, seed=seed, log_scale_mean=float(np.log(scale_mm))).to(dev)
+    specs, pix, grads = [], [], []
+    g = torch.Generator().manual_seed(seed)
+    for i, (H, W, s) in enumerate(sizes):
+        fr = scenes.linear_sweep(len(sizes), H, W, s, seed=seed)[i]
+        specs.append(UG.SliceSpec(H, W, s, s, fr.axial_near, fr.lateral_col_offset, fr.origin, fr.axis_lat,
+                                  fr.axis_ax, fr.axis_ele))
+        p = fr.pixels.clone()
+        if jitter > 0:
+            p += jitter * torch.randn(p.shape, generator=g)
+        pix.append(p)
+        grads.append(torch.randn(3, H * W, generator=g))
+    args = (sc.means, sc.precision_tril.contiguous(), sc.opacities, sc.intensities)
+    return args, UG.build_frame_table(specs, dev), torch.cat(pix).to(dev), torch.cat(grads, dim=1).to(dev)
+
+
+@pytest.mark.parametrize("jitter,scale", [(0.0, 1.0), (0.0, 0.3), (2e-3, 1.0), (0.5, 1.0)])
+def test_slice_cull_identical_results(jitter, scale, cuda_device):
+    """A slice-culled binning keeps fewer instances but gives bit-identical images, alpha,
+    depth and gradients (pixels on the frame grid, slightly off it, and far off it)."""
+    from us3d_b200 import ultragauss as UG
+
+    args, ft, pix, gg = _cull_case(cuda_device, jitter=jitter, scale_mm=scale)
+    out = {}
+    for cull in (False, True):
+        b = UG.bin_gaussians(*args, ft, 7.815, 1e-4, True, slice_cull_pixels=pix if cull else None)
+        img, alp, dep, cnt = UG.forward(b, pix, 1e-6, 0.0)
+        assert (cnt is None) == cull
+        d = UG.backward(b, pix, gg[0].contiguous(), gg[1].contiguous(), gg[2].contiguous(), alp, 1e-6, 0.0)
+        out[cull] = (b.total, img, alp, dep) + tuple(d)
+    assert out[True][0] <= out[False][0]
+    if jitter < 0.1:
+        assert out[True][0] < 0.9 * out[False][0], (out[True][0], out[False][0])
+    for a, c in zip(out[False][1:], out[True][1:]):
+        assert torch.equal(a, c)
+
+
+def test_slice_cull_dropin_renderer(cuda_device):
+    from ultragauss_renderer import SliceGeometry, UltraGaussRenderConfig, UltraGaussRenderer
+    from us3d_b200 import scenes
+
+    dev = cuda_device
+    sc = scenes.make_scene(40000, seed=9).to(dev)
+    fr = scenes.linear_sweep(3, 160, 160, 0.25, seed=9)[1].to(dev)
+    cfg = UltraGaussRenderConfig(H=160, W=160, lateral_spacing_mm_per_pix=0.25, axial_spacing_mm_per_pix=0.25,
+                                 axial_near_mm=fr.axial_near, lateral_col_offset=fr.lateral_col_offset)
+    geo = SliceGeometry(fr.origin, fr.axis_lat, fr.axis_ax, fr.axis_ele)
+    res = []
+    for inter in (True, False):
+        ps = [x.clone().requires_grad_(True) for x in (sc.means, sc.precision_tril, sc.opacities, sc.intensities)]
+        img, alpha, depth, _ = UltraGaussRenderer(cfg)(*ps, fr.pixels, geo, return_intermediates=inter)
+        (img.square().sum() + alpha.sum() + depth.sum()).backward()
+        res.append([img.detach(), alpha.detach(), depth.detach()] + [p.grad for p in ps])
+    for a, c in zip(*res):
+        assert torch.equal(a, c)

@@ -45,7 +45,9 @@ struct Workspace {
     int* tile_start;         // T + 1
     int* tile_cursor;        // T
     long long* bs_t;         // scan block sums over T
-    int* tile_frame;         // T
+    int* tile_frame;
+    float* tile_dev;     // per tile: largest distance of a pixel from its frame's grid (slice cull)
+    unsigned* frame_dev; // at a frame's first tile: the largest deviation of its tiles (float bits)         // T
     unsigned long long* keys;  // cap: (depth_key << 32) | g, sorted in place per tile
     int* slot_inst;          // cap: instance index of each bucket slot (unsorted)
     int* sorted_gid;         // cap
@@ -67,6 +69,8 @@ static Workspace carve(void* base, int64_t G, int64_t T, int64_t P, int64_t cap)
     w.tile_cursor = c.take<int>((size_t)T);
     w.bs_t = c.take<long long>((size_t)scan_num_blocks(T) + 1);
     w.tile_frame = c.take<int>((size_t)T);
+    w.tile_dev = c.take<float>((size_t)T);
+    w.frame_dev = c.take<unsigned>((size_t)T);
     w.keys = c.take<unsigned long long>((size_t)cap);
     w.slot_inst = c.take<int>((size_t)cap);
     w.sorted_gid = c.take<int>((size_t)cap);
@@ -181,11 +185,12 @@ __device__ __forceinline__ bool frame_ok(const us3d_slice_frame* __restrict__ fr
 // Clears the per-tile counters, marks every tile as belonging to no frame and records the
 // sizes the workspace was carved with.
 __global__ void init_tiles_kernel(int64_t T, int* __restrict__ tile_count, int* __restrict__ tile_cursor,
-                                  int* __restrict__ tile_frame, long long* __restrict__ header, int64_t cap,
-                                  int64_t G, int64_t P) {
+                                  int* __restrict__ tile_frame, unsigned* __restrict__ frame_dev,
+                                  long long* __restrict__ header, int64_t cap, int64_t G, int64_t P, int mode) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (blockIdx.x == 0 && threadIdx.x < H_WORDS) {
         long long v = 0;
+        if (threadIdx.x == H_MODE) v = mode;
         if (threadIdx.x == H_CAP) v = cap;
         if (threadIdx.x == H_G) v = G;
         if (threadIdx.x == H_T) v = T;
@@ -196,6 +201,7 @@ __global__ void init_tiles_kernel(int64_t T, int* __restrict__ tile_count, int* 
     tile_count[t] = 0;
     tile_cursor[t] = 0;
     tile_frame[t] = -1;
+    frame_dev[t] = 0u;
 }
 
 // Assigns each frame's tiles to it and validates the frame table against the sizes.
@@ -225,10 +231,161 @@ __global__ void pack_kernel(int64_t G, const float* __restrict__ means, const fl
     pack[3 * g + 2] = make_float4(t45.x, t45.y, inten[g], 0.0f);
 }
 
+__device__ __forceinline__ void precision_from_raw(float t0, float t1, float t2, float t3, float t4,
+                                                   float t5, float beta, float4& q1, float& s12, float& s22);
+
+// ------------------------------------------------------------------------------------
+// Slice cull (optional): a tile keeps a Gaussian only if the Gaussian's chi-square quadratic
+// restricted to the frame's pixel grid can be <= chi2 somewhere in the tile. On the grid
+// P(x, y) = o + (x - col_offset) dlat lat + (near + y dax) ax the quadratic is a 2D convex
+// quadratic in pixel coordinates; its minimum over the tile's pixel-centre rectangle is
+// found exactly (in double precision) and compared with chi2 plus a margin that bounds the
+// distance of the real pixels from the grid (`tile_dev`) and the float rounding of the
+// per-pixel test. A pixel that passes the chi-square test therefore always finds the
+// Gaussian in its tile list, in the same relative order: images are unchanged and the
+// dropped instances would have contributed nothing. Only the window-test counts (and the
+// candidate lists built from them) change, so they are not produced after such a binning.
+// ------------------------------------------------------------------------------------
+
+struct SliceQuad {
+    double w0[3], A[3], B[3];  // d(x, y) = P(x, y) - m = w0 + x A + y B
+    double L[6];               // precision l00 l01 l02 l11 l12 l22
+    double h00, h01, h11, xc, yc, lam;
+    int ok;
+};
+
+__device__ __forceinline__ double lam_form_d(const double* L, double dx, double dy, double dz) {
+    return dx * (L[0] * dx + L[1] * dy + L[2] * dz) + dy * (L[1] * dx + L[3] * dy + L[4] * dz) +
+           dz * (L[2] * dx + L[4] * dy + L[5] * dz);
+}
+
+__device__ __forceinline__ double slice_q(const SliceQuad& S, double x, double y) {
+    return lam_form_d(S.L, S.w0[0] + x * S.A[0] + y * S.B[0], S.w0[1] + x * S.A[1] + y * S.B[1],
+                      S.w0[2] + x * S.A[2] + y * S.B[2]);
+}
+
+__device__ __forceinline__ void slice_setup(const float4 a, const float4 b, const float4 c, const Geo& F, float beta,
+                                            SliceQuad& S) {
+    float4 q1;
+    float s12, s22;
+    precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
+    S.L[0] = q1.x; S.L[1] = q1.y; S.L[2] = q1.z; S.L[3] = q1.w; S.L[4] = s12; S.L[5] = s22;
+    const double lat[3] = {F.lat.x, F.lat.y, F.lat.z}, ax[3] = {F.ax.x, F.ax.y, F.ax.z};
+    const double o[3] = {F.o.x, F.o.y, F.o.z}, m[3] = {a.x, a.y, a.z};
+    double LA[3], LB[3], LW[3];
+    for (int i = 0; i < 3; ++i) {
+        S.A[i] = (double)F.dlat * lat[i];
+        S.B[i] = (double)F.dax * ax[i];
+        S.w0[i] = (o[i] - m[i]) - (double)F.coloff * S.A[i] + (double)F.near * ax[i];
+    }
+    for (int i = 0; i < 3; ++i) {
+        const int r0 = i == 0 ? 0 : (i == 1 ? 1 : 2), r1 = i == 0 ? 1 : (i == 1 ? 3 : 4), r2 = i == 0 ? 2 : (i == 1 ? 4 : 5);
+        LA[i] = S.L[r0] * S.A[0] + S.L[r1] * S.A[1] + S.L[r2] * S.A[2];
+        LB[i] = S.L[r0] * S.B[0] + S.L[r1] * S.B[1] + S.L[r2] * S.B[2];
+        LW[i] = S.L[r0] * S.w0[0] + S.L[r1] * S.w0[1] + S.L[r2] * S.w0[2];
+    }
+    S.h00 = S.A[0] * LA[0] + S.A[1] * LA[1] + S.A[2] * LA[2];
+    S.h01 = S.A[0] * LB[0] + S.A[1] * LB[1] + S.A[2] * LB[2];
+    S.h11 = S.B[0] * LB[0] + S.B[1] * LB[1] + S.B[2] * LB[2];
+    const double g0 = S.A[0] * LW[0] + S.A[1] * LW[1] + S.A[2] * LW[2];
+    const double g1 = S.B[0] * LW[0] + S.B[1] * LW[1] + S.B[2] * LW[2];
+    const double det = S.h00 * S.h11 - S.h01 * S.h01;
+    S.lam = S.L[0] + S.L[3] + S.L[5];
+    S.ok = S.h00 > 0.0 && S.h11 > 0.0 && det > 1e-12 * S.h00 * S.h11 && S.lam < 1e30;
+    S.xc = S.ok ? (-g0 * S.h11 + g1 * S.h01) / det : 0.0;
+    S.yc = S.ok ? (-g1 * S.h00 + g0 * S.h01) / det : 0.0;
+}
+
+// The region {q <= chi2 + tau} of one Gaussian on one frame's pixel grid: an ellipse
+// (x - xc, y - yc) H (x - xc, y - yc)^T <= rho. tau bounds the pixels' distance from the grid
+// (the frame's largest tile deviation `dev`) and the float rounding of the per-pixel test
+// over the reference rectangle `r` (tiles). Returns false when no pixel can pass.
+struct SliceEllipse {
+    double xc, yc, h00, h01, h11, det, rho;
+    int ok;  // 0: degenerate quadratic, keep every tile of the rectangle
+};
+
+__device__ __forceinline__ bool slice_ellipse(const SliceQuad& S, const int4 r, const Geo& F, float chi2, float dev,
+                                              SliceEllipse& E) {
+    E.ok = S.ok;
+    if (!S.ok) return true;
+    E.xc = S.xc; E.yc = S.yc; E.h00 = S.h00; E.h01 = S.h01; E.h11 = S.h11;
+    E.det = S.h00 * S.h11 - S.h01 * S.h01;
+    const double qc = slice_q(S, S.xc, S.yc);
+    const double x0 = r.x * TILE, x1 = min(r.z * TILE - 1, F.W - 1), y0 = r.y * TILE, y1 = min(r.w * TILE - 1, F.H - 1);
+    double dmax2 = 0.0;
+    for (int k = 0; k < 4; ++k) {
+        const double xx = (k & 1) ? x1 : x0, yy = (k & 2) ? y1 : y0;
+        const double dx = S.w0[0] + xx * S.A[0] + yy * S.B[0], dy = S.w0[1] + xx * S.A[1] + yy * S.B[1],
+                     dz = S.w0[2] + xx * S.A[2] + yy * S.B[2];
+        dmax2 = fmax(dmax2, dx * dx + dy * dy + dz * dz);
+    }
+    const double dv = (double)dev;
+    const double dm = sqrt(dmax2) + dv;
+    const double tau = 2.0 * sqrt(((double)chi2 + 1.0) * S.lam) * dv + S.lam * dv * dv + 1.2e-5 * S.lam * dm * dm + 1e-6;
+    E.rho = (double)chi2 + tau - qc;
+    return E.rho >= 0.0;
+}
+
+// Pixel-centre x-range [xl, xr] of the ellipse inside the tile row y in [y0, y1] (exact:
+// the ellipse's x-extent over a horizontal band); false if the band misses the ellipse.
+__device__ __forceinline__ bool ellipse_row_range(const SliceEllipse& E, double y0, double y1, double& xl,
+                                                  double& xr) {
+    const double ymax = sqrt(E.rho * E.h00 / E.det);
+    const double a = fmax(y0 - E.yc, -ymax), b = fmin(y1 - E.yc, ymax);
+    if (a > b) return false;
+    const double s1 = E.h01 / E.h00, kk = E.det / E.h00;
+    const double dys = -E.h01 * sqrt(E.rho / (E.h11 * E.det));  // dy of the rightmost point
+    const double dr = fmin(fmax(dys, a), b), dl = fmin(fmax(-dys, a), b);
+    xr = E.xc - s1 * dr + sqrt(fmax(0.0, (E.rho - kk * dr * dr) / E.h00));
+    xl = E.xc - s1 * dl - sqrt(fmax(0.0, (E.rho - kk * dl * dl) / E.h00));
+    const double slack = 1e-6 * (fabs(xl) + fabs(xr) + 1.0);
+    xl -= slack;
+    xr += slack;
+    return true;
+}
+
+// Largest distance of a tile's pixels from its frame's grid (double precision grid).
+__global__ void __launch_bounds__(TILE_PIX)
+tile_dev_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
+                const float* __restrict__ pixels, float* __restrict__ tile_dev, unsigned* __restrict__ frame_dev) {
+    __shared__ unsigned s_max;
+    const int64_t t = blockIdx.x;
+    if (t >= T) return;
+    if (tile_frame[t] < 0) {
+        if (threadIdx.x == 0) tile_dev[t] = 0.f;
+        return;
+    }
+    const Geo F = load_geo(frames + tile_frame[t]);
+    const int lt = (int)(t - F.tile_off);
+    const int tx = lt % F.tx, ty = lt / F.tx;
+    const int x = tx * TILE + (threadIdx.x & (TILE - 1)), y = ty * TILE + threadIdx.x / TILE;
+    if (threadIdx.x == 0) s_max = 0u;
+    __syncthreads();
+    if (x < F.W && y < F.H) {
+        const int64_t p = (int64_t)F.pix_off + (int64_t)y * F.W + x;
+        float e = 1e30f;
+        if (p < P) {
+            const double s = ((double)x - (double)F.coloff) * (double)F.dlat, u = (double)F.near + (double)y * (double)F.dax;
+            const double gx = (double)F.o.x + s * F.lat.x + u * F.ax.x, gy = (double)F.o.y + s * F.lat.y + u * F.ax.y,
+                         gz = (double)F.o.z + s * F.lat.z + u * F.ax.z;
+            const double ex = pixels[3 * p] - gx, ey = pixels[3 * p + 1] - gy, ez = pixels[3 * p + 2] - gz;
+            const double d = sqrt(ex * ex + ey * ey + ez * ez);
+            e = (d <= 1e30) ? (float)(d * 1.0001 + 1e-9) : 1e30f;
+        }
+        atomicMax(&s_max, __float_as_uint(e));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tile_dev[t] = __uint_as_float(s_max);
+        atomicMax(frame_dev + F.tile_off, s_max);
+    }
+}
+
 __global__ void __launch_bounds__(256)
 count_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, int F,
-             const float4* __restrict__ pack, float chi2, float beta, int* __restrict__ touched,
-             int* __restrict__ tile_count) {
+             const float4* __restrict__ pack, float chi2, float beta, const unsigned* __restrict__ frame_dev,
+             int* __restrict__ touched, int* __restrict__ tile_count) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
     const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
@@ -239,11 +396,38 @@ count_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict
         int4 r;
         float v_pix;
         if (!project_rect(a, b, c, geo, chi2, beta, r, v_pix)) continue;
-        total += (r.z - r.x) * (r.w - r.y);
-        for (int y = r.y; y < r.w; ++y)
-            for (int x = r.x; x < r.z; ++x) atomicAdd(&tile_count[geo.tile_off + y * geo.tx + x], 1);
+        SliceEllipse E;
+        E.ok = 0;
+        if (frame_dev) {
+            SliceQuad S;
+            slice_setup(a, b, c, geo, beta, S);
+            if (!slice_ellipse(S, r, geo, chi2, __uint_as_float(frame_dev[geo.tile_off]), E)) continue;
+        }
+        for (int y = r.y; y < r.w; ++y) {
+            int xa = r.x, xb = r.z;
+            if (E.ok) {
+                double xl, xr;
+                if (!ellipse_row_range(E, y * TILE, min(y * TILE + TILE - 1, geo.H - 1), xl, xr)) continue;
+                if (!(xl <= xr)) continue;  // NaN guard
+                xa = max(xa, (int)floor(fmax(xl, -1e9) / TILE));
+                xb = min(xb, (int)floor(fmin(xr, 1e9) / TILE) + 1);
+            }
+            for (int x = xa; x < xb; ++x) {
+                ++total;
+                atomicAdd(&tile_count[geo.tile_off + y * geo.tx + x], 1);
+            }
+        }
     }
     touched[g] = total;
+}
+
+// Every bucket must have been filled exactly as counted; otherwise later kernels see a flag.
+__global__ void verify_kernel(int64_t T, const int* __restrict__ tile_count, const int* __restrict__ tile_cursor,
+                              long long* __restrict__ header) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T || header[H_FLAGS] != 0) return;
+    if (tile_cursor[t] != tile_count[t])
+        atomicOr(reinterpret_cast<unsigned long long*>(header + H_FLAGS), (unsigned long long)FLAG_TABLE);
 }
 
 __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
@@ -258,6 +442,7 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
 __global__ void __launch_bounds__(256)
 scatter_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, int F,
                const float4* __restrict__ pack, float chi2, float beta, int sort_by_depth,
+               const unsigned* __restrict__ frame_dev,
                const int* __restrict__ inst_offset, const int* __restrict__ tile_start,
                int* __restrict__ tile_cursor, const long long* __restrict__ header,
                unsigned long long* __restrict__ keys, int* __restrict__ slot_inst) {
@@ -273,10 +458,26 @@ scatter_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restri
         if (!project_rect(a, b, c, geo, chi2, beta, r, v_pix)) continue;
         const unsigned long long key =
             ((unsigned long long)depth_key(v_pix, sort_by_depth) << 32) | (unsigned long long)(uint32_t)g;
+        SliceEllipse E;
+        E.ok = 0;
+        if (frame_dev) {
+            SliceQuad S;
+            slice_setup(a, b, c, geo, beta, S);
+            if (!slice_ellipse(S, r, geo, chi2, __uint_as_float(frame_dev[geo.tile_off]), E)) continue;
+        }
         for (int y = r.y; y < r.w; ++y) {
-            for (int x = r.x; x < r.z; ++x) {
+            int xa = r.x, xb = r.z;
+            if (E.ok) {
+                double xl, xr;
+                if (!ellipse_row_range(E, y * TILE, min(y * TILE + TILE - 1, geo.H - 1), xl, xr)) continue;
+                if (!(xl <= xr)) continue;  // NaN guard
+                xa = max(xa, (int)floor(fmax(xl, -1e9) / TILE));
+                xb = min(xb, (int)floor(fmin(xr, 1e9) / TILE) + 1);
+            }
+            for (int x = xa; x < xb; ++x) {
                 const int t = geo.tile_off + y * geo.tx + x;
                 const int slot = tile_start[t] + atomicAdd(&tile_cursor[t], 1);
+                if (slot >= tile_start[t + 1]) continue;  // never outside the bucket (verify_kernel flags it)
                 keys[slot] = key;
                 slot_inst[slot] = inst++;
             }
@@ -411,7 +612,7 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     out_alpha[p] = alpha_total;
     out_image[p] = fmaxf(0.0f, fminf(1.0f, img));
     out_depth[p] = sd / fmaxf(sa, 1e-8f);
-    if (out_counts) out_counts[p] = cnt;
+    if (out_counts && header[H_MODE] == 0) out_counts[p] = cnt;
     pixel_aux[p] = make_float2(sc_ns, sd_ns);
 }
 
@@ -559,7 +760,8 @@ pixel_csr_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ fram
     __shared__ float4 s_m[FWD_BATCH];   // mean, gaussian index (as float bits)
     __shared__ float2 s_r[FWD_BATCH];   // r_lat, r_ax
     const int64_t t = blockIdx.x;
-    if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
+    // candidate lists exist only for a full (reference) binning
+    if (t >= T || header[H_FLAGS] != 0 || header[H_MODE] != 0 || tile_frame[t] < 0) return;
     const Geo geo = load_geo(frames + tile_frame[t]);
     int tx, ty;
     find_tile_coords(geo, t, tx, ty);
@@ -665,11 +867,15 @@ static int read_header(const void* workspace, long long hdr[H_WORDS], cudaStream
     return US3D_OK;
 }
 
-extern "C" int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames,
-                           int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
-                           const float* means, const float* tril, const float* opac, const float* inten,
-                           float chi2, float beta, int32_t sort_by_depth, int64_t cap, void* stream_) {
+extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames,
+                              int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
+                              const float* means, const float* tril, const float* opac, const float* inten,
+                              float chi2, float beta, int32_t sort_by_depth, int64_t cap, const float* pixels,
+                              int32_t flags, void* stream_) {
     int st = check_common(frames, n_frames, n_tiles, n_pixels, n_gauss);
+    const int slice_cull = (flags & US3D_UG_BIN_SLICE_CULL) ? 1 : 0;
+    US3D_CHECK_ARG((flags & ~US3D_UG_BIN_SLICE_CULL) == 0, "unknown binning flags 0x%x", (unsigned)flags);
+    US3D_CHECK_ARG(!slice_cull || n_pixels == 0 || pixels != nullptr, "slice cull needs the pixel positions");
     if (st != US3D_OK) return st;
     US3D_CHECK_ARG(workspace != nullptr, "workspace is NULL");
     US3D_CHECK_ARG(cap >= 0 && cap <= 0x7fffffffLL, "instance capacity must be in [0, 2^31)");
@@ -682,15 +888,19 @@ extern "C" int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_s
 
     const int prof = prof_begin("ug_bin", stream);
     init_tiles_kernel<<<(unsigned)((n_tiles + 255) / 256 > 0 ? (n_tiles + 255) / 256 : 1), 256, 0, stream>>>(
-        n_tiles, w.tile_count, w.tile_cursor, w.tile_frame, w.header, cap, n_gauss, n_pixels);
+        n_tiles, w.tile_count, w.tile_cursor, w.tile_frame, w.frame_dev, w.header, cap, n_gauss, n_pixels, slice_cull);
     if (n_frames > 0)
         setup_kernel<<<n_frames, 256, 0, stream>>>(frames, n_frames, n_tiles, n_pixels, w.tile_frame, w.header);
     US3D_CHECK_LAUNCH("ug setup");
+    if (slice_cull && n_tiles > 0)
+        tile_dev_kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(n_tiles, n_pixels, frames, w.tile_frame, pixels,
+                                                                    w.tile_dev, w.frame_dev);
+    const unsigned* tdev = slice_cull ? w.frame_dev : nullptr;
     const int gb = (int)((n_gauss + 255) / 256);
     if (n_gauss > 0) {
         pack_kernel<<<gb, 256, 0, stream>>>(n_gauss, means, tril, opac, inten, w.pack);
-        count_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, w.touched,
-                                             w.tile_count);
+        count_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, tdev,
+                                             w.touched, w.tile_count);
         US3D_CHECK_LAUNCH("ug count");
     }
     US3D_CHECK_CUDA(exclusive_scan(w.touched, n_gauss, w.inst_offset, w.bs_g, w.header + H_SCAN_G, stream));
@@ -698,10 +908,13 @@ extern "C" int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_s
     check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
     if (n_gauss > 0) {
         scatter_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, sort_by_depth,
-                                               w.inst_offset, w.tile_start, w.tile_cursor, w.header, w.keys,
+                                               tdev, w.inst_offset, w.tile_start, w.tile_cursor, w.header, w.keys,
                                                w.slot_inst);
         US3D_CHECK_LAUNCH("ug scatter");
     }
+    if (n_tiles > 0)
+        verify_kernel<<<(unsigned)((n_tiles + 255) / 256), 256, 0, stream>>>(n_tiles, w.tile_count, w.tile_cursor,
+                                                                              w.header);
     if (n_tiles > 0) {
         st = ensure_sort_attr();
         if (st != US3D_OK) return st;
@@ -711,8 +924,17 @@ extern "C" int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_s
         US3D_CHECK_LAUNCH("ug tile sort");
     }
     prof_end(prof, stream);
-    count_launches(1 + (n_frames > 0) + 2 * (n_gauss > 0) + 6 + 1 + (n_gauss > 0) + (n_tiles > 0));
+    count_launches(1 + (n_frames > 0) + (slice_cull && n_tiles > 0) + 2 * (n_gauss > 0) + 6 + 1 + (n_gauss > 0) +
+                   2 * (n_tiles > 0));
     return US3D_OK;
+}
+
+extern "C" int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames,
+                           int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
+                           const float* means, const float* tril, const float* opac, const float* inten,
+                           float chi2, float beta, int32_t sort_by_depth, int64_t cap, void* stream) {
+    return us3d_ug_bin_ex(workspace, workspace_bytes, frames, n_frames, n_tiles, n_pixels, n_gauss, means, tril, opac,
+                          inten, chi2, beta, sort_by_depth, cap, nullptr, 0, stream);
 }
 
 extern "C" int us3d_ug_read_status(const void* workspace, int64_t* total, int32_t* overflow, void* stream_) {

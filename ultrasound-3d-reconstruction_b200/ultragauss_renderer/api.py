@@ -28,7 +28,7 @@ class UltraGaussRenderer(nn.Module):
         geometry: SliceGeometry,
         return_intermediates: bool = False,
     ) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor, Dict[str, torch.Tensor]]:
-        holder = {}
+        holder = {"want_counts": bool(return_intermediates)}
         image, alpha, depth, counts = _RenderFunction.apply(
             self.config,
             gauss_means_world,

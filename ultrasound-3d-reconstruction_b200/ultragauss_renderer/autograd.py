@@ -75,10 +75,16 @@ class _RenderFunction(torch.autograd.Function):
         if n_pixels != 0 and n_pixels != H * W:
             raise RuntimeError("n_pixels must equal H*W")
         frames = _ug.build_frame_table([_spec(config, origin, lat, ax, ele)] if n_pixels else [], pixels.device)
+        # Without a request for intermediates the tiles are culled to the Gaussians' in-slice
+        # chi-square ellipses (identical image and gradients, no candidate counts).
+        cull = holder is not None and not holder.get("want_counts", True) and n_pixels > 0
         b = _ug.bin_gaussians(means, tril, opac, inten, frames, float(config.chi2_threshold),
-                              float(config.diag_beta), bool(config.mapper_sort_by_depth))
+                              float(config.diag_beta), bool(config.mapper_sort_by_depth),
+                              slice_cull_pixels=pixels if cull else None)
         image, alpha, depth, counts = _ug.forward(b, pixels, float(config.fixed_bg_alpha),
                                                   float(config.fixed_bg_intensity))
+        if counts is None:
+            counts = torch.zeros(0, dtype=torch.int32, device=pixels.device)
         ctx.save_for_backward(pixels, alpha)
         ctx.binning = b
         ctx.config = config

@@ -66,6 +66,11 @@ _SIGNATURES = {
         [c_void_p, c_size_t, c_void_p, c_int32, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p,
          c_void_p, c_float, c_float, c_int32, c_int64, c_void_p],
     ),
+    "us3d_ug_bin_ex": (
+        c_int32,
+        [c_void_p, c_size_t, c_void_p, c_int32, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p,
+         c_void_p, c_float, c_float, c_int32, c_int64, c_void_p, c_int32, c_void_p],
+    ),
     "us3d_ug_read_status": (c_int32, [c_void_p, POINTER(c_int64), POINTER(c_int32), c_void_p]),
     "us3d_ug_forward": (
         c_int32,

@@ -19,8 +19,11 @@ from . import ultragauss as UG
 class _BatchFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, frames: UG.FrameTable, params: dict, means, tril, opac, inten, pixels, holder):
+        want_counts = params.get("want_counts", False)
+        cull = params.get("slice_cull", True) and not want_counts
         b = UG.bin_gaussians(means, tril, opac, inten, frames, params["chi2"], params["beta"], params["sort_by_depth"],
-                             capacity=params.get("capacity"), sync_check=params.get("sync_check", True))
+                             capacity=params.get("capacity"), sync_check=params.get("sync_check", True),
+                             slice_cull_pixels=pixels if cull else None)
         image, alpha, depth, counts = UG.forward(b, pixels, params["bg_alpha"], params["bg_intensity"],
                                                  want_counts=params.get("want_counts", False))
         ctx.b = b
@@ -43,10 +46,11 @@ class _BatchFunction(torch.autograd.Function):
 class UltraGaussBatchRenderer:
     def __init__(self, frames: Sequence[UG.SliceSpec], device: torch.device, chi2_threshold: float = 7.815,
                  diag_beta: float = 1e-4, mapper_sort_by_depth: bool = True, fixed_bg_alpha: float = 1e-6,
-                 fixed_bg_intensity: float = 0.0, capacity: Optional[int] = None):
+                 fixed_bg_intensity: float = 0.0, capacity: Optional[int] = None, slice_cull: bool = True):
         self.frames = UG.build_frame_table(list(frames), device)
         self.params = dict(chi2=float(chi2_threshold), beta=float(diag_beta), sort_by_depth=bool(mapper_sort_by_depth),
-                           bg_alpha=float(fixed_bg_alpha), bg_intensity=float(fixed_bg_intensity), capacity=capacity)
+                           bg_alpha=float(fixed_bg_alpha), bg_intensity=float(fixed_bg_intensity), capacity=capacity,
+                           slice_cull=bool(slice_cull))
         self.last = {}
 
     @property

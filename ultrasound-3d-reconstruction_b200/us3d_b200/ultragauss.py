@@ -106,6 +106,7 @@ class UGBinning:
     chi2: float
     beta: float
     sort_by_depth: bool
+    slice_cull: bool = False
     pixels: Optional[torch.Tensor] = None
     counts: Optional[torch.Tensor] = None
     alpha: Optional[torch.Tensor] = field(default=None, repr=False)
@@ -123,24 +124,29 @@ def _check_params(means, tril, opac, inten):
 
 def bin_gaussians(means: torch.Tensor, tril: torch.Tensor, opac: torch.Tensor, inten: torch.Tensor,
                   frames: FrameTable, chi2: float, beta: float, sort_by_depth: bool = True,
-                  capacity: Optional[int] = None, sync_check: bool = True) -> UGBinning:
+                  capacity: Optional[int] = None, sync_check: bool = True,
+                  slice_cull_pixels: Optional[torch.Tensor] = None) -> UGBinning:
     """Runs the mapper for all frames. With ``sync_check`` the instance total is read back
-    (one stream synchronisation) and the binning is redone with a larger capacity if needed."""
+    (one stream synchronisation) and the binning is redone with a larger capacity if needed.
+    Passing the frames' pixel positions as ``slice_cull_pixels`` drops the tiles a Gaussian's
+    chi-square ellipse cannot reach (same images and gradients; no per-pixel candidate counts
+    or lists afterwards)."""
     G = _check_params(means, tril, opac, inten)
     dev = means.device
     _set_device(dev)
-    key = (G, frames.n_tiles)
+    cull = slice_cull_pixels is not None
+    key = (G, frames.n_tiles, cull)
     cap = int(capacity if capacity is not None else _capacity_hint.get(key, max(4096, 4 * G)))
     for _attempt in range(3):
         nbytes = _lib.call("us3d_ug_workspace_bytes", G, frames.n_frames, frames.n_tiles, frames.n_pixels, cap)
         ws = torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
         st = _lib.call(
-            "us3d_ug_bin", _ptr(ws), int(nbytes), _ptr(frames.table), frames.n_frames, frames.n_tiles,
+            "us3d_ug_bin_ex", _ptr(ws), int(nbytes), _ptr(frames.table), frames.n_frames, frames.n_tiles,
             frames.n_pixels, G, _ptr(means), _ptr(tril), _ptr(opac), _ptr(inten), float(chi2), float(beta),
-            int(bool(sort_by_depth)), cap, _stream(),
+            int(bool(sort_by_depth)), cap, _ptr(slice_cull_pixels) if cull else None, 1 if cull else 0, _stream(),
         )
-        _lib.check(st, "us3d_ug_bin")
-        b = UGBinning(ws, cap, -1, frames, G, float(chi2), float(beta), bool(sort_by_depth))
+        _lib.check(st, "us3d_ug_bin_ex")
+        b = UGBinning(ws, cap, -1, frames, G, float(chi2), float(beta), bool(sort_by_depth), cull)
         if not sync_check:
             return b
         total, flags = read_status(b)
@@ -172,7 +178,8 @@ def forward(b: UGBinning, pixels: torch.Tensor, bg_alpha: float, bg_intensity: f
     image = torch.empty(P, dtype=torch.float32, device=dev)
     alpha = torch.empty(P, dtype=torch.float32, device=dev)
     depth = torch.empty(P, dtype=torch.float32, device=dev)
-    counts = torch.empty(P, dtype=torch.int32, device=dev) if want_counts else None
+    # a slice-culled binning has no per-pixel candidate counts
+    counts = torch.empty(P, dtype=torch.int32, device=dev) if (want_counts and not b.slice_cull) else None
     st = _lib.call(
         "us3d_ug_forward", _ptr(b.workspace), _ptr(b.frames.table), b.frames.n_frames, b.frames.n_tiles, P,
         b.n_gauss, b.capacity, _ptr(pixels), b.chi2, b.beta, float(bg_alpha), float(bg_intensity), _ptr(image),
