@@ -12,7 +12,7 @@ constexpr int SORT_THREADS = 512;
 constexpr int SORT_SMEM_CAP = 8192;  // keys sorted in shared memory per tile (96 KB)
 
 // Header words at the start of a binned workspace.
-enum { H_TOTAL = 0, H_FLAGS = 1, H_SCAN_G = 2, H_SCAN_T = 3, H_CAP = 4, H_G = 5, H_T = 6, H_P = 7, H_MODE = 8, H_WORDS = 16 };
+enum { H_TOTAL = 0, H_FLAGS = 1, H_SCAN_G = 2, H_SCAN_T = 3, H_CAP = 4, H_G = 5, H_T = 6, H_P = 7, H_MODE = 8, H_NTASK = 9, H_WORDS = 16 };
 enum { FLAG_OVERFLOW = 1, FLAG_TABLE = 2 };
 
 static __device__ __forceinline__ void cswap(unsigned long long* k, int* v, int a, int b) {

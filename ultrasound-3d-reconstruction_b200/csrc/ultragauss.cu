@@ -22,6 +22,8 @@
 // keys, the window test) is written with the same operations in the same order as the
 // reference so that, compiled with the same fast-math flags, keys, ranges and candidate
 // counts agree bit for bit.
+#include <algorithm>
+
 #include "us3d_common.cuh"
 #include "scan.cuh"
 #include "binning.cuh"
@@ -38,9 +40,16 @@ constexpr int FWD_BATCH = 256;       // Gaussians staged per shared-memory batch
 struct Workspace {
     long long* header;
     float4* pack;            // G x 3 float4: (m.xyz, o) (t0..t3) (t4, t5, c, 0)
-    int* touched;            // G
-    int* inst_offset;        // G + 1
+    int* gtasks;             // G: frames in which the Gaussian survives the cull (tasks)
+    int* task_offset;        // G + 1: exclusive scan of gtasks
     long long* bs_g;         // scan block sums over G
+    int* inst_offset;        // G + 1: first instance of each Gaussian
+    int4* task_rect;         // TC: (g, f) task's tile rectangle
+    int2* task_gf;           // TC: Gaussian, frame
+    float* task_v;           // TC: axial pixel coordinate (depth key source)
+    int* task_ntiles;        // TC: instances of the task
+    int* task_inst;          // TC + 1: exclusive scan of task_ntiles
+    long long* bs_k;         // scan block sums over TC
     int* tile_count;         // T
     int* tile_start;         // T + 1
     int* tile_cursor;        // T
@@ -56,14 +65,27 @@ struct Workspace {
     size_t bytes;
 };
 
+// (Gaussian, frame) tasks: every task yields at least one instance in a full binning, and
+// a culled binning keeps about a tenth as many tasks as instances; an overflow is flagged
+// with a total that makes the retried capacity large enough.
+static inline int64_t task_capacity(int64_t cap) { return cap / 4 + 4096; }
+
 static Workspace carve(void* base, int64_t G, int64_t T, int64_t P, int64_t cap) {
     Carver c(base);
     Workspace w;
     w.header = c.take<long long>(H_WORDS);
     w.pack = c.take<float4>((size_t)G * 3);
-    w.touched = c.take<int>((size_t)G);
-    w.inst_offset = c.take<int>((size_t)G + 1);
+    w.gtasks = c.take<int>((size_t)G);
+    w.task_offset = c.take<int>((size_t)G + 1);
     w.bs_g = c.take<long long>((size_t)scan_num_blocks(G) + 1);
+    w.inst_offset = c.take<int>((size_t)G + 1);
+    const int64_t tc = task_capacity(cap);
+    w.task_rect = c.take<int4>((size_t)tc);
+    w.task_gf = c.take<int2>((size_t)tc);
+    w.task_v = c.take<float>((size_t)tc);
+    w.task_ntiles = c.take<int>((size_t)tc);
+    w.task_inst = c.take<int>((size_t)tc + 1);
+    w.bs_k = c.take<long long>((size_t)scan_num_blocks(tc) + 1);
     w.tile_count = c.take<int>((size_t)T);
     w.tile_start = c.take<int>((size_t)T + 1);
     w.tile_cursor = c.take<int>((size_t)T);
@@ -382,43 +404,123 @@ tile_dev_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
     }
 }
 
+// Binning in three steps that keep every thread busy: (1) per Gaussian, the reference's
+// elevational cull and tile rectangle in each frame -> surviving (Gaussian, frame) tasks,
+// written in (g, f) order; (2) per task, the tiles of its rectangle (optionally only those
+// its in-slice ellipse reaches) are counted; (3) per task, the same tiles receive the
+// instance's key. Instance ids are the exclusive scan of the tasks' tile counts in (g, f)
+// order, hence Gaussian-major and deterministic.
+
 __global__ void __launch_bounds__(256)
-count_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, int F,
-             const float4* __restrict__ pack, float chi2, float beta, const unsigned* __restrict__ frame_dev,
-             int* __restrict__ touched, int* __restrict__ tile_count) {
+cull_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, int F,
+            const float4* __restrict__ pack, float chi2, float beta, const int* __restrict__ task_offset,
+            int64_t cap, int* __restrict__ gtasks, int4* __restrict__ task_rect, int2* __restrict__ task_gf,
+            float* __restrict__ task_v) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
     const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
-    int total = 0;
+    int k = task_offset ? task_offset[g] : 0;
+    int n = 0;
     for (int f = 0; f < F; ++f) {
         if (!frame_ok(frames + f, T, P)) continue;
         const Geo geo = load_geo(frames + f);
         int4 r;
         float v_pix;
         if (!project_rect(a, b, c, geo, chi2, beta, r, v_pix)) continue;
-        SliceEllipse E;
-        E.ok = 0;
-        if (frame_dev) {
-            SliceQuad S;
-            slice_setup(a, b, c, geo, beta, S);
-            if (!slice_ellipse(S, r, geo, chi2, __uint_as_float(frame_dev[geo.tile_off]), E)) continue;
+        ++n;
+        if (task_offset && k < cap) {
+            task_rect[k] = r;
+            task_gf[k] = make_int2((int)g, f);
+            task_v[k] = v_pix;
         }
-        for (int y = r.y; y < r.w; ++y) {
-            int xa = r.x, xb = r.z;
-            if (E.ok) {
-                double xl, xr;
-                if (!ellipse_row_range(E, y * TILE, min(y * TILE + TILE - 1, geo.H - 1), xl, xr)) continue;
-                if (!(xl <= xr)) continue;  // NaN guard
-                xa = max(xa, (int)floor(fmax(xl, -1e9) / TILE));
-                xb = min(xb, (int)floor(fmin(xr, 1e9) / TILE) + 1);
-            }
-            for (int x = xa; x < xb; ++x) {
-                ++total;
-                atomicAdd(&tile_count[geo.tile_off + y * geo.tx + x], 1);
-            }
+        ++k;
+    }
+    if (!task_offset) gtasks[g] = n;
+}
+
+__global__ void task_check_kernel(long long* __restrict__ header, int64_t tc) {
+    const long long nt = header[H_NTASK];
+    if (nt > tc || nt > 0x7fffffffLL) {
+        header[H_FLAGS] |= FLAG_OVERFLOW;
+        header[H_TOTAL] = 4 * nt;  // a retry with this capacity holds the tasks
+    }
+}
+
+// Tiles of task k in the order both passes enumerate them; calls fn(tile_index) for each.
+template <typename Fn>
+__device__ __forceinline__ int task_tiles(const int4 r, const Geo& geo, const float4 a, const float4 b,
+                                          const float4 c, float chi2, float beta, const unsigned* frame_dev, Fn fn) {
+    SliceEllipse E;
+    E.ok = 0;
+    if (frame_dev) {
+        SliceQuad S;
+        slice_setup(a, b, c, geo, beta, S);
+        if (!slice_ellipse(S, r, geo, chi2, __uint_as_float(frame_dev[geo.tile_off]), E)) return 0;
+    }
+    int n = 0;
+    for (int y = r.y; y < r.w; ++y) {
+        int xa = r.x, xb = r.z;
+        if (E.ok) {
+            double xl, xr;
+            if (!ellipse_row_range(E, y * TILE, min(y * TILE + TILE - 1, geo.H - 1), xl, xr)) continue;
+            if (!(xl <= xr)) continue;  // NaN guard
+            xa = max(xa, (int)floor(fmax(xl, -1e9) / TILE));
+            xb = min(xb, (int)floor(fmin(xr, 1e9) / TILE) + 1);
+        }
+        for (int x = xa; x < xb; ++x) {
+            fn(geo.tile_off + y * geo.tx + x, n);
+            ++n;
         }
     }
-    touched[g] = total;
+    return n;
+}
+
+__global__ void __launch_bounds__(128)
+task_count_kernel(const long long* __restrict__ header, const us3d_slice_frame* __restrict__ frames,
+                  const float4* __restrict__ pack, float chi2, float beta, const unsigned* __restrict__ frame_dev,
+                  const int4* __restrict__ task_rect, const int2* __restrict__ task_gf, int* __restrict__ task_ntiles,
+                  int* __restrict__ tile_count) {
+    if (header[H_FLAGS] != 0) return;
+    const long long nt = header[H_NTASK];
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += (long long)gridDim.x * blockDim.x) {
+        const int2 gf = task_gf[k];
+        const float4 a = pack[3 * (int64_t)gf.x], b = pack[3 * (int64_t)gf.x + 1], c = pack[3 * (int64_t)gf.x + 2];
+        const Geo geo = load_geo(frames + gf.y);
+        task_ntiles[k] = task_tiles(task_rect[k], geo, a, b, c, chi2, beta, frame_dev,
+                                    [&](int t, int) { atomicAdd(&tile_count[t], 1); });
+    }
+}
+
+__global__ void inst_offset_kernel(int64_t G, const int* __restrict__ task_offset, const int* __restrict__ task_inst,
+                                   const long long* __restrict__ header, int* __restrict__ inst_offset) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g > G) return;
+    inst_offset[g] = header[H_FLAGS] != 0 ? 0 : task_inst[task_offset[g]];
+}
+
+__global__ void __launch_bounds__(128)
+task_scatter_kernel(const long long* __restrict__ header, const us3d_slice_frame* __restrict__ frames,
+                    const float4* __restrict__ pack, float chi2, float beta, int sort_by_depth,
+                    const unsigned* __restrict__ frame_dev, const int4* __restrict__ task_rect,
+                    const int2* __restrict__ task_gf, const float* __restrict__ task_v,
+                    const int* __restrict__ task_inst, const int* __restrict__ tile_start, int* __restrict__ tile_cursor,
+                    unsigned long long* __restrict__ keys, int* __restrict__ slot_inst) {
+    if (header[H_FLAGS] != 0) return;
+    const long long nt = header[H_NTASK];
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += (long long)gridDim.x * blockDim.x) {
+        const int2 gf = task_gf[k];
+        const float4 a = pack[3 * (int64_t)gf.x], b = pack[3 * (int64_t)gf.x + 1], c = pack[3 * (int64_t)gf.x + 2];
+        const Geo geo = load_geo(frames + gf.y);
+        const unsigned long long key =
+            ((unsigned long long)depth_key(task_v[k], sort_by_depth) << 32) | (unsigned long long)(uint32_t)gf.x;
+        const int i0 = task_inst[k];
+        task_tiles(task_rect[k], geo, a, b, c, chi2, beta, frame_dev, [&](int t, int i) {
+            const int slot = tile_start[t] + atomicAdd(&tile_cursor[t], 1);
+            if (slot >= tile_start[t + 1]) return;  // never outside the bucket (verify_kernel flags it)
+            keys[slot] = key;
+            slot_inst[slot] = i0 + i;
+        });
+    }
 }
 
 // Every bucket must have been filled exactly as counted; otherwise later kernels see a flag.
@@ -435,54 +537,8 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
     long long flags = header[H_FLAGS];
     if (tg != tt) flags |= FLAG_TABLE;
     if (tg > cap || tg > 0x7fffffffLL) flags |= FLAG_OVERFLOW;
-    header[H_TOTAL] = tg;
+    header[H_TOTAL] = tg > header[H_TOTAL] ? tg : header[H_TOTAL];
     header[H_FLAGS] = flags;
-}
-
-__global__ void __launch_bounds__(256)
-scatter_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, int F,
-               const float4* __restrict__ pack, float chi2, float beta, int sort_by_depth,
-               const unsigned* __restrict__ frame_dev,
-               const int* __restrict__ inst_offset, const int* __restrict__ tile_start,
-               int* __restrict__ tile_cursor, const long long* __restrict__ header,
-               unsigned long long* __restrict__ keys, int* __restrict__ slot_inst) {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= G || header[H_FLAGS] != 0) return;
-    const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
-    int inst = inst_offset[g];
-    for (int f = 0; f < F; ++f) {
-        if (!frame_ok(frames + f, T, P)) continue;
-        const Geo geo = load_geo(frames + f);
-        int4 r;
-        float v_pix;
-        if (!project_rect(a, b, c, geo, chi2, beta, r, v_pix)) continue;
-        const unsigned long long key =
-            ((unsigned long long)depth_key(v_pix, sort_by_depth) << 32) | (unsigned long long)(uint32_t)g;
-        SliceEllipse E;
-        E.ok = 0;
-        if (frame_dev) {
-            SliceQuad S;
-            slice_setup(a, b, c, geo, beta, S);
-            if (!slice_ellipse(S, r, geo, chi2, __uint_as_float(frame_dev[geo.tile_off]), E)) continue;
-        }
-        for (int y = r.y; y < r.w; ++y) {
-            int xa = r.x, xb = r.z;
-            if (E.ok) {
-                double xl, xr;
-                if (!ellipse_row_range(E, y * TILE, min(y * TILE + TILE - 1, geo.H - 1), xl, xr)) continue;
-                if (!(xl <= xr)) continue;  // NaN guard
-                xa = max(xa, (int)floor(fmax(xl, -1e9) / TILE));
-                xb = min(xb, (int)floor(fmin(xr, 1e9) / TILE) + 1);
-            }
-            for (int x = xa; x < xb; ++x) {
-                const int t = geo.tile_off + y * geo.tx + x;
-                const int slot = tile_start[t] + atomicAdd(&tile_cursor[t], 1);
-                if (slot >= tile_start[t + 1]) continue;  // never outside the bucket (verify_kernel flags it)
-                keys[slot] = key;
-                slot_inst[slot] = inst++;
-            }
-        }
-    }
 }
 
 // ------------------------------------------------------------------------------------
@@ -897,19 +953,33 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
                                                                     w.tile_dev, w.frame_dev);
     const unsigned* tdev = slice_cull ? w.frame_dev : nullptr;
     const int gb = (int)((n_gauss + 255) / 256);
+    const int64_t tc = task_capacity(cap);
+    const unsigned tb = (unsigned)std::min<int64_t>((tc + 127) / 128, 148 * 16);
     if (n_gauss > 0) {
         pack_kernel<<<gb, 256, 0, stream>>>(n_gauss, means, tril, opac, inten, w.pack);
-        count_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, tdev,
-                                             w.touched, w.tile_count);
-        US3D_CHECK_LAUNCH("ug count");
+        cull_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, nullptr,
+                                            tc, w.gtasks, w.task_rect, w.task_gf, w.task_v);
+        US3D_CHECK_LAUNCH("ug cull");
     }
-    US3D_CHECK_CUDA(exclusive_scan(w.touched, n_gauss, w.inst_offset, w.bs_g, w.header + H_SCAN_G, stream));
+    US3D_CHECK_CUDA(exclusive_scan(w.gtasks, n_gauss, w.task_offset, w.bs_g, w.header + H_NTASK, stream));
+    task_check_kernel<<<1, 1, 0, stream>>>(w.header, tc);
+    US3D_CHECK_CUDA(cudaMemsetAsync(w.task_ntiles, 0, sizeof(int) * (size_t)tc, stream));
+    if (n_gauss > 0) {
+        cull_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta,
+                                            w.task_offset, tc, w.gtasks, w.task_rect, w.task_gf, w.task_v);
+        task_count_kernel<<<tb, 128, 0, stream>>>(w.header, frames, w.pack, chi2, beta, tdev, w.task_rect, w.task_gf,
+                                                  w.task_ntiles, w.tile_count);
+        US3D_CHECK_LAUNCH("ug task count");
+    }
+    US3D_CHECK_CUDA(exclusive_scan(w.task_ntiles, tc, w.task_inst, w.bs_k, w.header + H_SCAN_G, stream));
+    inst_offset_kernel<<<(unsigned)((n_gauss + 256) / 256), 256, 0, stream>>>(n_gauss, w.task_offset, w.task_inst,
+                                                                             w.header, w.inst_offset);
     US3D_CHECK_CUDA(exclusive_scan(w.tile_count, n_tiles, w.tile_start, w.bs_t, w.header + H_SCAN_T, stream));
     check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
     if (n_gauss > 0) {
-        scatter_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, sort_by_depth,
-                                               tdev, w.inst_offset, w.tile_start, w.tile_cursor, w.header, w.keys,
-                                               w.slot_inst);
+        task_scatter_kernel<<<tb, 128, 0, stream>>>(w.header, frames, w.pack, chi2, beta, sort_by_depth, tdev,
+                                                    w.task_rect, w.task_gf, w.task_v, w.task_inst, w.tile_start,
+                                                    w.tile_cursor, w.keys, w.slot_inst);
         US3D_CHECK_LAUNCH("ug scatter");
     }
     if (n_tiles > 0)
@@ -924,7 +994,7 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
         US3D_CHECK_LAUNCH("ug tile sort");
     }
     prof_end(prof, stream);
-    count_launches(1 + (n_frames > 0) + (slice_cull && n_tiles > 0) + 2 * (n_gauss > 0) + 6 + 1 + (n_gauss > 0) +
+    count_launches(1 + (n_frames > 0) + (slice_cull && n_tiles > 0) + 4 * (n_gauss > 0) + 9 + 3 + (n_gauss > 0) +
                    2 * (n_tiles > 0));
     return US3D_OK;
 }
