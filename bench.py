@@ -302,10 +302,17 @@ def run_b200(a):
 
 
 def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed):
+    """End to end through the public autograd API: every step copies its inputs (Gaussian
+    parameters, pixel positions, targets) from pinned host memory and reads its loss and
+    gradients back. The next step's inputs are copied on a second stream while the current
+    step computes (double buffering); after a synchronised priming pass the renderers run
+    without a per-step instance-total readback, and their overflow flags are checked after
+    the timed region."""
     import torch
 
-    from us3d_b200.batch import UltraGaussBatchRenderer
     from us3d_b200 import scenes
+    from us3d_b200 import ultragauss as UG
+    from us3d_b200.batch import UltraGaussBatchRenderer
 
     F = a.frames_per_step
     P1 = a.size * a.size
@@ -319,25 +326,59 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed):
     renderers = [UltraGaussBatchRenderer(specs[s:s + F], dev) for s in range(0, n_pool, F)]
     grad_host = [torch.empty_like(x).pin_memory() for x in host]
     loss_host = torch.empty((), dtype=torch.float32).pin_memory()
+    copy_stream = torch.cuda.Stream(device=dev)
+    compute = torch.cuda.current_stream()
+    slots = [dict(step=-1, ready=torch.cuda.Event(), free=torch.cuda.Event()) for _ in range(2)]
 
-    def step(i):
+    def prefetch(i):
+        sl = slots[i % 2]
         k = i % len(renderers)
         s = k * F
-        ps = [x.to(dev, non_blocking=True).requires_grad_(True) for x in host]
-        pix = sweep_pix[s * P1:(s + F) * P1].to(dev, non_blocking=True)
-        tgt = tgt_host[s * P1:(s + F) * P1].to(dev, non_blocking=True)
-        img, alpha, depth = renderers[k](*ps, pix)
+        with torch.cuda.stream(copy_stream):
+            copy_stream.wait_event(sl["free"])
+            sl["ps"] = [x.to(dev, non_blocking=True) for x in host]
+            sl["pix"] = sweep_pix[s * P1:(s + F) * P1].to(dev, non_blocking=True)
+            sl["tgt"] = tgt_host[s * P1:(s + F) * P1].to(dev, non_blocking=True)
+            sl["ready"].record(copy_stream)
+        sl["step"] = i
+
+    def step(i):
+        sl = slots[i % 2]
+        if sl["step"] != i:
+            prefetch(i)
+        compute.wait_event(sl["ready"])
+        ps, pix, tgt = sl["ps"], sl["pix"], sl["tgt"]
+        for t in ps + [pix, tgt]:
+            t.record_stream(compute)
+        prefetch(i + 1)
+        ps = [x.requires_grad_(True) for x in ps]
+        img, alpha, depth = renderers[i % len(renderers)](*ps, pix)
         loss = (img - tgt).abs().mean()
         loss.backward()
         loss_host.copy_(loss.detach(), non_blocking=True)
         for gh, p in zip(grad_host, ps):
             gh.copy_(p.grad, non_blocking=True)
+        sl["free"].record(compute)
 
+    # priming: one synchronised call per renderer fixes the instance capacity
+    cap = 0
+    for k, r in enumerate(renderers):
+        step(k)
+        cap = max(cap, int(r.last["binning"].total * 1.25) + 1024)
+    for r in renderers:
+        r.params["capacity"] = cap
+        r.params["sync_check"] = False
     ms = timed(step, a.steps, a.warmup)
+    for r in renderers:
+        if "binning" in r.last:
+            total, flags = UG.read_status(r.last["binning"])
+            if flags:
+                raise RuntimeError(f"e2e: binning flags {flags} (instances {total}, capacity {cap})")
     h2d = sum(x.numel() * x.element_size() for x in host) + F * P1 * 3 * 4 + F * P1 * 4
     d2h = 4 + sum(x.numel() * x.element_size() for x in host)
     return {"value": round(a.steps * F * world / (ms / 1e3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "api": "us3d_b200.batch.UltraGaussBatchRenderer (autograd)"}
+            "d2h_bytes_per_step": int(d2h), "api": "us3d_b200.batch.UltraGaussBatchRenderer (autograd)",
+            "copies": "next step's inputs prefetched on a second stream (double buffered)"}
 
 
 def cpu_baseline(a, sc, specs, frames: int = 1):
