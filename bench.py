@@ -39,7 +39,8 @@ BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (param
 # DRAM bytes (read + write) per frame of each stage's dominant kernel, from one ncu capture
 # of a 4-frame launch of the same scene, scaled linearly to the frames of a launch.
 NCU_TRAFFIC_PER_FRAME = {
-    "ug_backward": (119.58e6 + 212.23e6) / 4,  # backward_kernel, profiles/ultragauss_backward_kernel_4frames.md
+    "ug_backward": (91.150336e6 + 111.721216e6) / 4,  # backward_kernel, profiles/ultragauss_backward_kernel_4frames.md
+    "ug_forward": (45.9328e6 + 4.483584e6) / 4,       # forward_kernel, profiles/ultragauss_forward_kernel_4frames.md
 }
 
 
