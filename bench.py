@@ -253,6 +253,29 @@ def run_b200(a):
     stage_avg_ms = tot.value / max(n.value, 1)
     clocks = clk.summary()
 
+    # The same batched step captured once per frame batch as a CUDA graph and replayed (no
+    # host round trip or launch gaps inside a step); the overflow flags are checked after.
+    from us3d_b200.batch import GraphedTrainingStep
+
+    graphed = []
+    for ft_k, (ft, pix, tgt) in enumerate(batches):
+        graphed.append(GraphedTrainingStep(specs[ft_k * F:(ft_k + 1) * F], dev, params, pix,
+                                           lambda img, alpha, depth, tgt=tgt: (l1_grad(img, tgt), torch.zeros_like(img),
+                                                                               torch.zeros_like(img)),
+                                           grads=grad_bufs))
+
+    def graphed_step(i):
+        graphed[i % len(graphed)].replay()
+
+    with Clocks(local) as clk_g:
+        ms_graphed = timed(graphed_step, a.steps, a.warmup)
+    for gs in graphed:
+        gs.check()
+    uncaptured_value = a.steps * F * world / (ms_batched / 1e3)
+    if ms_graphed < ms_batched:
+        ms_batched = ms_graphed
+        clocks = clk_g.summary()
+
     frames_total = a.steps * F * world
     value = frames_total / (ms_batched / 1e3)
     I = statistics.mean(inst_per_frame)
@@ -281,6 +304,10 @@ def run_b200(a):
         "data": "synthetic: seeded headline scene (no dataset offline); targets U(0,1)",
         "config": workload_config(a, world), "instances_per_frame": round(I, 1), "roofline": roofline,
         "clocks": clocks, "gpu_launches": gpu_launches,
+        "batched_form": "CUDA-graph replay of bin + forward + L1 gradient + backward per 16-frame batch",
+        "uncaptured": {"value": round(uncaptured_value, 3), "unit": UNIT,
+                       "note": "same step launched from Python with one instance-total readback; "
+                               "the roofline stage times come from this run's CUDA events"},
     }
 
     if not a.no_plain:

@@ -344,3 +344,42 @@ def test_slice_cull_dropin_renderer(cuda_device):
         res.append([img.detach(), alpha.detach(), depth.detach()] + [p.grad for p in ps])
     for a, c in zip(*res):
         assert torch.equal(a, c)
+
+
+def test_graphed_training_step_matches_eager(cuda_device):
+    """A CUDA-graph replay of bin + forward + loss gradient + backward equals the same step
+    run eagerly, also after the parameters are updated in place between replays."""
+    from us3d_b200 import ultragauss as UG
+    from us3d_b200.batch import GraphedTrainingStep
+
+    dev = cuda_device
+    args, ft, pix, gg = _cull_case(dev, G=60000, sizes=((128, 128, 0.25), (96, 160, 0.3)))
+    params = [a.clone() for a in args]
+    tgt = torch.rand(pix.shape[0], generator=torch.Generator().manual_seed(1)).to(dev)
+
+    def loss_grad(img, alpha, depth):
+        return torch.sign(img - tgt) / img.numel(), 0.1 * alpha, torch.zeros_like(depth)
+
+    from us3d_b200 import scenes
+
+    sizes = ((128, 128, 0.25), (96, 160, 0.3))
+    specs = []
+    for i, (H, W, s) in enumerate(sizes):
+        fr = scenes.linear_sweep(len(sizes), H, W, s, seed=8)[i]
+        specs.append(UG.SliceSpec(H, W, s, s, fr.axial_near, fr.lateral_col_offset, fr.origin, fr.axis_lat,
+                                  fr.axis_ax, fr.axis_ele))
+    step = GraphedTrainingStep(specs, dev, params, pix, loss_grad)
+
+    def eager():
+        b = UG.bin_gaussians(*params, ft, 7.815, 1e-4, True)
+        img, alpha, depth, _ = UG.forward(b, pix, 1e-6, 0.0)
+        dI, dA, dD = loss_grad(img, alpha, depth)
+        return UG.backward(b, pix, dI, dA, dD, alpha, 1e-6, 0.0)
+
+    for it in range(2):
+        got = [x.clone() for x in step.replay()]
+        step.check()
+        ref = eager()
+        for a_, b_ in zip(got, ref):
+            assert torch.equal(a_, b_), it
+        params[0].add_(0.01)  # in-place update seen by the next replay

@@ -31,6 +31,14 @@
 namespace us3d {
 namespace ug {
 
+// Resident CTAs per SM the shading kernels are compiled for (register budget 65536 / (256 x n)).
+#ifndef US3D_UG_FWD_MIN_CTAS
+#define US3D_UG_FWD_MIN_CTAS 5
+#endif
+#ifndef US3D_UG_BWD_MIN_CTAS
+#define US3D_UG_BWD_MIN_CTAS 4
+#endif
+
 constexpr int TILE = 16;           // reference SLICE_TILE_SIZE (include/mapper/core.cuh:5)
 constexpr int TILE_PIX = TILE * TILE;
 constexpr int FWD_BATCH = 256;       // Gaussians staged per shared-memory batch
@@ -608,7 +616,7 @@ __device__ __forceinline__ int find_tile_coords(const Geo& geo, int64_t t, int& 
     return lt;
 }
 
-__global__ void __launch_bounds__(TILE_PIX)
+__global__ void __launch_bounds__(TILE_PIX, US3D_UG_FWD_MIN_CTAS)
 forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
                const long long* __restrict__ header, const float4* __restrict__ pack,
@@ -674,7 +682,7 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
 
 // One block per tile; thread k owns instance k of the tile list (strided by the block) and
 // sweeps the tile's pixels, which sit in shared memory with their upstream coefficients.
-__global__ void __launch_bounds__(TILE_PIX)
+__global__ void __launch_bounds__(TILE_PIX, US3D_UG_BWD_MIN_CTAS)
 backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                 const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
                 const int* __restrict__ sorted_inst, const long long* __restrict__ header,

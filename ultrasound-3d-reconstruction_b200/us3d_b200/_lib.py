@@ -7,6 +7,7 @@ renderer raises instead of falling back to anything else.
 from __future__ import annotations
 
 import ctypes
+import os
 import threading
 from ctypes import c_float, c_int32, c_int64, c_size_t, c_void_p, c_char_p, POINTER
 
@@ -204,7 +205,7 @@ def load(path=None):
     with _lock:
         if _lib is not None and path is None:
             return _lib
-        p = str(path or LIB_PATH)
+        p = str(path or os.environ.get("US3D_B200_LIB") or LIB_PATH)
         try:
             lib = ctypes.CDLL(p)
         except OSError as exc:  # missing build: fail loudly, there is no other compute path

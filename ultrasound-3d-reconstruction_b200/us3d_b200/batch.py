@@ -61,3 +61,57 @@ class UltraGaussBatchRenderer:
         self.last = {}
         return _BatchFunction.apply(self.frames, self.params, means, precision_tril.contiguous(),
                                     opacities.reshape(-1), intensities.reshape(-1), pixels, self.last)
+
+
+class GraphedTrainingStep:
+    """One training step of a batch of frames, captured once as a CUDA graph and replayed.
+
+    The step is: bin (slice-culled, fixed instance capacity, no host readback), forward,
+    ``loss_grad(image, alpha, depth) -> (d_image, d_alpha, d_depth)`` (any stream-ordered
+    PyTorch code), backward into the static gradient buffers ``grads``. Parameters, pixel
+    positions and whatever ``loss_grad`` reads must stay at the same addresses between
+    replays (update them in place). The capacity is set from a synchronised priming binning
+    times ``margin``; ``check()`` reads the last replay's flags (one synchronisation) and
+    raises if the instances outgrew it, after which the step should be rebuilt."""
+
+    def __init__(self, frames: Sequence[UG.SliceSpec], device: torch.device, params, pixels, loss_grad,
+                 grads=None, chi2_threshold: float = 7.815, diag_beta: float = 1e-4, sort_by_depth: bool = True,
+                 bg_alpha: float = 1e-6, bg_intensity: float = 0.0, margin: float = 1.25):
+        self.frames = UG.build_frame_table(list(frames), device)
+        self.params = [params[0], params[1].contiguous(), params[2].reshape(-1), params[3].reshape(-1)]
+        self.pixels = pixels
+        self.loss_grad = loss_grad
+        self.cfg = (float(chi2_threshold), float(diag_beta), bool(sort_by_depth))
+        self.bg = (float(bg_alpha), float(bg_intensity))
+        G = self.params[0].shape[0]
+        self.grads = grads if grads is not None else (
+            torch.empty((G, 3), device=device), torch.empty((G, 6), device=device), torch.empty((G,), device=device),
+            torch.empty((G,), device=device))
+        prime = UG.bin_gaussians(*self.params, self.frames, *self.cfg, slice_cull_pixels=pixels)
+        self.capacity = int(prime.total * margin) + 1024
+        self.binning = None
+        self._run()  # uncaptured: sets kernel attributes and allocator state
+        torch.cuda.synchronize(device)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._run()
+
+    def _run(self):
+        b = UG.bin_gaussians(*self.params, self.frames, *self.cfg, capacity=self.capacity, sync_check=False,
+                             slice_cull_pixels=self.pixels)
+        image, alpha, depth, _ = UG.forward(b, self.pixels, *self.bg, want_counts=False)
+        d_image, d_alpha, d_depth = self.loss_grad(image, alpha, depth)
+        UG.backward(b, self.pixels, d_image.contiguous(), d_alpha.contiguous(), d_depth.contiguous(), alpha, *self.bg,
+                    out=self.grads)
+        self.binning = b
+        self.outputs = (image, alpha, depth)
+
+    def replay(self):
+        self.graph.replay()
+        return self.grads
+
+    def check(self):
+        total, flags = UG.read_status(self.binning)
+        if flags:
+            raise RuntimeError(f"graphed step: binning flags {flags} ({total} instances, capacity {self.capacity})")
+        return total
