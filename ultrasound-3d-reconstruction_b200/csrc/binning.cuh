@@ -9,7 +9,14 @@
 namespace us3d {
 
 constexpr int SORT_THREADS = 512;
-constexpr int SORT_SMEM_CAP = 8192;  // keys sorted in shared memory per tile (96 KB)
+// Tiles of up to SORT_SMEM_CAP keys are ordered in shared memory by the first sort pass
+// (48 KB, four 512-thread blocks per SM); larger ones, up to SORT_BIG_CAP, by a second pass
+// with 96 KB; beyond that the network runs on global memory (one block per tile).
+constexpr int SORT_SMEM_CAP = 4096;
+constexpr int SORT_BIG_CAP = 8192;
+constexpr int SORT_MIN_BLOCKS = 4;
+// Above every real key: a key's low word is a Gaussian (or instance) index below 2^31.
+constexpr unsigned long long SORT_PAD_KEY = ~0ull;
 
 // Header words at the start of a binned workspace.
 enum { H_TOTAL = 0, H_FLAGS = 1, H_SCAN_G = 2, H_SCAN_T = 3, H_CAP = 4, H_G = 5, H_T = 6, H_P = 7, H_MODE = 8, H_NTASK = 9, H_WORDS = 16 };
@@ -28,23 +35,27 @@ static __device__ __forceinline__ void cswap(unsigned long long* k, int* v, int 
 
 // Ascending bitonic sort of n (not necessarily a power of two) keys with payload, in the
 // "mirror" formulation where every compare-exchange puts the smaller key at the lower
-// index; positions >= n act as +infinity and are never touched.
+// index; positions >= n act as +infinity and are never touched. Used on global memory for
+// buckets too large for shared memory.
 static __device__ void bitonic_sort(unsigned long long* k, int* v, int n) {
-    int npow = 1;
-    while (npow < n) npow <<= 1;
+    int npow = 1, lp = 0;
+    while (npow < n) {
+        npow <<= 1;
+        ++lp;
+    }
     const int half_n = npow >> 1;
-    for (int size = 2; size <= npow; size <<= 1) {
-        const int hs = size >> 1;
+    for (int ls = 1; ls <= lp; ++ls) {
+        const int size = 1 << ls, lh = ls - 1, hs = size >> 1;
         for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
-            const int blk = i / hs, off = i - blk * hs;
-            const int a = blk * size + off, b = blk * size + size - 1 - off;
-            if (b < n) cswap(k, v, a, b);
+            const int base = (i >> lh) << ls, off = i & (hs - 1);
+            const int b = base + size - 1 - off;
+            if (b < n) cswap(k, v, base + off, b);
         }
         __syncthreads();
-        for (int h = hs >> 1; h >= 1; h >>= 1) {
+        for (int l2 = lh - 1; l2 >= 0; --l2) {
+            const int h = 1 << l2;
             for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
-                const int blk = i / h, off = i - blk * h;
-                const int a = blk * 2 * h + off, b = a + h;
+                const int a = ((i >> l2) << (l2 + 1)) + (i & (h - 1)), b = a + h;
                 if (b < n) cswap(k, v, a, b);
             }
             __syncthreads();
@@ -52,36 +63,161 @@ static __device__ void bitonic_sort(unsigned long long* k, int* v, int n) {
     }
 }
 
+// Register-resident part of the shared-memory sort. A warp owns a 64-element segment; lane
+// l holds its elements 2l (x0) and 2l + 1 (x1). A compare-exchange of stride h >= 2 pairs
+// lane l with lane l ^ h/2 (same slot); a mirror pass over blocks of `size` pairs element
+// e with e ^ (size - 1), i.e. slot 0 of lane l with slot 1 of lane l ^ (size/2 - 1).
+struct SortKV {
+    unsigned long long k;
+    int v;
+};
+
+static __device__ __forceinline__ SortKV kv_shfl_xor(const SortKV& x, int mask) {
+    SortKV y;
+    y.k = __shfl_xor_sync(0xffffffffu, x.k, mask);
+    y.v = __shfl_xor_sync(0xffffffffu, x.v, mask);
+    return y;
+}
+
+// x becomes the smaller (keep_low) or the larger key of the pair; an equal key keeps x.
+static __device__ __forceinline__ void kv_keep(SortKV& x, const SortKV& y, bool keep_low) {
+    if (keep_low ? (y.k < x.k) : (x.k < y.k)) x = y;
+}
+
+static __device__ __forceinline__ void kv_order(SortKV& a, SortKV& b) {
+    if (b.k < a.k) {
+        const SortKV t = a;
+        a = b;
+        b = t;
+    }
+}
+
+static __device__ __forceinline__ void warp_stride_pass(SortKV& x0, SortKV& x1, int h, int lane) {
+    if (h == 1) {
+        kv_order(x0, x1);
+        return;
+    }
+    const int m = h >> 1;
+    const bool low = (lane & m) == 0;
+    const SortKV y0 = kv_shfl_xor(x0, m), y1 = kv_shfl_xor(x1, m);
+    kv_keep(x0, y0, low);
+    kv_keep(x1, y1, low);
+}
+
+static __device__ __forceinline__ void warp_mirror_pass(SortKV& x0, SortKV& x1, int size, int lane) {
+    if (size == 2) {
+        kv_order(x0, x1);
+        return;
+    }
+    const int m = (size >> 1) - 1;
+    const bool low = (lane & (size >> 2)) == 0;
+    const SortKV y0 = kv_shfl_xor(x1, m), y1 = kv_shfl_xor(x0, m);
+    kv_keep(x0, y0, low);
+    kv_keep(x1, y1, low);
+}
+
+static __device__ __forceinline__ void seg_load(const unsigned long long* sk, const int* sv, int seg, int lane,
+                                                SortKV& x0, SortKV& x1) {
+    const ulonglong2 k = reinterpret_cast<const ulonglong2*>(sk)[seg * 32 + lane];
+    const int2 v = reinterpret_cast<const int2*>(sv)[seg * 32 + lane];
+    x0 = {k.x, v.x};
+    x1 = {k.y, v.y};
+}
+
+static __device__ __forceinline__ void seg_store(unsigned long long* sk, int* sv, int seg, int lane,
+                                                 const SortKV& x0, const SortKV& x1) {
+    reinterpret_cast<ulonglong2*>(sk)[seg * 32 + lane] = make_ulonglong2(x0.k, x1.k);
+    reinterpret_cast<int2*>(sv)[seg * 32 + lane] = make_int2(x0.v, x1.v);
+}
+
+// Ascending sort of the npow (a power of two >= 64) keys with payload in shared memory
+// (16-byte aligned key array, 8-byte aligned payload array), the same mirror network as
+// bitonic_sort: passes that stay inside 64-element segments run in registers with warp
+// shuffles, the others as shared-memory compare-exchanges between block barriers. The
+// caller pads the keys past the bucket with SORT_PAD_KEY and synchronises first.
+static __device__ void block_sort_smem(unsigned long long* sk, int* sv, int npow) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int nseg = npow >> 6, half_n = npow >> 1;
+    for (int s = warp; s < nseg; s += nwarp) {
+        SortKV x0, x1;
+        seg_load(sk, sv, s, lane, x0, x1);
+#pragma unroll
+        for (int size = 2; size <= 64; size <<= 1) {
+            warp_mirror_pass(x0, x1, size, lane);
+#pragma unroll
+            for (int h = size >> 2; h >= 1; h >>= 1) warp_stride_pass(x0, x1, h, lane);
+        }
+        seg_store(sk, sv, s, lane, x0, x1);
+    }
+    __syncthreads();
+    for (int ls = 7; (1 << ls) <= npow; ++ls) {
+        const int size = 1 << ls, lh = ls - 1, hs = size >> 1;
+        for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
+            const int base = (i >> lh) << ls, off = i & (hs - 1);
+            cswap(sk, sv, base + off, base + size - 1 - off);
+        }
+        __syncthreads();
+        for (int l2 = lh - 1; l2 >= 6; --l2) {
+            const int h = 1 << l2;
+            for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
+                const int a = ((i >> l2) << (l2 + 1)) + (i & (h - 1));
+                cswap(sk, sv, a, a + h);
+            }
+            __syncthreads();
+        }
+        for (int s = warp; s < nseg; s += nwarp) {
+            SortKV x0, x1;
+            seg_load(sk, sv, s, lane, x0, x1);
+#pragma unroll
+            for (int h = 32; h >= 1; h >>= 1) warp_stride_pass(x0, x1, h, lane);
+            seg_store(sk, sv, s, lane, x0, x1);
+        }
+        __syncthreads();
+    }
+}
+
+// Orders bucket t (n keys at s0) in shared memory of capacity `cap` (a power of two >= n)
+// and writes the sorted Gaussian indices, instance ids and keys.
+static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_keys, int* s_idx, int s0, int n,
+                                                        unsigned long long* __restrict__ keys,
+                                                        const int* __restrict__ slot_inst,
+                                                        int* __restrict__ sorted_gid, int* __restrict__ sorted_inst) {
+    int npow = 64;
+    while (npow < n) npow <<= 1;
+    for (int i = threadIdx.x; i < npow; i += blockDim.x) {
+        s_keys[i] = i < n ? keys[s0 + i] : SORT_PAD_KEY;
+        s_idx[i] = i;
+    }
+    __syncthreads();
+    block_sort_smem(s_keys, s_idx, npow);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const unsigned long long k = s_keys[i];
+        sorted_gid[s0 + i] = (int)(uint32_t)(k & 0xffffffffull);
+        sorted_inst[s0 + i] = slot_inst[s0 + s_idx[i]];
+        keys[s0 + i] = k;
+    }
+}
+
 // One block per tile: order the tile's bucket by (depth key, Gaussian index), which is the
 // order the reference's stable radix sort of (tile << 32 | depth key) over instances
-// enumerated Gaussian by Gaussian produces (src/mapper/wrapper_mapper.cu:134-146).
-static __global__ void __launch_bounds__(SORT_THREADS)
+// enumerated Gaussian by Gaussian produces (src/mapper/wrapper_mapper.cu:134-146). Keys
+// within a bucket are distinct (a Gaussian enters a tile's bucket at most once), so any
+// correct sorting network gives that order.
+static __global__ void __launch_bounds__(SORT_THREADS, SORT_MIN_BLOCKS)
 tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
                  unsigned long long* __restrict__ keys, int* __restrict__ slot_inst,
                  int* __restrict__ sorted_gid, int* __restrict__ sorted_inst) {
-    extern __shared__ unsigned long long s_keys[];
-    int* s_idx = reinterpret_cast<int*>(s_keys + SORT_SMEM_CAP);
+    __shared__ __align__(16) unsigned long long s_keys[SORT_SMEM_CAP];
+    __shared__ __align__(16) int s_idx[SORT_SMEM_CAP];
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0) return;
     const int s0 = tile_start[t];
     const int n = tile_start[t + 1] - s0;
     if (n <= 0) return;
     if (n <= SORT_SMEM_CAP) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            s_keys[i] = keys[s0 + i];
-            s_idx[i] = i;
-        }
-        __syncthreads();
-        bitonic_sort(s_keys, s_idx, n);
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const unsigned long long k = s_keys[i];
-            sorted_gid[s0 + i] = (int)(uint32_t)(k & 0xffffffffull);
-            sorted_inst[s0 + i] = slot_inst[s0 + s_idx[i]];
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) keys[s0 + i] = s_keys[i];
-    } else {
-        // Oversized bucket: same network directly on global memory (one block owns it).
+        sort_bucket_smem(s_keys, s_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst);
+    } else if (n > SORT_BIG_CAP) {
+        // Oversized bucket: the network directly on global memory (one block owns it).
         bitonic_sort(keys + s0, slot_inst + s0, n);
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             sorted_gid[s0 + i] = (int)(uint32_t)(keys[s0 + i] & 0xffffffffull);
@@ -90,20 +226,70 @@ tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long*
     }
 }
 
+// Second pass: buckets of SORT_SMEM_CAP < n <= SORT_BIG_CAP keys with 96 KB of shared
+// memory. Each block inspects SORT_BIG_TILES consecutive tiles and orders its large ones.
+constexpr int SORT_BIG_TILES = 16;
 
-// Raises the sort kernel's dynamic shared-memory limit once per device for the calling
-// translation unit's copy of the kernel.
-static inline cudaError_t ensure_tile_sort_smem(bool* done_per_device, int n_devices) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev >= 0 && dev < n_devices && done_per_device[dev]) return cudaSuccess;
-    e = cudaFuncSetAttribute(tile_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SORT_SMEM_CAP * (int)(sizeof(unsigned long long) + sizeof(int)));
-    if (e == cudaSuccess && dev >= 0 && dev < n_devices) done_per_device[dev] = true;
-    return e;
+static __global__ void __launch_bounds__(SORT_THREADS)
+tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
+                     unsigned long long* __restrict__ keys, int* __restrict__ slot_inst,
+                     int* __restrict__ sorted_gid, int* __restrict__ sorted_inst) {
+    extern __shared__ __align__(16) unsigned long long s_big_keys[];
+    int* s_big_idx = reinterpret_cast<int*>(s_big_keys + SORT_BIG_CAP);
+    if (header[H_FLAGS] != 0) return;
+    const int64_t t0 = (int64_t)blockIdx.x * SORT_BIG_TILES;
+    const int64_t t = t0 + threadIdx.x;
+    bool big = false;
+    if (threadIdx.x < SORT_BIG_TILES && t < T) {
+        const int n = tile_start[t + 1] - tile_start[t];
+        big = n > SORT_SMEM_CAP && n <= SORT_BIG_CAP;
+    }
+    __shared__ unsigned s_mask;
+    if (threadIdx.x < 32) {
+        const unsigned m = __ballot_sync(0xffffffffu, big);
+        if (threadIdx.x == 0) s_mask = m;
+    }
+    __syncthreads();
+    unsigned mask = s_mask;
+    while (mask != 0u) {
+        const int j = __ffs(mask) - 1;
+        mask &= mask - 1u;
+        const int s0 = tile_start[t0 + j];
+        const int n = tile_start[t0 + j + 1] - s0;
+        sort_bucket_smem(s_big_keys, s_big_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst);
+        __syncthreads();
+    }
 }
 
-static inline size_t tile_sort_smem_bytes() { return SORT_SMEM_CAP * (sizeof(unsigned long long) + sizeof(int)); }
+static inline size_t tile_sort_big_smem_bytes() { return SORT_BIG_CAP * (sizeof(unsigned long long) + sizeof(int)); }
+
+// Launches the tile sort on `stream`: the shared-memory pass over all T tiles and, for large
+// buckets, the 96 KB pass. `attr_done` records per device that the second kernel's
+// shared-memory limit was raised (one array per translation unit, 128 devices).
+static inline cudaError_t launch_tile_sort(int64_t T, const int* tile_start, const long long* header,
+                                           unsigned long long* keys, int* slot_inst, int* sorted_gid,
+                                           int* sorted_inst, bool* attr_done, cudaStream_t stream) {
+    if (T <= 0) return cudaSuccess;
+    tile_sort_kernel<<<(unsigned)T, SORT_THREADS, 0, stream>>>(T, tile_start, header, keys, slot_inst, sorted_gid,
+                                                                sorted_inst);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (!(dev >= 0 && dev < 128 && attr_done[dev])) {
+        e = cudaFuncSetAttribute(tile_sort_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_sort_big_smem_bytes());
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 128) attr_done[dev] = true;
+    }
+    const unsigned grid = (unsigned)((T + SORT_BIG_TILES - 1) / SORT_BIG_TILES);
+    tile_sort_big_kernel<<<grid, SORT_THREADS, tile_sort_big_smem_bytes(), stream>>>(
+        T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst);
+    return cudaGetLastError();
+}
+
+// Kernel launches launch_tile_sort makes for T > 0 tiles.
+constexpr int TILE_SORT_LAUNCHES = 2;
 
 }  // namespace us3d

@@ -829,15 +829,14 @@ extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t 
     if (n_gauss > 0)
         scatter_kernel<<<gb, 256, 0, stream>>>(n_gauss, tx, w.rects, w.dkey, w.inst_offset, w.tile_start,
                                                w.tile_cursor, w.header, w.keys, w.slot_inst);
-    US3D_CHECK_CUDA(ensure_tile_sort_smem(g_gp_sort_attr, 128));
-    tile_sort_kernel<<<(unsigned)T, SORT_THREADS, tile_sort_smem_bytes(), stream>>>(
-        T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst);
+    US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
+                                     g_gp_sort_attr, stream));
     forward_kernel<<<(unsigned)T, tile_size * tile_size, 0, stream>>>(H, W, tile_size, tx, grid_pack, focus_params,
                                                                      w.tile_start, w.sorted_gid, w.header, w.cand,
                                                                      out_image);
     US3D_CHECK_LAUNCH("gp forward");
     prof_end(prof, stream);
-    count_launches(1 + (n_gauss > 0) * 2 + 6 + 1 + 1 + 1);
+    count_launches(1 + (n_gauss > 0) * 2 + 6 + 1 + TILE_SORT_LAUNCHES + 1);
     return US3D_OK;
 }
 

@@ -470,15 +470,14 @@ extern "C" int us3d_sa_bounded_forward(void* workspace, size_t workspace_bytes, 
     if (n > 0)
         scatter_kernel<<<gb, 256, 0, stream>>>(n, gw, w.rects, w.inst_offset, w.tile_start, w.tile_cursor, w.header,
                                                w.keys, w.slot_inst);
-    US3D_CHECK_CUDA(ensure_tile_sort_smem(g_sa_sort_attr, 128));
-    tile_sort_kernel<<<(unsigned)T, SORT_THREADS, tile_sort_smem_bytes(), stream>>>(
-        T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst);
+    US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
+                                     g_sa_sort_attr, stream));
     forward_kernel<<<(unsigned)T, TILE * TILE, 0, stream>>>(H, W, gw, half_width, half_height, radius_sigma, m2, iv,
                                                             weights, colors, w.tile_start, w.sorted_gid, w.header,
                                                             out_image, out_alpha);
     US3D_CHECK_LAUNCH("sa forward");
     prof_end(prof, stream);
-    count_launches(1 + 2 * (n > 0) + 6 + 1 + 1 + 1);
+    count_launches(1 + 2 * (n > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
     return US3D_OK;
 }
 

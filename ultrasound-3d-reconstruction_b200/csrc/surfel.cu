@@ -1061,15 +1061,13 @@ extern "C" int us3d_gs_forward(void* workspace, size_t workspace_bytes, int64_t 
     if (n_gauss > 0)
         scatter_kernel<<<gb, 256, 0, stream>>>((int)n_gauss, p.gx, w.rect, w.depth, w.inst_offset, w.tile_start,
                                                w.tile_cursor, w.header, w.keys, w.slot_inst);
-    US3D_CHECK_CUDA(ensure_tile_sort_smem(g_gs_sort_attr, 128));
-    tile_sort_kernel<<<(unsigned)T, SORT_THREADS, tile_sort_smem_bytes(), stream>>>(T, w.tile_start, w.header, w.keys,
-                                                                                   w.slot_inst, w.sorted_gid,
-                                                                                   w.sorted_inst);
+    US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
+                                     g_gs_sort_attr, stream));
     forward_kernel<<<(unsigned)T, BLOCK, 0, stream>>>(width, height, p.gx, w.tile_start, w.sorted_gid, w.header, w.rec,
                                                       background, out_color, out_others, w.accum, w.n_contrib);
     US3D_CHECK_LAUNCH("gs forward");
     prof_end(prof, stream);
-    count_launches(1 + 2 * (n_gauss > 0) + 6 + 1 + 1 + 1);
+    count_launches(1 + 2 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
     return US3D_OK;
 }
 

@@ -889,18 +889,8 @@ __global__ void export_kernel(int tile_off, int n_tiles_frame, const int* __rest
 using namespace us3d;
 using namespace us3d::ug;
 
-// Per-device flag: the sort kernel's dynamic shared-memory limit has been raised.
+// Per-device flag: the large-bucket sort kernel's shared-memory limit has been raised.
 static bool g_sort_attr_done[128];
-
-static int ensure_sort_attr() {
-    int dev = 0;
-    US3D_CHECK_CUDA(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 128 && g_sort_attr_done[dev]) return US3D_OK;
-    US3D_CHECK_CUDA(cudaFuncSetAttribute(tile_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         SORT_SMEM_CAP * (int)(sizeof(unsigned long long) + sizeof(int))));
-    if (dev >= 0 && dev < 128) g_sort_attr_done[dev] = true;
-    return US3D_OK;
-}
 
 extern "C" size_t us3d_ug_workspace_bytes(int64_t n_gauss, int32_t n_frames, int64_t n_tiles,
                                           int64_t n_pixels, int64_t instance_capacity) {
@@ -994,16 +984,12 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
         verify_kernel<<<(unsigned)((n_tiles + 255) / 256), 256, 0, stream>>>(n_tiles, w.tile_count, w.tile_cursor,
                                                                               w.header);
     if (n_tiles > 0) {
-        st = ensure_sort_attr();
-        if (st != US3D_OK) return st;
-        tile_sort_kernel<<<(unsigned)n_tiles, SORT_THREADS,
-                           SORT_SMEM_CAP * (sizeof(unsigned long long) + sizeof(int)), stream>>>(
-            n_tiles, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst);
-        US3D_CHECK_LAUNCH("ug tile sort");
+        US3D_CHECK_CUDA(launch_tile_sort(n_tiles, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid,
+                                         w.sorted_inst, g_sort_attr_done, stream));
     }
     prof_end(prof, stream);
     count_launches(1 + (n_frames > 0) + (slice_cull && n_tiles > 0) + 4 * (n_gauss > 0) + 9 + 3 + (n_gauss > 0) +
-                   2 * (n_tiles > 0));
+                   (1 + TILE_SORT_LAUNCHES) * (n_tiles > 0));
     return US3D_OK;
 }
 

@@ -685,16 +685,15 @@ extern "C" int us3d_ugr_forward(void* workspace, size_t workspace_bytes, int64_t
     if (n_gauss > 0)
         scatter_kernel<<<gb, 256, 0, stream>>>(n_gauss, w.ray_range, w.dkey, w.inst_offset, w.ray_start, w.ray_cursor,
                                                w.header, w.keys, w.slot_inst);
-    US3D_CHECK_CUDA(ensure_tile_sort_smem(g_ugr_sort_attr, 128));
-    tile_sort_kernel<<<(unsigned)W, SORT_THREADS, tile_sort_smem_bytes(), stream>>>(
-        W, w.ray_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst);
+    US3D_CHECK_CUDA(launch_tile_sort(W, w.ray_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
+                                     g_ugr_sort_attr, stream));
     forward_kernel<<<(unsigned)W, 256, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions,
                                                     ray_origins, ray_dirs, axis_ele, ray_perturbations, w.dkey,
                                                     k_sigma, quadrature_window_radius_mm, local_window_only ? 1 : 0,
                                                     local_max_window_mm, out_image, w.pixel_state);
     US3D_CHECK_LAUNCH("ugr forward");
     prof_end(prof, stream);
-    count_launches(1 + 2 * (n_gauss > 0) + 6 + 1 + 1 + 1);
+    count_launches(1 + 2 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
     return US3D_OK;
 }
 
