@@ -89,50 +89,71 @@ def _torch_flags():
     return inc, libdirs, abi
 
 
-def build_module(name: str, reference: Path, force: bool = False) -> Path:
+def _plan(name: str, reference: Path):
+    """Compile commands (source -> object) and the link command of one module."""
     rdir, srcs, nvflags = MODULES[name]
     root = reference / rdir
     nvflags = [f.replace("{root}", str(root)) for f in nvflags]
     suffix = sysconfig.get_config_var("EXT_SUFFIX")
     out = OUT_DIR / f"{name}{suffix}"
-    if out.exists() and not force:
-        return out
-    OUT_DIR.mkdir(parents=True, exist_ok=True)
     obj_dir = OUT_DIR / f"obj_{name}"
-    obj_dir.mkdir(parents=True, exist_ok=True)
     inc, libdirs, abi = _torch_flags()
     defs = [f"-DTORCH_EXTENSION_NAME={name}", "-DTORCH_API_INCLUDE_EXTENSION_H", f"-D_GLIBCXX_USE_CXX11_ABI={abi}"]
     incs = ["-I", str(root / "include"), "-I", str(root / "src"), "-I", str(SHIM)] + [x for p in inc for x in ("-I", p)]
-    objs = []
+    compiles, objs = [], []
     for s in srcs:
         src = (HERE / "ref_harness" / s.split(":", 1)[1]) if s.startswith("HARNESS:") else root / s
         obj = obj_dir / (s.replace("/", "_").replace(":", "_") + ".o")
-        if s.endswith(".cu") and not s.startswith("HARNESS:"):
-            cmd = ["nvcc", "-c", str(src), "-o", str(obj), *ARCH, *nvflags, "-std=c++17", "-Xcompiler", "-fPIC",
-                   "--expt-relaxed-constexpr", *defs, *incs]
-        elif s.endswith(".cu"):
+        if s.endswith(".cu"):
             cmd = ["nvcc", "-c", str(src), "-o", str(obj), *ARCH, *nvflags, "-std=c++17", "-Xcompiler", "-fPIC",
                    "--expt-relaxed-constexpr", *defs, *incs]
         else:
             cmd = ["g++", "-c", str(src), "-o", str(obj), "-O3", "-std=c++17", "-fPIC", "-include", "cstdint", *defs,
                    *incs, *[f for f in nvflags if f.startswith("-I")]]
-        subprocess.run(cmd, check=True)
+        compiles.append(cmd)
         objs.append(str(obj))
     link = ["g++", "-shared", "-o", str(out), *objs]
     for d in libdirs:
         link += ["-L", d, f"-Wl,-rpath,{d}"]
     link += ["-lc10", "-lc10_cuda", "-ltorch", "-ltorch_cpu", "-ltorch_cuda", "-ltorch_python", "-lcudart"]
-    subprocess.run(link, check=True)
-    for o in objs:
-        os.remove(o)
-    obj_dir.rmdir()
-    return out
+    return out, obj_dir, compiles, objs, link
 
 
-def build_all(reference: Path = DEFAULT_REFERENCE, force: bool = False) -> list[Path]:
+def _run_plans(plans, jobs: int) -> None:
+    from concurrent.futures import ThreadPoolExecutor
+
+    for _, obj_dir, _, _, _ in plans:
+        obj_dir.mkdir(parents=True, exist_ok=True)
+    cmds = [c for plan in plans for c in plan[2]]
+    with ThreadPoolExecutor(max_workers=max(1, jobs)) as ex:
+        for f in [ex.submit(subprocess.run, c, check=True) for c in cmds]:
+            f.result()
+    for out, obj_dir, _, objs, link in plans:
+        subprocess.run(link, check=True)
+        for o in objs:
+            os.remove(o)
+        obj_dir.rmdir()
+
+
+def build_module(name: str, reference: Path, force: bool = False, jobs: int = 0) -> Path:
+    plan = _plan(name, reference)
+    if plan[0].exists() and not force:
+        return plan[0]
+    OUT_DIR.mkdir(parents=True, exist_ok=True)
+    _run_plans([plan], jobs or os.cpu_count() or 1)
+    return plan[0]
+
+
+def build_all(reference: Path = DEFAULT_REFERENCE, force: bool = False, jobs: int = 0) -> list[Path]:
+    """Builds every module; the translation units of all modules compile in parallel."""
     if not reference.exists():
         return []
-    return [build_module(n, reference, force) for n in MODULES]
+    plans = [_plan(n, reference) for n in MODULES]
+    todo = [p for p in plans if force or not p[0].exists()]
+    if todo:
+        OUT_DIR.mkdir(parents=True, exist_ok=True)
+        _run_plans(todo, jobs or os.cpu_count() or 1)
+    return [p[0] for p in plans]
 
 
 if __name__ == "__main__":
