@@ -181,7 +181,9 @@ static __device__ void block_sort_smem(unsigned long long* sk, int* sv, int npow
 static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_keys, int* s_idx, int s0, int n,
                                                         unsigned long long* __restrict__ keys,
                                                         const int* __restrict__ slot_inst,
-                                                        int* __restrict__ sorted_gid, int* __restrict__ sorted_inst) {
+                                                        int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
+                                                        const unsigned char* __restrict__ slot_mask,
+                                                        unsigned char* __restrict__ sorted_mask) {
     int npow = 64;
     while (npow < n) npow <<= 1;
     for (int i = threadIdx.x; i < npow; i += blockDim.x) {
@@ -194,6 +196,7 @@ static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_ke
         const unsigned long long k = s_keys[i];
         sorted_gid[s0 + i] = (int)(uint32_t)(k & 0xffffffffull);
         sorted_inst[s0 + i] = slot_inst[s0 + s_idx[i]];
+        if (sorted_mask) sorted_mask[s0 + i] = slot_mask[s0 + s_idx[i]];
         keys[s0 + i] = k;
     }
 }
@@ -202,11 +205,13 @@ static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_ke
 // order the reference's stable radix sort of (tile << 32 | depth key) over instances
 // enumerated Gaussian by Gaussian produces (src/mapper/wrapper_mapper.cu:134-146). Keys
 // within a bucket are distinct (a Gaussian enters a tile's bucket at most once), so any
-// correct sorting network gives that order.
+// correct sorting network gives that order. The optional per-slot byte (slot_mask) follows
+// its instance into sorted_mask.
 static __global__ void __launch_bounds__(SORT_THREADS, SORT_MIN_BLOCKS)
 tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
-                 unsigned long long* __restrict__ keys, int* __restrict__ slot_inst,
-                 int* __restrict__ sorted_gid, int* __restrict__ sorted_inst) {
+                 unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
+                 int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
+                 const unsigned char* __restrict__ slot_mask, unsigned char* __restrict__ sorted_mask) {
     __shared__ __align__(16) unsigned long long s_keys[SORT_SMEM_CAP];
     __shared__ __align__(16) int s_idx[SORT_SMEM_CAP];
     const int64_t t = blockIdx.x;
@@ -215,13 +220,18 @@ tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long*
     const int n = tile_start[t + 1] - s0;
     if (n <= 0) return;
     if (n <= SORT_SMEM_CAP) {
-        sort_bucket_smem(s_keys, s_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst);
+        sort_bucket_smem(s_keys, s_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
     } else if (n > SORT_BIG_CAP) {
-        // Oversized bucket: the network directly on global memory (one block owns it).
-        bitonic_sort(keys + s0, slot_inst + s0, n);
+        // Oversized bucket: the network directly on global memory (one block owns it), with
+        // the slot indices as payload in sorted_inst.
+        for (int i = threadIdx.x; i < n; i += blockDim.x) sorted_inst[s0 + i] = i;
+        __syncthreads();
+        bitonic_sort(keys + s0, sorted_inst + s0, n);
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int slot = sorted_inst[s0 + i];
             sorted_gid[s0 + i] = (int)(uint32_t)(keys[s0 + i] & 0xffffffffull);
-            sorted_inst[s0 + i] = slot_inst[s0 + i];
+            sorted_inst[s0 + i] = slot_inst[s0 + slot];
+            if (sorted_mask) sorted_mask[s0 + i] = slot_mask[s0 + slot];
         }
     }
 }
@@ -232,8 +242,9 @@ constexpr int SORT_BIG_TILES = 16;
 
 static __global__ void __launch_bounds__(SORT_THREADS)
 tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
-                     unsigned long long* __restrict__ keys, int* __restrict__ slot_inst,
-                     int* __restrict__ sorted_gid, int* __restrict__ sorted_inst) {
+                     unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
+                     int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
+                     const unsigned char* __restrict__ slot_mask, unsigned char* __restrict__ sorted_mask) {
     extern __shared__ __align__(16) unsigned long long s_big_keys[];
     int* s_big_idx = reinterpret_cast<int*>(s_big_keys + SORT_BIG_CAP);
     if (header[H_FLAGS] != 0) return;
@@ -256,7 +267,8 @@ tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long l
         mask &= mask - 1u;
         const int s0 = tile_start[t0 + j];
         const int n = tile_start[t0 + j + 1] - s0;
-        sort_bucket_smem(s_big_keys, s_big_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst);
+        sort_bucket_smem(s_big_keys, s_big_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask,
+                         sorted_mask);
         __syncthreads();
     }
 }
@@ -265,13 +277,16 @@ static inline size_t tile_sort_big_smem_bytes() { return SORT_BIG_CAP * (sizeof(
 
 // Launches the tile sort on `stream`: the shared-memory pass over all T tiles and, for large
 // buckets, the 96 KB pass. `attr_done` records per device that the second kernel's
-// shared-memory limit was raised (one array per translation unit, 128 devices).
+// shared-memory limit was raised (one array per translation unit, 128 devices). slot_mask /
+// sorted_mask may be NULL.
 static inline cudaError_t launch_tile_sort(int64_t T, const int* tile_start, const long long* header,
-                                           unsigned long long* keys, int* slot_inst, int* sorted_gid,
-                                           int* sorted_inst, bool* attr_done, cudaStream_t stream) {
+                                           unsigned long long* keys, const int* slot_inst, int* sorted_gid,
+                                           int* sorted_inst, bool* attr_done, cudaStream_t stream,
+                                           const unsigned char* slot_mask = nullptr,
+                                           unsigned char* sorted_mask = nullptr) {
     if (T <= 0) return cudaSuccess;
     tile_sort_kernel<<<(unsigned)T, SORT_THREADS, 0, stream>>>(T, tile_start, header, keys, slot_inst, sorted_gid,
-                                                                sorted_inst);
+                                                                sorted_inst, slot_mask, sorted_mask);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int dev = 0;
@@ -285,7 +300,7 @@ static inline cudaError_t launch_tile_sort(int64_t T, const int* tile_start, con
     }
     const unsigned grid = (unsigned)((T + SORT_BIG_TILES - 1) / SORT_BIG_TILES);
     tile_sort_big_kernel<<<grid, SORT_THREADS, tile_sort_big_smem_bytes(), stream>>>(
-        T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst);
+        T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
     return cudaGetLastError();
 }
 

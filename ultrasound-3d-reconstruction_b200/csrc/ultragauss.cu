@@ -42,6 +42,11 @@ namespace ug {
 constexpr int TILE = 16;           // reference SLICE_TILE_SIZE (include/mapper/core.cuh:5)
 constexpr int TILE_PIX = TILE * TILE;
 constexpr int FWD_BATCH = 256;       // Gaussians staged per shared-memory batch
+// A tile's pixels are shaded by 8 warps, each owning a block of 8 columns x 4 rows; bit
+// (band * 2 + half) of an instance's block mask is set when the Gaussian can reach block
+// (4-row band `band`, 8-column half `half`) of that tile.
+constexpr int BLK_W = 8, BLK_H = 4;
+constexpr int BWD_CHUNK = 1024;      // instances regrouped per backward pass
 
 // Header words at the start of the workspace.
 
@@ -69,6 +74,8 @@ struct Workspace {
     int* slot_inst;          // cap: instance index of each bucket slot (unsorted)
     int* sorted_gid;         // cap
     int* sorted_inst;        // cap
+    unsigned char* slot_mask;    // cap: warp-block mask of each bucket slot (unsorted)
+    unsigned char* sorted_mask;  // cap
     float2* pixel_aux;       // P: no-skip sums (sum a*c, sum a*depth) for the backward
     size_t bytes;
 };
@@ -105,6 +112,8 @@ static Workspace carve(void* base, int64_t G, int64_t T, int64_t P, int64_t cap)
     w.slot_inst = c.take<int>((size_t)cap);
     w.sorted_gid = c.take<int>((size_t)cap);
     w.sorted_inst = c.take<int>((size_t)cap);
+    w.slot_mask = c.take<unsigned char>((size_t)cap);
+    w.sorted_mask = c.take<unsigned char>((size_t)cap);
     w.pixel_aux = c.take<float2>((size_t)P);
     w.bytes = align_up(c.off, 256);
     return w;
@@ -454,8 +463,12 @@ __global__ void task_check_kernel(long long* __restrict__ header, int64_t tc) {
     }
 }
 
-// Tiles of task k in the order both passes enumerate them; calls fn(tile_index) for each.
-template <typename Fn>
+// Tiles of task k in the order both passes enumerate them; calls fn(tile_index, i, blocks)
+// for each, i counting the task's tiles. With WANT_BLOCKS, `blocks` marks the tile's warp
+// blocks that the in-slice ellipse reaches: each 4-row band's exact pixel-centre x-range,
+// tested against the block's columns (the same conservative bound as the tile cull, so a
+// pixel that passes the chi-square test always lies in a marked block); 0xff without a cull.
+template <bool WANT_BLOCKS, typename Fn>
 __device__ __forceinline__ int task_tiles(const int4 r, const Geo& geo, const float4 a, const float4 b,
                                           const float4 c, float chi2, float beta, const unsigned* frame_dev, Fn fn) {
     SliceEllipse E;
@@ -468,15 +481,41 @@ __device__ __forceinline__ int task_tiles(const int4 r, const Geo& geo, const fl
     int n = 0;
     for (int y = r.y; y < r.w; ++y) {
         int xa = r.x, xb = r.z;
+        double bl[TILE / BLK_H], br[TILE / BLK_H];
         if (E.ok) {
             double xl, xr;
             if (!ellipse_row_range(E, y * TILE, min(y * TILE + TILE - 1, geo.H - 1), xl, xr)) continue;
             if (!(xl <= xr)) continue;  // NaN guard
             xa = max(xa, (int)floor(fmax(xl, -1e9) / TILE));
             xb = min(xb, (int)floor(fmin(xr, 1e9) / TILE) + 1);
+            if (WANT_BLOCKS && xa < xb) {
+#pragma unroll
+                for (int sb = 0; sb < TILE / BLK_H; ++sb) {
+                    const int ya = y * TILE + sb * BLK_H;
+                    double u = 1e300, v = -1e300;  // empty band
+                    if (ya <= geo.H - 1 && ellipse_row_range(E, ya, min(ya + BLK_H - 1, geo.H - 1), u, v) &&
+                        !(u <= v)) {
+                        u = -1e300;  // NaN: keep the whole band
+                        v = 1e300;
+                    }
+                    bl[sb] = u;
+                    br[sb] = v;
+                }
+            }
         }
         for (int x = xa; x < xb; ++x) {
-            fn(geo.tile_off + y * geo.tx + x, n);
+            unsigned blocks = 0xffu;
+            if (WANT_BLOCKS && E.ok) {
+                blocks = 0u;
+#pragma unroll
+                for (int sb = 0; sb < TILE / BLK_H; ++sb)
+#pragma unroll
+                    for (int bx = 0; bx < TILE / BLK_W; ++bx) {
+                        const double c0 = (double)(x * TILE + bx * BLK_W), c1 = c0 + (BLK_W - 1);
+                        if (bl[sb] <= c1 && br[sb] >= c0) blocks |= 1u << (sb * (TILE / BLK_W) + bx);
+                    }
+            }
+            fn(geo.tile_off + y * geo.tx + x, n, blocks);
             ++n;
         }
     }
@@ -494,8 +533,8 @@ task_count_kernel(const long long* __restrict__ header, const us3d_slice_frame* 
         const int2 gf = task_gf[k];
         const float4 a = pack[3 * (int64_t)gf.x], b = pack[3 * (int64_t)gf.x + 1], c = pack[3 * (int64_t)gf.x + 2];
         const Geo geo = load_geo(frames + gf.y);
-        task_ntiles[k] = task_tiles(task_rect[k], geo, a, b, c, chi2, beta, frame_dev,
-                                    [&](int t, int) { atomicAdd(&tile_count[t], 1); });
+        task_ntiles[k] = task_tiles<false>(task_rect[k], geo, a, b, c, chi2, beta, frame_dev,
+                                           [&](int t, int, unsigned) { atomicAdd(&tile_count[t], 1); });
     }
 }
 
@@ -512,7 +551,8 @@ task_scatter_kernel(const long long* __restrict__ header, const us3d_slice_frame
                     const unsigned* __restrict__ frame_dev, const int4* __restrict__ task_rect,
                     const int2* __restrict__ task_gf, const float* __restrict__ task_v,
                     const int* __restrict__ task_inst, const int* __restrict__ tile_start, int* __restrict__ tile_cursor,
-                    unsigned long long* __restrict__ keys, int* __restrict__ slot_inst) {
+                    unsigned long long* __restrict__ keys, int* __restrict__ slot_inst,
+                    unsigned char* __restrict__ slot_mask) {
     if (header[H_FLAGS] != 0) return;
     const long long nt = header[H_NTASK];
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += (long long)gridDim.x * blockDim.x) {
@@ -522,11 +562,12 @@ task_scatter_kernel(const long long* __restrict__ header, const us3d_slice_frame
         const unsigned long long key =
             ((unsigned long long)depth_key(task_v[k], sort_by_depth) << 32) | (unsigned long long)(uint32_t)gf.x;
         const int i0 = task_inst[k];
-        task_tiles(task_rect[k], geo, a, b, c, chi2, beta, frame_dev, [&](int t, int i) {
+        task_tiles<true>(task_rect[k], geo, a, b, c, chi2, beta, frame_dev, [&](int t, int i, unsigned blocks) {
             const int slot = tile_start[t] + atomicAdd(&tile_cursor[t], 1);
             if (slot >= tile_start[t + 1]) return;  // never outside the bucket (verify_kernel flags it)
             keys[slot] = key;
             slot_inst[slot] = i0 + i;
+            slot_mask[slot] = (unsigned char)blocks;
         });
     }
 }
@@ -616,22 +657,29 @@ __device__ __forceinline__ int find_tile_coords(const Geo& geo, int64_t t, int& 
     return lt;
 }
 
+// Pixel (column, row) within its tile of thread / slot k: warp-block-major order.
+__device__ __forceinline__ int block_col(int k) { return ((k >> 5) & 1) * BLK_W + (k & (BLK_W - 1)); }
+__device__ __forceinline__ int block_row(int k) { return (k >> 6) * BLK_H + ((k & 31) >> 3); }
+
+// One block per tile, one thread per pixel; warp w owns warp block w of the tile and visits
+// only the staged Gaussians whose block mask has bit w (the others reach none of its pixels).
 __global__ void __launch_bounds__(TILE_PIX, US3D_UG_FWD_MIN_CTAS)
 forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
-               const long long* __restrict__ header, const float4* __restrict__ pack,
-               const float* __restrict__ pixels, float chi2, float beta, float bg_alpha,
-               float bg_intensity, float* __restrict__ out_image, float* __restrict__ out_alpha,
-               float* __restrict__ out_depth, int* __restrict__ out_counts,
-               float2* __restrict__ pixel_aux) {
+               const unsigned char* __restrict__ sorted_mask, const long long* __restrict__ header,
+               const float4* __restrict__ pack, const float* __restrict__ pixels, float chi2, float beta,
+               float bg_alpha, float bg_intensity, float* __restrict__ out_image, float* __restrict__ out_alpha,
+               float* __restrict__ out_depth, int* __restrict__ out_counts, float2* __restrict__ pixel_aux) {
     __shared__ Staged sg[FWD_BATCH];
+    __shared__ unsigned char s_blocks[FWD_BATCH];
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
     const Geo geo = load_geo(frames + tile_frame[t]);
     int tx, ty;
     find_tile_coords(geo, t, tx, ty);
-    const int px = tx * TILE + (threadIdx.x & (TILE - 1));
-    const int py = ty * TILE + (threadIdx.x / TILE);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int px = tx * TILE + block_col(threadIdx.x);
+    const int py = ty * TILE + block_row(threadIdx.x);
     const int64_t p = (int64_t)geo.pix_off + (int64_t)py * geo.W + px;
     const bool valid = px < geo.W && py < geo.H && p < P;
     float3 pv = make_float3(0.f, 0.f, 0.f);
@@ -644,11 +692,18 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     for (int b0 = 0; b0 < n; b0 += FWD_BATCH) {
         const int nb = min(FWD_BATCH, n - b0);
         __syncthreads();
-        for (int j = threadIdx.x; j < nb; j += blockDim.x)
+        for (int j = threadIdx.x; j < nb; j += blockDim.x) {
             sg[j] = stage_gaussian(pack, sorted_gid[s0 + b0 + j], geo, chi2, beta);
+            s_blocks[j] = sorted_mask[s0 + b0 + j];
+        }
         __syncthreads();
-        if (valid) {
-            for (int j = 0; j < nb; ++j) {
+        // Lanes of an invalid pixel run along (their sums are never stored).
+        for (int jc = 0; jc < nb; jc += 32) {
+            const int jl = jc + lane;
+            unsigned bits = __ballot_sync(0xffffffffu, jl < nb && ((s_blocks[jl] >> warp) & 1u));
+            while (bits != 0u) {
+                const int j = jc + __ffs(bits) - 1;
+                bits &= bits - 1u;
                 const float4 q0 = sg[j].q0;
                 const float4 q3 = sg[j].q3;
                 const float3 d = make_float3(pv.x - q0.x, pv.y - q0.y, pv.z - q0.z);
@@ -680,19 +735,26 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     pixel_aux[p] = make_float2(sc_ns, sd_ns);
 }
 
-// One block per tile; thread k owns instance k of the tile list (strided by the block) and
-// sweeps the tile's pixels, which sit in shared memory with their upstream coefficients.
+// One block per tile; each thread owns one instance of the tile list at a time and sweeps the
+// pixels of the warp blocks its mask marks (pixels and their upstream coefficients sit in
+// shared memory in warp-block-major order). Instances are regrouped by the number of marked
+// blocks so that the lanes of a warp do similar amounts of work; every instance's sums run
+// over its blocks in ascending order, pixel order within block b rotated by b (conflict-free
+// shared-memory reads across lanes in different blocks), so its partial does not depend on
+// the grouping, and blocks without a contributing pixel add nothing.
 __global__ void __launch_bounds__(TILE_PIX, US3D_UG_BWD_MIN_CTAS)
 backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                 const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
-                const int* __restrict__ sorted_inst, const long long* __restrict__ header,
-                const float4* __restrict__ pack, const float* __restrict__ pixels,
-                const float* __restrict__ d_image, const float* __restrict__ d_alpha,
+                const int* __restrict__ sorted_inst, const unsigned char* __restrict__ sorted_mask,
+                const long long* __restrict__ header, const float4* __restrict__ pack,
+                const float* __restrict__ pixels, const float* __restrict__ d_image, const float* __restrict__ d_alpha,
                 const float* __restrict__ d_depth, const float* __restrict__ saved_alpha,
                 const float2* __restrict__ pixel_aux, float chi2, float beta, float bg_alpha,
                 float bg_intensity, float4* __restrict__ partial) {
     __shared__ float4 s_pa[TILE_PIX];  // pixel position, dL/dnum
     __shared__ float4 s_pb[TILE_PIX];  // dL/dalpha_total + dL/dsum_alpha (depth), dL/ddepth_weighted
+    __shared__ short s_perm[BWD_CHUNK];
+    __shared__ int s_class[9];
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0) return;
     const int s0 = tile_start[t];
@@ -701,87 +763,117 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
     const Geo geo = load_geo(frames + tile_frame[t]);
     int tx, ty;
     find_tile_coords(geo, t, tx, ty);
-    const int rows = min(TILE, geo.H - ty * TILE);
-    const int cols = min(TILE, geo.W - tx * TILE);
-    const int nv = rows * cols;
-    if (threadIdx.x < nv) {
-        const int r = threadIdx.x / cols, c = threadIdx.x - (threadIdx.x / cols) * cols;
+    {
+        const int r = block_row(threadIdx.x), c = block_col(threadIdx.x);
         const int64_t p = (int64_t)geo.pix_off + (int64_t)(ty * TILE + r) * geo.W + (tx * TILE + c);
-        // Per-pixel adjoint coefficients (reference src/shader/backward.cu:175-197).
-        const float sum_alpha = saved_alpha[p] - bg_alpha;
-        const float2 aux = pixel_aux[p];
-        const float alpha_total = sum_alpha + bg_alpha;
-        const float inv_alpha = 1.0f / fmaxf(alpha_total, 1e-8f);
-        const float num = aux.x + bg_alpha * bg_intensity;
-        const float gI = d_image[p], gA = d_alpha[p], gD = d_depth[p];
-        const float dnum = gI * inv_alpha;
-        const float dtot = gA - gI * num * inv_alpha * inv_alpha;
-        const float inv_sa = 1.0f / fmaxf(sum_alpha, 1e-8f);
-        const float ddw = gD * inv_sa;
-        const float dsad = -gD * aux.y * inv_sa * inv_sa;
-        s_pa[threadIdx.x] = make_float4(pixels[3 * p], pixels[3 * p + 1], pixels[3 * p + 2], dnum);
-        s_pb[threadIdx.x] = make_float4(dtot + dsad, ddw, 0.f, 0.f);
-    }
-    __syncthreads();
-
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int g = sorted_gid[s0 + k];
-        const int inst = sorted_inst[s0 + k];
-        const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
-        float4 q1;
-        float s12, s22;
-        precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
-        const float3 m = make_float3(a.x, a.y, a.z);
-        const float dterm = f3_dot(f3_sub(m, geo.o), geo.ele);
-        float r_lat, r_ax, r_ele;
-        window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax, r_ele);
-        const float o = a.w, ci = c.z;
-        float acc_c = 0.f, acc_o = 0.f, acc_e = 0.f;
-        float sdx = 0.f, sdy = 0.f, sdz = 0.f;
-        float sxx = 0.f, sxy = 0.f, sxz = 0.f, syy = 0.f, syz = 0.f, szz = 0.f;
-        for (int j = 0; j < nv; ++j) {
-            const float4 pa = s_pa[j];
-            const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
-            if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
-            const float q = quad_form(d, q1, s12, s22);
-            if (q > chi2) continue;
-            const float4 pb = s_pb[j];
-            const float w = __expf(-0.5f * q);
-            const float ah = o * w;
-            const float dah = pa.w * ci + pb.x + pb.y * dterm;
-            acc_c += pa.w * ah;
-            acc_o += dah * w;
-            acc_e += pb.y * ah;
-            const float dq = -0.5f * dah * ah;
-            const float ux = dq * d.x, uy = dq * d.y, uz = dq * d.z;
-            sdx += ux;
-            sdy += uy;
-            sdz += uz;
-            sxx += ux * d.x;
-            sxy += ux * d.y;
-            sxz += ux * d.z;
-            syy += uy * d.y;
-            syz += uy * d.z;
-            szz += uz * d.z;
+        if (ty * TILE + r < geo.H && tx * TILE + c < geo.W && p < P) {
+            // Per-pixel adjoint coefficients (reference src/shader/backward.cu:175-197).
+            const float sum_alpha = saved_alpha[p] - bg_alpha;
+            const float2 aux = pixel_aux[p];
+            const float alpha_total = sum_alpha + bg_alpha;
+            const float inv_alpha = 1.0f / fmaxf(alpha_total, 1e-8f);
+            const float num = aux.x + bg_alpha * bg_intensity;
+            const float gI = d_image[p], gA = d_alpha[p], gD = d_depth[p];
+            const float dnum = gI * inv_alpha;
+            const float dtot = gA - gI * num * inv_alpha * inv_alpha;
+            const float inv_sa = 1.0f / fmaxf(sum_alpha, 1e-8f);
+            const float ddw = gD * inv_sa;
+            const float dsad = -gD * aux.y * inv_sa * inv_sa;
+            s_pa[threadIdx.x] = make_float4(pixels[3 * p], pixels[3 * p + 1], pixels[3 * p + 2], dnum);
+            s_pb[threadIdx.x] = make_float4(dtot + dsad, ddw, 0.f, 0.f);
+        } else {
+            // outside the frame: zero coefficients make every term of this slot vanish
+            s_pa[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s_pb[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        // d/dmean = -2 Lambda sum(dq d) + sum(ddw * ah) * ele (reference backward.cu:218-228).
-        const float vx = q1.x * sdx + q1.y * sdy + q1.z * sdz;
-        const float vy = q1.y * sdx + q1.w * sdy + s12 * sdz;
-        const float vz = q1.z * sdx + s12 * sdy + s22 * sdz;
-        // dL/dL (lower triangle) from dL/dLambda = sum(dq d d^T) (reference backward.cu:230-255).
-        const float l11 = b.x * b.x + beta, l12 = b.y, l13 = b.z;
-        const float l22 = b.w * b.w + beta, l23 = c.x, l33 = c.y * c.y + beta;
-        const float dl11 = 2.0f * (sxx * l11 + sxy * l12 + sxz * l13);
-        const float dl12 = 2.0f * (sxy * l11 + syy * l12 + syz * l13);
-        const float dl13 = 2.0f * (sxz * l11 + syz * l12 + szz * l13);
-        const float dl22 = 2.0f * (syy * l22 + syz * l23);
-        const float dl23 = 2.0f * (syz * l22 + szz * l23);
-        const float dl33 = 2.0f * (szz * l33);
-        float4* out = partial + 3 * (int64_t)inst;
-        out[0] = make_float4(-2.0f * vx + acc_e * geo.ele.x, -2.0f * vy + acc_e * geo.ele.y,
-                             -2.0f * vz + acc_e * geo.ele.z, acc_o);
-        out[1] = make_float4(dl11 * (2.0f * b.x), dl12, dl13, dl22 * (2.0f * b.w));
-        out[2] = make_float4(dl23, dl33 * (2.0f * c.y), acc_c, 0.f);
+    }
+
+    for (int c0 = 0; c0 < n; c0 += BWD_CHUNK) {
+        const int nc = min(BWD_CHUNK, n - c0);
+        if (threadIdx.x < 9) s_class[threadIdx.x] = 0;
+        __syncthreads();
+        for (int k = threadIdx.x; k < nc; k += blockDim.x)
+            atomicAdd(&s_class[8 - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int i = 0; i < 9; ++i) {
+                const int v = s_class[i];
+                s_class[i] = acc;
+                acc += v;
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < nc; k += blockDim.x)
+            s_perm[atomicAdd(&s_class[8 - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1)] = (short)k;
+        __syncthreads();
+
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+            const int k = s0 + c0 + s_perm[i];
+            const int g = sorted_gid[k];
+            const int inst = sorted_inst[k];
+            const unsigned blocks = sorted_mask[k];
+            const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+            float4 q1;
+            float s12, s22;
+            precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
+            const float3 m = make_float3(a.x, a.y, a.z);
+            const float dterm = f3_dot(f3_sub(m, geo.o), geo.ele);
+            float r_lat, r_ax, r_ele;
+            window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax, r_ele);
+            const float o = a.w, ci = c.z;
+            float acc_c = 0.f, acc_o = 0.f, acc_e = 0.f;
+            float sdx = 0.f, sdy = 0.f, sdz = 0.f;
+            float sxx = 0.f, sxy = 0.f, sxz = 0.f, syy = 0.f, syz = 0.f, szz = 0.f;
+            for (unsigned mb = blocks; mb != 0u; mb &= mb - 1u) {
+                const int blk = __ffs(mb) - 1;
+                for (int jj = 0; jj < 32; ++jj) {
+                    const int j = blk * 32 + ((jj + blk) & 31);
+                    const float4 pa = s_pa[j];
+                    const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
+                    if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
+                    const float q = quad_form(d, q1, s12, s22);
+                    if (q > chi2) continue;
+                    const float4 pb = s_pb[j];
+                    const float w = __expf(-0.5f * q);
+                    const float ah = o * w;
+                    const float dah = pa.w * ci + pb.x + pb.y * dterm;
+                    acc_c += pa.w * ah;
+                    acc_o += dah * w;
+                    acc_e += pb.y * ah;
+                    const float dq = -0.5f * dah * ah;
+                    const float ux = dq * d.x, uy = dq * d.y, uz = dq * d.z;
+                    sdx += ux;
+                    sdy += uy;
+                    sdz += uz;
+                    sxx += ux * d.x;
+                    sxy += ux * d.y;
+                    sxz += ux * d.z;
+                    syy += uy * d.y;
+                    syz += uy * d.z;
+                    szz += uz * d.z;
+                }
+            }
+            // d/dmean = -2 Lambda sum(dq d) + sum(ddw * ah) * ele (reference backward.cu:218-228).
+            const float vx = q1.x * sdx + q1.y * sdy + q1.z * sdz;
+            const float vy = q1.y * sdx + q1.w * sdy + s12 * sdz;
+            const float vz = q1.z * sdx + s12 * sdy + s22 * sdz;
+            // dL/dL (lower triangle) from dL/dLambda = sum(dq d d^T) (reference backward.cu:230-255).
+            const float l11 = b.x * b.x + beta, l12 = b.y, l13 = b.z;
+            const float l22 = b.w * b.w + beta, l23 = c.x, l33 = c.y * c.y + beta;
+            const float dl11 = 2.0f * (sxx * l11 + sxy * l12 + sxz * l13);
+            const float dl12 = 2.0f * (sxy * l11 + syy * l12 + syz * l13);
+            const float dl13 = 2.0f * (sxz * l11 + syz * l12 + szz * l13);
+            const float dl22 = 2.0f * (syy * l22 + syz * l23);
+            const float dl23 = 2.0f * (syz * l22 + szz * l23);
+            const float dl33 = 2.0f * (szz * l33);
+            float4* out = partial + 3 * (int64_t)inst;
+            out[0] = make_float4(-2.0f * vx + acc_e * geo.ele.x, -2.0f * vy + acc_e * geo.ele.y,
+                                 -2.0f * vz + acc_e * geo.ele.z, acc_o);
+            out[1] = make_float4(dl11 * (2.0f * b.x), dl12, dl13, dl22 * (2.0f * b.w));
+            out[2] = make_float4(dl23, dl33 * (2.0f * c.y), acc_c, 0.f);
+        }
+        __syncthreads();
     }
 }
 
@@ -977,7 +1069,7 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
     if (n_gauss > 0) {
         task_scatter_kernel<<<tb, 128, 0, stream>>>(w.header, frames, w.pack, chi2, beta, sort_by_depth, tdev,
                                                     w.task_rect, w.task_gf, w.task_v, w.task_inst, w.tile_start,
-                                                    w.tile_cursor, w.keys, w.slot_inst);
+                                                    w.tile_cursor, w.keys, w.slot_inst, w.slot_mask);
         US3D_CHECK_LAUNCH("ug scatter");
     }
     if (n_tiles > 0)
@@ -985,7 +1077,7 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
                                                                               w.header);
     if (n_tiles > 0) {
         US3D_CHECK_CUDA(launch_tile_sort(n_tiles, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid,
-                                         w.sorted_inst, g_sort_attr_done, stream));
+                                         w.sorted_inst, g_sort_attr_done, stream, w.slot_mask, w.sorted_mask));
     }
     prof_end(prof, stream);
     count_launches(1 + (n_frames > 0) + (slice_cull && n_tiles > 0) + 4 * (n_gauss > 0) + 9 + 3 + (n_gauss > 0) +
@@ -1024,8 +1116,8 @@ extern "C" int us3d_ug_forward(void* workspace, const us3d_slice_frame* frames, 
     cudaStream_t stream = (cudaStream_t)stream_;
     const int prof = prof_begin("ug_forward", stream);
     forward_kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(
-        n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.header, w.pack, pixels, chi2, beta,
-        bg_alpha, bg_intensity, out_image, out_alpha, out_depth, out_counts, w.pixel_aux);
+        n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_mask, w.header, w.pack, pixels,
+        chi2, beta, bg_alpha, bg_intensity, out_image, out_alpha, out_depth, out_counts, w.pixel_aux);
     US3D_CHECK_LAUNCH("ug forward");
     prof_end(prof, stream);
     count_launches(1);
@@ -1054,8 +1146,9 @@ extern "C" int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames,
     const int prof = prof_begin("ug_backward", stream);
     if (n_tiles > 0) {
         backward_kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(
-            n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_inst, w.header, w.pack,
-            pixels, d_image, d_alpha, d_depth, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha, bg_intensity, partial);
+            n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_inst, w.sorted_mask, w.header,
+            w.pack, pixels, d_image, d_alpha, d_depth, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha, bg_intensity,
+            partial);
         US3D_CHECK_LAUNCH("ug backward");
     }
     if (n_gauss > 0) {
