@@ -318,7 +318,7 @@ def run_b200(a):
         out["batched_over_plain"] = round(value / plain_value, 3)
 
     if not a.no_e2e:
-        out["e2e"] = run_e2e(a, dev, sc, specs, n_pool, world, rank, timed)
+        out["e2e"] = run_e2e(a, dev, sc, specs, n_pool, world, rank, barrier)
 
     if rank == 0 and world == 1 and not a.no_cpu:
         out["cpu_baseline"] = cpu_baseline(a, sc, specs)
@@ -329,18 +329,20 @@ def run_b200(a):
         print(json.dumps(out), flush=True)
 
 
-def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed):
+def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
     """End to end through the public autograd API: every step copies its inputs (Gaussian
     parameters, pixel positions, targets) from pinned host memory and reads its loss and
     gradients back. The next step's inputs are copied on a second stream while the current
-    step computes (double buffering); after a synchronised priming pass the renderers run
-    without a per-step instance-total readback, and their overflow flags are checked after
-    the timed region."""
+    step computes (double buffering), and a step's loss and gradients go back to the host on a
+    third stream while the next step computes; the timed region ends after the last of those
+    copies. After a synchronised priming pass the renderers run without a per-step
+    instance-total readback, and their overflow flags are checked after the timed region."""
     import torch
 
     from us3d_b200 import scenes
     from us3d_b200 import ultragauss as UG
     from us3d_b200.batch import UltraGaussBatchRenderer
+    from us3d_b200.dist import max_over_ranks
 
     F = a.frames_per_step
     P1 = a.size * a.size
@@ -355,6 +357,7 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed):
     grad_host = [torch.empty_like(x).pin_memory() for x in host]
     loss_host = torch.empty((), dtype=torch.float32).pin_memory()
     copy_stream = torch.cuda.Stream(device=dev)
+    d2h_stream = torch.cuda.Stream(device=dev)
     compute = torch.cuda.current_stream()
     slots = [dict(step=-1, ready=torch.cuda.Event(), free=torch.cuda.Event()) for _ in range(2)]
 
@@ -383,10 +386,45 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed):
         img, alpha, depth = renderers[i % len(renderers)](*ps, pix)
         loss = (img - tgt).abs().mean()
         loss.backward()
-        loss_host.copy_(loss.detach(), non_blocking=True)
-        for gh, p in zip(grad_host, ps):
-            gh.copy_(p.grad, non_blocking=True)
+        outs = [loss.detach()] + [p.grad for p in ps]
+        done = torch.cuda.Event()
+        done.record(compute)
+        with torch.cuda.stream(d2h_stream):
+            d2h_stream.wait_event(done)
+            loss_host.copy_(outs[0], non_blocking=True)
+            for gh, g in zip(grad_host, outs[1:]):
+                gh.copy_(g, non_blocking=True)
+            for t in outs:
+                t.record_stream(d2h_stream)
         sl["free"].record(compute)
+
+    def timed_e2e(steps, warm):
+        for i in range(warm):
+            step(i)
+        compute.wait_stream(d2h_stream)
+        timed_barrier()
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st.record(compute)
+        for i in range(steps):
+            step(warm + i)
+        compute.wait_stream(d2h_stream)  # the last step's results have reached the host
+        en.record(compute)
+        timed_barrier()
+        return max_over_ranks(st.elapsed_time(en), device=dev)
+
+    # pinned-memory copy bandwidth of this machine, one transfer of a step's inputs each way
+    probe = torch.empty(sum(x.numel() for x in host) + 2 * F * P1 * 4, dtype=torch.float32).pin_memory()
+    probe_dev = torch.empty(probe.shape, dtype=torch.float32, device=dev)
+    link = {}
+    for name, dst, src in (("h2d", probe_dev, probe), ("d2h", probe, probe_dev)):
+        dst.copy_(src, non_blocking=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        link[name] = round(probe.numel() * 4 / (e0.elapsed_time(e1) / 1e3) / 1e9, 1)
+    del probe, probe_dev
 
     # priming: one synchronised call per renderer fixes the instance capacity
     cap = 0
@@ -396,7 +434,7 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed):
     for r in renderers:
         r.params["capacity"] = cap
         r.params["sync_check"] = False
-    ms = timed(step, a.steps, a.warmup)
+    ms = timed_e2e(a.steps, a.warmup)
     for r in renderers:
         if "binning" in r.last:
             total, flags = UG.read_status(r.last["binning"])
@@ -406,7 +444,8 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed):
     d2h = 4 + sum(x.numel() * x.element_size() for x in host)
     return {"value": round(a.steps * F * world / (ms / 1e3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "api": "us3d_b200.batch.UltraGaussBatchRenderer (autograd)",
-            "copies": "next step's inputs prefetched on a second stream (double buffered)"}
+            "copies": "next step's inputs prefetched on a second stream (double buffered); results read back on a "
+                      "third stream", "pinned_copy_gbs": link}
 
 
 def cpu_baseline(a, sc, specs, frames: int = 1):

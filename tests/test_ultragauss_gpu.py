@@ -318,6 +318,27 @@ def _cull_case(dev, G=120000, sizes=((256, 256, 0.125), (200, 330, 0.2), (128, 9
     return args, UG.build_frame_table(specs, dev), torch.cat(pix).to(dev), torch.cat(grads, dim=1).to(dev)
 
 
+def test_culled_batched_deterministic(cuda_device):
+    """Slice-culled batched binning + forward + backward, three times, each on device memory
+    that held random bytes just before (freed to the caching allocator, so the workspace
+    reuses it): images and gradients are bit-identical, i.e. nothing reads memory that the
+    step did not write and no result depends on the order of atomic updates."""
+    from us3d_b200 import ultragauss as UG
+
+    args, ft, pix, grads = _cull_case(cuda_device, G=200000)
+    runs = []
+    for r in range(3):
+        junk = torch.randint(0, 256, (int(3e8),), dtype=torch.uint8, device=cuda_device)
+        del junk
+        b = UG.bin_gaussians(*args, ft, 7.815, 1e-4, True, slice_cull_pixels=pix)
+        img, alpha, depth, _ = UG.forward(b, pix, 1e-6, 0.0, want_counts=False)
+        g = UG.backward(b, pix, grads[0], grads[1], grads[2], alpha, 1e-6, 0.0)
+        runs.append([x.cpu().numpy() for x in (img, alpha, depth, *g)])
+    for r in runs[1:]:
+        for x, y in zip(runs[0], r):
+            assert np.array_equal(x, y)
+
+
 @pytest.mark.parametrize("jitter,scale", [(0.0, 1.0), (0.0, 0.3), (2e-3, 1.0), (0.5, 1.0)])
 def test_slice_cull_identical_results(jitter, scale, cuda_device):
     """A slice-culled binning keeps fewer instances but gives bit-identical images, alpha,

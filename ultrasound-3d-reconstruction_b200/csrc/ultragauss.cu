@@ -31,17 +31,25 @@
 namespace us3d {
 namespace ug {
 
-// Resident CTAs per SM the shading kernels are compiled for (register budget 65536 / (256 x n)).
+// Threads of a backward CTA, and resident CTAs per SM the shading kernels are compiled for
+// (register budget 65536 / (threads x n)); Gaussians staged per forward batch.
+#ifndef US3D_UG_BWD_THREADS
+#define US3D_UG_BWD_THREADS 256
+#endif
 #ifndef US3D_UG_FWD_MIN_CTAS
 #define US3D_UG_FWD_MIN_CTAS 5
 #endif
 #ifndef US3D_UG_BWD_MIN_CTAS
-#define US3D_UG_BWD_MIN_CTAS 4
+#define US3D_UG_BWD_MIN_CTAS (1024 / US3D_UG_BWD_THREADS)
+#endif
+#ifndef US3D_UG_FWD_BATCH
+#define US3D_UG_FWD_BATCH 512
 #endif
 
 constexpr int TILE = 16;           // reference SLICE_TILE_SIZE (include/mapper/core.cuh:5)
 constexpr int TILE_PIX = TILE * TILE;
-constexpr int FWD_BATCH = 256;       // Gaussians staged per shared-memory batch
+constexpr int FWD_BATCH = US3D_UG_FWD_BATCH;  // Gaussians staged per shared-memory batch
+constexpr int BWD_THREADS = US3D_UG_BWD_THREADS;
 // A tile's pixels are shaded by 8 warps, each owning a block of 8 columns x 4 rows; bit
 // (band * 2 + half) of an instance's block mask is set when the Gaussian can reach block
 // (4-row band `band`, 8-column half `half`) of that tile.
@@ -689,6 +697,27 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
 
     int cnt = 0;
     float sa = 0.f, sc = 0.f, sd = 0.f, sc_ns = 0.f, sd_ns = 0.f;
+    auto shade = [&](int j) {
+        const float4 q0 = sg[j].q0;
+        const float4 q3 = sg[j].q3;
+        const float3 d = make_float3(pv.x - q0.x, pv.y - q0.y, pv.z - q0.z);
+        if (!window_hit(d, geo.lat, geo.ax, q3.x, q3.y)) return;
+        ++cnt;
+        const float4 q1 = sg[j].q1;
+        const float4 q2 = sg[j].q2;
+        const float q = quad_form(d, q1, q2.x, q2.y);
+        if (q > chi2) return;
+        const float w = __expf(-0.5f * q);
+        const float ah = q0.w * w;
+        sc_ns += ah * q2.z;
+        sd_ns += ah * q2.w;
+        if (ah <= 1e-8f) return;
+        sa += ah;
+        sc += ah * q2.z;
+        sd += ah * q2.w;
+    };
+    // Without a slice cull every mask is full: plain sweep, same order and sums.
+    const bool culled = header[H_MODE] != 0;
     for (int b0 = 0; b0 < n; b0 += FWD_BATCH) {
         const int nb = min(FWD_BATCH, n - b0);
         __syncthreads();
@@ -698,29 +727,17 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
         }
         __syncthreads();
         // Lanes of an invalid pixel run along (their sums are never stored).
+        if (!culled) {
+            for (int j = 0; j < nb; ++j) shade(j);
+            continue;
+        }
         for (int jc = 0; jc < nb; jc += 32) {
             const int jl = jc + lane;
             unsigned bits = __ballot_sync(0xffffffffu, jl < nb && ((s_blocks[jl] >> warp) & 1u));
             while (bits != 0u) {
                 const int j = jc + __ffs(bits) - 1;
                 bits &= bits - 1u;
-                const float4 q0 = sg[j].q0;
-                const float4 q3 = sg[j].q3;
-                const float3 d = make_float3(pv.x - q0.x, pv.y - q0.y, pv.z - q0.z);
-                if (!window_hit(d, geo.lat, geo.ax, q3.x, q3.y)) continue;
-                ++cnt;
-                const float4 q1 = sg[j].q1;
-                const float4 q2 = sg[j].q2;
-                const float q = quad_form(d, q1, q2.x, q2.y);
-                if (q > chi2) continue;
-                const float w = __expf(-0.5f * q);
-                const float ah = q0.w * w;
-                sc_ns += ah * q2.z;
-                sd_ns += ah * q2.w;
-                if (ah <= 1e-8f) continue;
-                sa += ah;
-                sc += ah * q2.z;
-                sd += ah * q2.w;
+                shade(j);
             }
         }
     }
@@ -742,7 +759,7 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
 // over its blocks in ascending order, pixel order within block b rotated by b (conflict-free
 // shared-memory reads across lanes in different blocks), so its partial does not depend on
 // the grouping, and blocks without a contributing pixel add nothing.
-__global__ void __launch_bounds__(TILE_PIX, US3D_UG_BWD_MIN_CTAS)
+__global__ void __launch_bounds__(BWD_THREADS, US3D_UG_BWD_MIN_CTAS)
 backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                 const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
                 const int* __restrict__ sorted_inst, const unsigned char* __restrict__ sorted_mask,
@@ -751,8 +768,10 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
                 const float* __restrict__ d_depth, const float* __restrict__ saved_alpha,
                 const float2* __restrict__ pixel_aux, float chi2, float beta, float bg_alpha,
                 float bg_intensity, float4* __restrict__ partial) {
-    __shared__ float4 s_pa[TILE_PIX];  // pixel position, dL/dnum
-    __shared__ float4 s_pb[TILE_PIX];  // dL/dalpha_total + dL/dsum_alpha (depth), dL/ddepth_weighted
+    // Per warp block b, entries [64 b, 64 b + 64) hold its 32 pixels twice, so that the sweep
+    // rotated by b reads 32 consecutive entries from 65 b.
+    __shared__ float4 s_pa[2 * TILE_PIX];  // pixel position, dL/dnum
+    __shared__ float2 s_pb[2 * TILE_PIX];  // dL/dalpha_total + dL/dsum_alpha (depth), dL/ddepth_weighted
     __shared__ short s_perm[BWD_CHUNK];
     __shared__ int s_class[9];
     const int64_t t = blockIdx.x;
@@ -763,8 +782,9 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
     const Geo geo = load_geo(frames + tile_frame[t]);
     int tx, ty;
     find_tile_coords(geo, t, tx, ty);
-    {
-        const int r = block_row(threadIdx.x), c = block_col(threadIdx.x);
+    for (int slot = threadIdx.x; slot < TILE_PIX; slot += BWD_THREADS) {
+        const int r = block_row(slot), c = block_col(slot);
+        const int e0 = (slot >> 5) * 64 + (slot & 31), e1 = e0 + 32;
         const int64_t p = (int64_t)geo.pix_off + (int64_t)(ty * TILE + r) * geo.W + (tx * TILE + c);
         if (ty * TILE + r < geo.H && tx * TILE + c < geo.W && p < P) {
             // Per-pixel adjoint coefficients (reference src/shader/backward.cu:175-197).
@@ -779,37 +799,40 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
             const float inv_sa = 1.0f / fmaxf(sum_alpha, 1e-8f);
             const float ddw = gD * inv_sa;
             const float dsad = -gD * aux.y * inv_sa * inv_sa;
-            s_pa[threadIdx.x] = make_float4(pixels[3 * p], pixels[3 * p + 1], pixels[3 * p + 2], dnum);
-            s_pb[threadIdx.x] = make_float4(dtot + dsad, ddw, 0.f, 0.f);
+            s_pa[e0] = s_pa[e1] = make_float4(pixels[3 * p], pixels[3 * p + 1], pixels[3 * p + 2], dnum);
+            s_pb[e0] = s_pb[e1] = make_float2(dtot + dsad, ddw);
         } else {
             // outside the frame: zero coefficients make every term of this slot vanish
-            s_pa[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-            s_pb[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s_pa[e0] = s_pa[e1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s_pb[e0] = s_pb[e1] = make_float2(0.f, 0.f);
         }
     }
+    const bool culled = header[H_MODE] != 0;  // otherwise every mask is full: no regrouping
 
     for (int c0 = 0; c0 < n; c0 += BWD_CHUNK) {
         const int nc = min(BWD_CHUNK, n - c0);
         if (threadIdx.x < 9) s_class[threadIdx.x] = 0;
         __syncthreads();
-        for (int k = threadIdx.x; k < nc; k += blockDim.x)
-            atomicAdd(&s_class[8 - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int acc = 0;
-            for (int i = 0; i < 9; ++i) {
-                const int v = s_class[i];
-                s_class[i] = acc;
-                acc += v;
+        if (culled) {
+            for (int k = threadIdx.x; k < nc; k += blockDim.x)
+                atomicAdd(&s_class[8 - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int acc = 0;
+                for (int i = 0; i < 9; ++i) {
+                    const int v = s_class[i];
+                    s_class[i] = acc;
+                    acc += v;
+                }
             }
+            __syncthreads();
+            for (int k = threadIdx.x; k < nc; k += blockDim.x)
+                s_perm[atomicAdd(&s_class[8 - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1)] = (short)k;
+            __syncthreads();
         }
-        __syncthreads();
-        for (int k = threadIdx.x; k < nc; k += blockDim.x)
-            s_perm[atomicAdd(&s_class[8 - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1)] = (short)k;
-        __syncthreads();
 
         for (int i = threadIdx.x; i < nc; i += blockDim.x) {
-            const int k = s0 + c0 + s_perm[i];
+            const int k = s0 + c0 + (culled ? (int)s_perm[i] : i);
             const int g = sorted_gid[k];
             const int inst = sorted_inst[k];
             const unsigned blocks = sorted_mask[k];
@@ -827,14 +850,16 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
             float sxx = 0.f, sxy = 0.f, sxz = 0.f, syy = 0.f, syz = 0.f, szz = 0.f;
             for (unsigned mb = blocks; mb != 0u; mb &= mb - 1u) {
                 const int blk = __ffs(mb) - 1;
+                const float4* pa_b = s_pa + blk * 65;
+                const float2* pb_b = s_pb + blk * 65;
+#pragma unroll
                 for (int jj = 0; jj < 32; ++jj) {
-                    const int j = blk * 32 + ((jj + blk) & 31);
-                    const float4 pa = s_pa[j];
+                    const float4 pa = pa_b[jj];
                     const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
                     if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
                     const float q = quad_form(d, q1, s12, s22);
                     if (q > chi2) continue;
-                    const float4 pb = s_pb[j];
+                    const float2 pb = pb_b[jj];
                     const float w = __expf(-0.5f * q);
                     const float ah = o * w;
                     const float dah = pa.w * ci + pb.x + pb.y * dterm;
@@ -1145,7 +1170,7 @@ extern "C" int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames,
     float4* partial = reinterpret_cast<float4*>(scratch);
     const int prof = prof_begin("ug_backward", stream);
     if (n_tiles > 0) {
-        backward_kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(
+        backward_kernel<<<(unsigned)n_tiles, BWD_THREADS, 0, stream>>>(
             n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_inst, w.sorted_mask, w.header,
             w.pack, pixels, d_image, d_alpha, d_depth, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha, bg_intensity,
             partial);
