@@ -39,8 +39,8 @@ BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (param
 # DRAM bytes (read + write) per frame of each stage's dominant kernel, from one ncu capture
 # of a 4-frame launch of the same scene, scaled linearly to the frames of a launch.
 NCU_TRAFFIC_PER_FRAME = {
-    "ug_backward": (91.150336e6 + 111.721216e6) / 4,  # backward_kernel, profiles/ultragauss_backward_kernel_4frames.md
-    "ug_forward": (45.9328e6 + 4.483584e6) / 4,       # forward_kernel, profiles/ultragauss_forward_kernel_4frames.md
+    "ug_backward": (98.878464e6 + 115.803392e6) / 4,  # backward_kernel, profiles/ultragauss_backward_kernel_4frames.md
+    "ug_forward": (49.083136e6 + 3.089408e6) / 4,     # forward_kernel, profiles/ultragauss_forward_kernel_4frames.md
 }
 
 
@@ -282,9 +282,9 @@ def run_b200(a):
     G = a.gaussians
     P = P1
     alg = {
-        "ug_backward": G * (BP + BG) + I * 4 + P * (BO + BD),
-        "ug_forward": I * 4 + P * BO,
-        "ug_bin": G * BP + I * 12,
+        "ug_backward": G * (BP + BG) + I * 5 + P * (BO + BD),
+        "ug_forward": I * 5 + P * BO,
+        "ug_bin": G * BP + I * 13,
     }[dominant] * F
     peaks = json.load(open(ROOT / "MEASURED_PEAKS.json")) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
