@@ -310,6 +310,28 @@ def run_b200(a):
                                "the roofline stage times come from this run's CUDA events"},
     }
 
+    # The whole training step of the reference's loop (activations, L1 loss, backward, Adam
+    # over all parameters) on the same batches, forward + loss + backward replayed from a CUDA
+    # graph per batch, Adam one launch; the parameters are raw (logit) copies of the scene's.
+    from us3d_b200.train import TrainConfig, UltraGaussParameters, UltraGaussTrainer
+
+    tp = UltraGaussParameters(params[0].clone(), params[1].clone(), torch.logit(params[2].clamp(1e-6, 1 - 1e-6)),
+                              torch.logit(params[3].clamp(1e-6, 1 - 1e-6)))
+    trainer = UltraGaussTrainer(tp, [(specs[k * F:(k + 1) * F], pix, tgt) for k, (ft, pix, tgt) in enumerate(batches)],
+                                TrainConfig())
+
+    def train_step(i):
+        trainer.step(i % len(batches))
+
+    ms_train = timed(train_step, a.steps, a.warmup)
+    trainer.check()
+    out["train_step"] = {"value": round(a.steps * F * world / (ms_train / 1e3), 3), "unit": UNIT,
+                         "ms_per_step": round(ms_train / a.steps, 4),
+                         "step": "bin (logistic activation fused) + forward + per-frame L1 loss + backward with the "
+                                 "fused loss gradient (CUDA-graph replay) + Adam over all 4 parameter tensors "
+                                 "(one launch)"}
+    del trainer, tp
+
     if not a.no_plain:
         steps_p = max(2, a.steps // 2)
         ms_plain = timed(plain_step, steps_p, 1)

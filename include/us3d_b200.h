@@ -140,6 +140,13 @@ US3D_API int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_sli
  * the full window rectangle).
  */
 #define US3D_UG_BIN_SLICE_CULL 1
+/*
+ * flags |= US3D_UG_BIN_LOGIT_ATTRIBUTES: `opacities` and `intensities` are raw logits and the
+ * binning activates them with the logistic function (the reference's training
+ * parameterisation, GaussianParameters.opacities()/intensities() in pipeline_god_file.py:
+ * 368-372, torch.sigmoid), so that a training step needs no separate activation pass.
+ */
+#define US3D_UG_BIN_LOGIT_ATTRIBUTES 2
 US3D_API int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames_dev,
                             int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
                             const float* means, const float* precision_tril, const float* opacities,
@@ -183,6 +190,66 @@ US3D_API int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames_de
                      float bg_intensity, void* scratch, size_t scratch_bytes,
                      float* d_means, float* d_precision_tril, float* d_opacities,
                      float* d_intensities, void* stream);
+
+/*
+ * Per-frame image loss of the reference's training step (image_loss in
+ * pipeline_god_file.py:606-617 with simple_ssim at :627-637): for each frame f of the table,
+ * loss_f = l1_weight * mean|x - y| + ssim_weight * (1 - SSIM_f), SSIM_f the global SSIM of
+ * the frame's image x against its target y (means, population variances and covariance over
+ * the frame's H*W pixels; c1 = 0.01^2, c2 = 0.03^2). Writes out_stats (n_frames x 8 doubles:
+ * mean x, mean y, var x, var y, cov xy, mean |x - y|, SSIM, loss) and out_coef (n_frames x 4
+ * floats, 16-byte aligned): the per-frame coefficients (a, b, c, d) of dL_f/dx_i =
+ * a*sign(x_i - y_i) + b + c*x_i + d*y_i, which us3d_ug_backward_loss uses. A batch of frames
+ * is trained on the sum of its frames' losses, so every frame keeps the gradient of a
+ * single-frame step. scratch: us3d_ug_loss_scratch_bytes(n_frames) bytes. Deterministic
+ * (fixed-order double-precision reductions); never synchronises. No counterpart in the
+ * reference's CUDA (its loss is PyTorch code).
+ */
+US3D_API size_t us3d_ug_loss_scratch_bytes(int32_t n_frames);
+US3D_API int us3d_ug_loss(const us3d_slice_frame* frames_dev, int32_t n_frames, int64_t n_pixels,
+                          const float* image, const float* target, float l1_weight, float ssim_weight,
+                          void* scratch, size_t scratch_bytes, double* out_stats, float* out_coef, void* stream);
+
+/*
+ * us3d_ug_backward with dL/dimage fused in from the per-frame loss of us3d_ug_loss (image,
+ * target, and its coefficients `loss_coef`), and dL/dalpha = dL/ddepth = 0. Same gradients as
+ * us3d_ug_backward given the loss gradient image, without materialising it. No counterpart
+ * in the reference (there ShaderBackwardCUDA receives the autograd gradient of the PyTorch
+ * loss).
+ */
+US3D_API int us3d_ug_backward_loss(void* workspace, const us3d_slice_frame* frames_dev, int32_t n_frames,
+                                   int64_t n_tiles, int64_t n_pixels, int64_t n_gauss, int64_t instance_capacity,
+                                   const float* pixel_positions, const float* image, const float* target,
+                                   const float* loss_coef, const float* saved_alpha, float chi2_threshold,
+                                   float diag_beta, float bg_alpha, float bg_intensity, void* scratch,
+                                   size_t scratch_bytes, float* d_means, float* d_precision_tril,
+                                   float* d_opacities, float* d_intensities, void* stream);
+
+/*
+ * One Adam step over up to US3D_ADAM_MAX_TENSORS parameter tensors in a single launch,
+ * with torch.optim.Adam's update (defaults: no weight decay, no amsgrad; the optimiser the
+ * reference's training loop uses, pipeline_god_file.py:740,764): m = lerp(m, g, 1 - beta1),
+ * v = beta2 v + (1 - beta2) g^2, p -= lr / (1 - beta1^step) * m / (sqrt(v) / sqrt(1 -
+ * beta2^step) + eps), `step` counted from 1. A tensor with activation
+ * US3D_ADAM_LOGISTIC holds logits whose gradient was taken w.r.t. their logistic
+ * activation: the chain rule g * (1 - s) * s, s = sigmoid(p), is applied first (the
+ * backward of torch.sigmoid). The hyper-parameters are rounded to float once, like torch's
+ * Python-float ones. Never synchronises.
+ */
+#define US3D_ADAM_MAX_TENSORS 8
+#define US3D_ADAM_IDENTITY 0
+#define US3D_ADAM_LOGISTIC 1
+typedef struct us3d_adam_tensor {
+    float* param;
+    const float* grad;
+    float* exp_avg;
+    float* exp_avg_sq;
+    int64_t numel;
+    int32_t activation;
+    int32_t reserved;
+} us3d_adam_tensor;
+US3D_API int us3d_adam_step(const us3d_adam_tensor* tensors, int32_t n_tensors, double lr, double beta1,
+                            double beta2, double eps, int64_t step, void* stream);
 
 /*
  * Per-pixel candidate lists in the reference's CSR layout (pixel_gauss_indices of

@@ -265,17 +265,21 @@ __global__ void setup_kernel(const us3d_slice_frame* __restrict__ frames, int F,
     for (int i = threadIdx.x; i < n; i += blockDim.x) tile_frame[fr.tile_offset + i] = f;
 }
 
+// logits != 0: opacities and intensities are raw logits, activated here by the logistic
+// function (the training parameterisation).
 __global__ void pack_kernel(int64_t G, const float* __restrict__ means, const float* __restrict__ tril,
-                            const float* __restrict__ opac, const float* __restrict__ inten,
+                            const float* __restrict__ opac, const float* __restrict__ inten, int logits,
                             float4* __restrict__ pack) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
     const float* m = means + 3 * g;
     const float2* t = reinterpret_cast<const float2*>(tril + 6 * g);  // 8-byte aligned rows
     const float2 t01 = t[0], t23 = t[1], t45 = t[2];
-    pack[3 * g + 0] = make_float4(m[0], m[1], m[2], opac[g]);
+    const float o = logits ? sigmoid_logit(opac[g]) : opac[g];
+    const float c = logits ? sigmoid_logit(inten[g]) : inten[g];
+    pack[3 * g + 0] = make_float4(m[0], m[1], m[2], o);
     pack[3 * g + 1] = make_float4(t01.x, t01.y, t23.x, t23.y);
-    pack[3 * g + 2] = make_float4(t45.x, t45.y, inten[g], 0.0f);
+    pack[3 * g + 2] = make_float4(t45.x, t45.y, c, 0.0f);
 }
 
 __device__ __forceinline__ void precision_from_raw(float t0, float t1, float t2, float t3, float t4,
@@ -759,6 +763,10 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
 // over its blocks in ascending order, pixel order within block b rotated by b (conflict-free
 // shared-memory reads across lanes in different blocks), so its partial does not depend on
 // the grouping, and blocks without a contributing pixel add nothing.
+// LOSS: dL/dimage comes from the fused per-frame loss (L1 + global SSIM of image against
+// target, coefficients per frame in loss_coef; see us3d_ug_loss) and dL/dalpha = dL/ddepth =
+// 0; otherwise from d_image, d_alpha, d_depth.
+template <bool LOSS>
 __global__ void __launch_bounds__(BWD_THREADS, US3D_UG_BWD_MIN_CTAS)
 backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                 const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
@@ -767,7 +775,8 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
                 const float* __restrict__ pixels, const float* __restrict__ d_image, const float* __restrict__ d_alpha,
                 const float* __restrict__ d_depth, const float* __restrict__ saved_alpha,
                 const float2* __restrict__ pixel_aux, float chi2, float beta, float bg_alpha,
-                float bg_intensity, float4* __restrict__ partial) {
+                float bg_intensity, const float* __restrict__ loss_image, const float* __restrict__ loss_target,
+                const float4* __restrict__ loss_coef, float4* __restrict__ partial) {
     // Per warp block b, entries [64 b, 64 b + 64) hold its 32 pixels twice, so that the sweep
     // rotated by b reads 32 consecutive entries from 65 b.
     __shared__ float4 s_pa[2 * TILE_PIX];  // pixel position, dL/dnum
@@ -793,7 +802,18 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
             const float alpha_total = sum_alpha + bg_alpha;
             const float inv_alpha = 1.0f / fmaxf(alpha_total, 1e-8f);
             const float num = aux.x + bg_alpha * bg_intensity;
-            const float gI = d_image[p], gA = d_alpha[p], gD = d_depth[p];
+            float gI, gA, gD;
+            if (LOSS) {
+                const float x = loss_image[p], y = loss_target[p];
+                const float4 k = loss_coef[tile_frame[t]];
+                gI = k.x * (float)((x > y) - (x < y)) + k.y + k.z * x + k.w * y;
+                gA = 0.f;
+                gD = 0.f;
+            } else {
+                gI = d_image[p];
+                gA = d_alpha[p];
+                gD = d_depth[p];
+            }
             const float dnum = gI * inv_alpha;
             const float dtot = gA - gI * num * inv_alpha * inv_alpha;
             const float inv_sa = 1.0f / fmaxf(sum_alpha, 1e-8f);
@@ -1045,7 +1065,8 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
                               int32_t flags, void* stream_) {
     int st = check_common(frames, n_frames, n_tiles, n_pixels, n_gauss);
     const int slice_cull = (flags & US3D_UG_BIN_SLICE_CULL) ? 1 : 0;
-    US3D_CHECK_ARG((flags & ~US3D_UG_BIN_SLICE_CULL) == 0, "unknown binning flags 0x%x", (unsigned)flags);
+    US3D_CHECK_ARG((flags & ~(US3D_UG_BIN_SLICE_CULL | US3D_UG_BIN_LOGIT_ATTRIBUTES)) == 0,
+                   "unknown binning flags 0x%x", (unsigned)flags);
     US3D_CHECK_ARG(!slice_cull || n_pixels == 0 || pixels != nullptr, "slice cull needs the pixel positions");
     if (st != US3D_OK) return st;
     US3D_CHECK_ARG(workspace != nullptr, "workspace is NULL");
@@ -1071,7 +1092,8 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
     const int64_t tc = task_capacity(cap);
     const unsigned tb = (unsigned)std::min<int64_t>((tc + 127) / 128, 148 * 16);
     if (n_gauss > 0) {
-        pack_kernel<<<gb, 256, 0, stream>>>(n_gauss, means, tril, opac, inten, w.pack);
+        pack_kernel<<<gb, 256, 0, stream>>>(n_gauss, means, tril, opac, inten,
+                                            (flags & US3D_UG_BIN_LOGIT_ATTRIBUTES) ? 1 : 0, w.pack);
         cull_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, nullptr,
                                             tc, w.gtasks, w.task_rect, w.task_gf, w.task_v);
         US3D_CHECK_LAUNCH("ug cull");
@@ -1149,12 +1171,14 @@ extern "C" int us3d_ug_forward(void* workspace, const us3d_slice_frame* frames, 
     return US3D_OK;
 }
 
-extern "C" int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames, int32_t n_frames, int64_t n_tiles,
-                                int64_t n_pixels, int64_t n_gauss, int64_t cap, const float* pixels,
-                                const float* d_image, const float* d_alpha, const float* d_depth,
-                                const float* saved_alpha, float chi2, float beta, float bg_alpha,
-                                float bg_intensity, void* scratch, size_t scratch_bytes, float* d_means,
-                                float* d_tril, float* d_opac, float* d_inten, void* stream_) {
+static int ug_backward_impl(void* workspace, const us3d_slice_frame* frames, int32_t n_frames, int64_t n_tiles,
+                            int64_t n_pixels, int64_t n_gauss, int64_t cap, const float* pixels,
+                            const float* d_image, const float* d_alpha, const float* d_depth,
+                            const float* loss_image, const float* loss_target, const float4* loss_coef,
+                            const float* saved_alpha, float chi2, float beta, float bg_alpha, float bg_intensity,
+                            void* scratch, size_t scratch_bytes, float* d_means, float* d_tril, float* d_opac,
+                            float* d_inten, cudaStream_t stream) {
+    const bool fused = loss_coef != nullptr;
     int st = check_common(frames, n_frames, n_tiles, n_pixels, n_gauss);
     if (st != US3D_OK) return st;
     US3D_CHECK_ARG(workspace != nullptr, "workspace is NULL");
@@ -1163,17 +1187,25 @@ extern "C" int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames,
     US3D_CHECK_ARG(scratch_bytes >= us3d_ug_backward_scratch_bytes(cap), "backward scratch too small: %zu < %zu",
                    scratch_bytes, us3d_ug_backward_scratch_bytes(cap));
     US3D_CHECK_ARG(n_gauss == 0 || (d_means && d_tril && d_opac && d_inten), "gradient pointer is NULL");
-    US3D_CHECK_ARG(n_pixels == 0 || (pixels && d_image && d_alpha && d_depth && saved_alpha),
-                   "input pointer is NULL");
+    if (fused)
+        US3D_CHECK_ARG(n_pixels == 0 || (pixels && loss_image && loss_target && saved_alpha), "input pointer is NULL");
+    else
+        US3D_CHECK_ARG(n_pixels == 0 || (pixels && d_image && d_alpha && d_depth && saved_alpha),
+                       "input pointer is NULL");
     const Workspace w = carve(workspace, n_gauss, n_tiles, n_pixels, cap);
-    cudaStream_t stream = (cudaStream_t)stream_;
     float4* partial = reinterpret_cast<float4*>(scratch);
     const int prof = prof_begin("ug_backward", stream);
     if (n_tiles > 0) {
-        backward_kernel<<<(unsigned)n_tiles, BWD_THREADS, 0, stream>>>(
-            n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_inst, w.sorted_mask, w.header,
-            w.pack, pixels, d_image, d_alpha, d_depth, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha, bg_intensity,
-            partial);
+        if (fused)
+            backward_kernel<true><<<(unsigned)n_tiles, BWD_THREADS, 0, stream>>>(
+                n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_inst, w.sorted_mask,
+                w.header, w.pack, pixels, nullptr, nullptr, nullptr, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha,
+                bg_intensity, loss_image, loss_target, loss_coef, partial);
+        else
+            backward_kernel<false><<<(unsigned)n_tiles, BWD_THREADS, 0, stream>>>(
+                n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_inst, w.sorted_mask,
+                w.header, w.pack, pixels, d_image, d_alpha, d_depth, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha,
+                bg_intensity, nullptr, nullptr, nullptr, partial);
         US3D_CHECK_LAUNCH("ug backward");
     }
     if (n_gauss > 0) {
@@ -1185,6 +1217,31 @@ extern "C" int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames,
     prof_end(prof, stream);
     count_launches((n_tiles > 0) + (n_gauss > 0));
     return US3D_OK;
+}
+
+extern "C" int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames, int32_t n_frames, int64_t n_tiles,
+                                int64_t n_pixels, int64_t n_gauss, int64_t cap, const float* pixels,
+                                const float* d_image, const float* d_alpha, const float* d_depth,
+                                const float* saved_alpha, float chi2, float beta, float bg_alpha,
+                                float bg_intensity, void* scratch, size_t scratch_bytes, float* d_means,
+                                float* d_tril, float* d_opac, float* d_inten, void* stream_) {
+    return ug_backward_impl(workspace, frames, n_frames, n_tiles, n_pixels, n_gauss, cap, pixels, d_image, d_alpha,
+                            d_depth, nullptr, nullptr, nullptr, saved_alpha, chi2, beta, bg_alpha, bg_intensity,
+                            scratch, scratch_bytes, d_means, d_tril, d_opac, d_inten, (cudaStream_t)stream_);
+}
+
+extern "C" int us3d_ug_backward_loss(void* workspace, const us3d_slice_frame* frames, int32_t n_frames,
+                                     int64_t n_tiles, int64_t n_pixels, int64_t n_gauss, int64_t cap,
+                                     const float* pixels, const float* image, const float* target,
+                                     const float* loss_coef, const float* saved_alpha, float chi2, float beta,
+                                     float bg_alpha, float bg_intensity, void* scratch, size_t scratch_bytes,
+                                     float* d_means, float* d_tril, float* d_opac, float* d_inten, void* stream_) {
+    US3D_CHECK_ARG(loss_coef != nullptr || n_frames == 0, "loss coefficients are NULL");
+    US3D_CHECK_ARG((reinterpret_cast<uintptr_t>(loss_coef) & 15) == 0, "loss coefficients must be 16-byte aligned");
+    return ug_backward_impl(workspace, frames, n_frames, n_tiles, n_pixels, n_gauss, cap, pixels, nullptr, nullptr,
+                            nullptr, image, target, reinterpret_cast<const float4*>(loss_coef), saved_alpha, chi2,
+                            beta, bg_alpha, bg_intensity, scratch, scratch_bytes, d_means, d_tril, d_opac, d_inten,
+                            (cudaStream_t)stream_);
 }
 
 extern "C" int us3d_ug_pixel_csr(void* workspace, const us3d_slice_frame* frames, int32_t n_frames, int64_t n_tiles,

@@ -78,4 +78,8 @@ __device__ __forceinline__ float f3_dot(const float3 a, const float3 b) {
 // oracle can state the same rule.
 __device__ __forceinline__ uint32_t f32_to_u32_sat(float x) { return (uint32_t)x; }
 
+// Logistic function of a raw (logit) parameter, computed in double and rounded once, so that it
+// does not depend on the fast single-precision exponential this library is compiled with.
+__device__ __forceinline__ float sigmoid_logit(float x) { return (float)(1.0 / (1.0 + exp(-(double)x))); }
+
 }  // namespace us3d

@@ -52,6 +52,28 @@ class SliceFrame(ctypes.Structure):
 
 assert ctypes.sizeof(SliceFrame) == 96
 
+
+class AdamTensor(ctypes.Structure):
+    """Host mirror of ``us3d_adam_tensor`` (48 bytes)."""
+
+    _fields_ = [
+        ("param", c_void_p),
+        ("grad", c_void_p),
+        ("exp_avg", c_void_p),
+        ("exp_avg_sq", c_void_p),
+        ("numel", c_int64),
+        ("activation", c_int32),
+        ("reserved", c_int32),
+    ]
+
+
+assert ctypes.sizeof(AdamTensor) == 48
+ADAM_MAX_TENSORS = 8
+ADAM_IDENTITY = 0
+ADAM_LOGISTIC = 1
+UG_BIN_SLICE_CULL = 1
+UG_BIN_LOGIT_ATTRIBUTES = 2
+
 # name -> (restype, argtypes)
 _SIGNATURES = {
     "us3d_last_error": (c_char_p, []),
@@ -83,6 +105,22 @@ _SIGNATURES = {
         [c_void_p, c_void_p, c_int32, c_int64, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
          c_void_p, c_float, c_float, c_float, c_float, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p,
          c_void_p],
+    ),
+    "us3d_ug_loss_scratch_bytes": (c_size_t, [c_int32]),
+    "us3d_ug_loss": (
+        c_int32,
+        [c_void_p, c_int32, c_int64, c_void_p, c_void_p, c_float, c_float, c_void_p, c_size_t, c_void_p, c_void_p,
+         c_void_p],
+    ),
+    "us3d_ug_backward_loss": (
+        c_int32,
+        [c_void_p, c_void_p, c_int32, c_int64, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_void_p, c_float, c_float, c_float, c_float, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_void_p],
+    ),
+    "us3d_adam_step": (
+        c_int32, [POINTER(AdamTensor), c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                  c_int64, c_void_p]
     ),
     "us3d_ug_pixel_csr": (
         c_int32,

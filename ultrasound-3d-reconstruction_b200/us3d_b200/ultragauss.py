@@ -125,12 +125,14 @@ def _check_params(means, tril, opac, inten):
 def bin_gaussians(means: torch.Tensor, tril: torch.Tensor, opac: torch.Tensor, inten: torch.Tensor,
                   frames: FrameTable, chi2: float, beta: float, sort_by_depth: bool = True,
                   capacity: Optional[int] = None, sync_check: bool = True,
-                  slice_cull_pixels: Optional[torch.Tensor] = None) -> UGBinning:
+                  slice_cull_pixels: Optional[torch.Tensor] = None, logit_attributes: bool = False) -> UGBinning:
     """Runs the mapper for all frames. With ``sync_check`` the instance total is read back
     (one stream synchronisation) and the binning is redone with a larger capacity if needed.
     Passing the frames' pixel positions as ``slice_cull_pixels`` drops the tiles a Gaussian's
     chi-square ellipse cannot reach (same images and gradients; no per-pixel candidate counts
-    or lists afterwards)."""
+    or lists afterwards). With ``logit_attributes`` the opacities and intensities are raw
+    logits, activated by the logistic function inside the binning (the gradients that
+    ``backward`` returns are then still w.r.t. the activated values)."""
     G = _check_params(means, tril, opac, inten)
     dev = means.device
     _set_device(dev)
@@ -143,7 +145,8 @@ def bin_gaussians(means: torch.Tensor, tril: torch.Tensor, opac: torch.Tensor, i
         st = _lib.call(
             "us3d_ug_bin_ex", _ptr(ws), int(nbytes), _ptr(frames.table), frames.n_frames, frames.n_tiles,
             frames.n_pixels, G, _ptr(means), _ptr(tril), _ptr(opac), _ptr(inten), float(chi2), float(beta),
-            int(bool(sort_by_depth)), cap, _ptr(slice_cull_pixels) if cull else None, 1 if cull else 0, _stream(),
+            int(bool(sort_by_depth)), cap, _ptr(slice_cull_pixels) if cull else None,
+            (_lib.UG_BIN_SLICE_CULL if cull else 0) | (_lib.UG_BIN_LOGIT_ATTRIBUTES if logit_attributes else 0), _stream(),
         )
         _lib.check(st, "us3d_ug_bin_ex")
         b = UGBinning(ws, cap, -1, frames, G, float(chi2), float(beta), bool(sort_by_depth), cull)
@@ -216,6 +219,54 @@ def backward(b: UGBinning, pixels: torch.Tensor, d_image: torch.Tensor, d_alpha:
         _ptr(dm), _ptr(dt), _ptr(do), _ptr(di), _stream(),
     )
     _lib.check(st, "us3d_ug_backward")
+    return dm, dt, do, di
+
+
+def loss(frames: FrameTable, image: torch.Tensor, target: torch.Tensor, l1_weight: float = 1.0,
+         ssim_weight: float = 0.0, scratch: Optional[torch.Tensor] = None, out=None):
+    """Per-frame loss l1_weight * mean|x - y| + ssim_weight * (1 - global SSIM) of the frames'
+    images against their targets. Returns (stats (F,8) float64: mean x, mean y, var x, var y,
+    cov xy, mean |x - y|, SSIM, loss; coef (F,4) float32: the per-frame coefficients of the
+    loss gradient, consumed by ``backward_loss``). Never synchronises."""
+    dev = image.device
+    F = frames.n_frames
+    sbytes = int(_lib.call("us3d_ug_loss_scratch_bytes", F))
+    if scratch is None or scratch.numel() < sbytes:
+        scratch = torch.empty(max(sbytes, 16), dtype=torch.uint8, device=dev)
+    if out is None:
+        out = (torch.empty((F, 8), dtype=torch.float64, device=dev), torch.empty((F, 4), dtype=torch.float32, device=dev))
+    stats, coef = out
+    _lib.check(_lib.call("us3d_ug_loss", _ptr(frames.table), F, frames.n_pixels, _ptr(image), _ptr(target),
+                         float(l1_weight), float(ssim_weight), _ptr(scratch), int(scratch.numel()), _ptr(stats),
+                         _ptr(coef), _stream()), "us3d_ug_loss")
+    return stats, coef
+
+
+def backward_loss(b: UGBinning, pixels: torch.Tensor, image: torch.Tensor, target: torch.Tensor,
+                  coef: torch.Tensor, saved_alpha: torch.Tensor, bg_alpha: float, bg_intensity: float,
+                  scratch: Optional[torch.Tensor] = None, out=None):
+    """``backward`` with dL/dimage taken from the fused per-frame loss (``loss``'s coefficients)
+    and zero dL/dalpha, dL/ddepth."""
+    G = b.n_gauss
+    dev = pixels.device
+    sbytes = int(_lib.call("us3d_ug_backward_scratch_bytes", b.capacity))
+    if scratch is None or scratch.numel() < sbytes:
+        scratch = torch.empty(max(sbytes, 16), dtype=torch.uint8, device=dev)
+    if out is None:
+        out = (
+            torch.empty((G, 3), dtype=torch.float32, device=dev),
+            torch.empty((G, 6), dtype=torch.float32, device=dev),
+            torch.empty((G,), dtype=torch.float32, device=dev),
+            torch.empty((G,), dtype=torch.float32, device=dev),
+        )
+    dm, dt, do, di = out
+    st = _lib.call(
+        "us3d_ug_backward_loss", _ptr(b.workspace), _ptr(b.frames.table), b.frames.n_frames, b.frames.n_tiles,
+        b.frames.n_pixels, G, b.capacity, _ptr(pixels), _ptr(image), _ptr(target), _ptr(coef), _ptr(saved_alpha),
+        b.chi2, b.beta, float(bg_alpha), float(bg_intensity), _ptr(scratch), int(scratch.numel()), _ptr(dm),
+        _ptr(dt), _ptr(do), _ptr(di), _stream(),
+    )
+    _lib.check(st, "us3d_ug_backward_loss")
     return dm, dt, do, di
 
 
