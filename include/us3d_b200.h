@@ -252,6 +252,30 @@ US3D_API int us3d_adam_step(const us3d_adam_tensor* tensors, int32_t n_tensors, 
                             double beta2, double eps, int64_t step, void* stream);
 
 /*
+ * A batch of frames assembled on the device from a dataset held in device memory (the
+ * batched replacement of NpzUltrasoundDataset.get_frame, pipeline_god_file.py:212-245): for
+ * each of the n_batch dataset indices (device int64; an index outside [0, n_all) sets bit 0
+ * of *status and takes frame 0), the frame record of all_frames (n_all records of height x
+ * width frames) with this batch's pixel and tile offsets; its pixel centre positions, gathered
+ * from all_pixel_positions (n_all x height*width x 3) or, if that is NULL, generated from the
+ * record exactly as the reference does (pipeline_god_file.py:299-306: lateral = (u -
+ * lateral_col_offset) * lateral_spacing, axial = axial_near + v * axial_spacing, p = (origin +
+ * lateral * axis_lat) + axial * axis_ax, float operations rounded one by one); and its target
+ * image from `images` (n_all x height*width) in `image_format`. The _DIV255 formats apply the
+ * reference's scaling of images whose maximum exceeds 1.5 (pipeline_god_file.py:184-186):
+ * float(x) / 255. Outputs: out_frames (n_batch records), out_pixel_positions (n_batch*H*W x
+ * 3), out_targets (n_batch*H*W). Never synchronises.
+ */
+#define US3D_IMAGES_F32 0
+#define US3D_IMAGES_F32_DIV255 1
+#define US3D_IMAGES_U8 2
+#define US3D_IMAGES_U8_DIV255 3
+US3D_API int us3d_frames_gather(const us3d_slice_frame* all_frames, int64_t n_all, const int64_t* indices,
+                                int32_t n_batch, int32_t height, int32_t width, const float* all_pixel_positions,
+                                const void* images, int32_t image_format, us3d_slice_frame* out_frames,
+                                float* out_pixel_positions, float* out_targets, int32_t* status, void* stream);
+
+/*
  * Per-pixel candidate lists in the reference's CSR layout (pixel_gauss_indices of
  * MapperForwardCUDA, src/mapper/core.cu:237-287): for each pixel, in tile-list order,
  * the Gaussians passing the window test. `offsets` is the exclusive scan of the counts

@@ -71,7 +71,8 @@ def test_loss_and_gradient_coefficients(w1, ws, cuda_device):
         L = _image_loss(xd, yd, float(np.float32(w1)), float(np.float32(ws)))
         L.backward()
         st = stats[f].cpu()
-        assert abs(float(st[7]) - float(L)) <= 1e-9 * max(1.0, abs(float(L))), (f, float(st[7]), float(L))
+        lv = float(L.detach())
+        assert abs(float(st[7]) - lv) <= 1e-9 * max(1.0, abs(lv)), (f, float(st[7]), lv)
         assert abs(float(st[6]) - float(_simple_ssim(xd.detach(), yd))) <= 1e-9
         k = coef[f]
         xs, ys = x[off:off + n], y[off:off + n]

@@ -73,6 +73,7 @@ ADAM_IDENTITY = 0
 ADAM_LOGISTIC = 1
 UG_BIN_SLICE_CULL = 1
 UG_BIN_LOGIT_ATTRIBUTES = 2
+IMAGES_F32, IMAGES_F32_DIV255, IMAGES_U8, IMAGES_U8_DIV255 = 0, 1, 2, 3
 
 # name -> (restype, argtypes)
 _SIGNATURES = {
@@ -121,6 +122,11 @@ _SIGNATURES = {
     "us3d_adam_step": (
         c_int32, [POINTER(AdamTensor), c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                   c_int64, c_void_p]
+    ),
+    "us3d_frames_gather": (
+        c_int32,
+        [c_void_p, c_int64, c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
+         c_void_p, c_void_p, c_void_p],
     ),
     "us3d_ug_pixel_csr": (
         c_int32,

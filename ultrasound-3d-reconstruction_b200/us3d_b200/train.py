@@ -126,12 +126,13 @@ class UltraGaussTrainer:
     folded in) -> forward -> per-frame loss -> backward with the fused loss gradient, replayed
     from one CUDA graph per batch, then Adam on all four parameter tensors (one launch).
 
-    ``batches`` is a list of (frame specs, pixel positions (P,3), targets (P,)) on the device;
-    pixel positions and targets must stay at their addresses (refresh them in place). The
-    instance capacity of each batch is fixed from a synchronised priming binning times
-    ``margin``; ``check()`` reads the flags of every batch's last replay (one synchronisation
-    per batch) and raises if a binning outgrew its capacity. ``losses()`` returns the last
-    replay's per-frame statistics (synchronises)."""
+    ``batches`` is a list of (frame specs or a FrameTable, pixel positions (P,3), targets (P,))
+    on the device; frame tables, pixel positions and targets must stay at their addresses
+    (refresh them in place). The instance capacity of each batch is fixed from a synchronised
+    priming binning times ``margin``; ``check()`` reads the flags of every batch's last replay
+    (one synchronisation per batch) and raises if a binning outgrew its capacity. ``losses()``
+    returns the last replay's per-frame statistics (synchronises). ``from_source`` trains on
+    random batches drawn on the device from a ``frames.DeviceFrameSource``."""
 
     def __init__(self, params: UltraGaussParameters, batches, cfg: Optional[TrainConfig] = None,
                  margin: float = 1.25, graph: bool = True):
@@ -144,8 +145,9 @@ class UltraGaussTrainer:
         self.optimizer = Adam(params.tensors(), self.cfg.lr, (self.cfg.beta1, self.cfg.beta2), self.cfg.eps,
                               logistic=[False, False, True, True])
         self._batches = []
+        self.source = None
         for specs, pixels, targets in batches:
-            frames = UG.build_frame_table(list(specs), dev)
+            frames = specs if isinstance(specs, UG.FrameTable) else UG.build_frame_table(list(specs), dev)
             prime = UG.bin_gaussians(*self._render_args(), frames, self.cfg.chi2_threshold, self.cfg.diag_beta,
                                      self.cfg.sort_by_depth, slice_cull_pixels=pixels, logit_attributes=True)
             cap = int(prime.total * margin) + 1024
@@ -154,6 +156,38 @@ class UltraGaussTrainer:
                                       coef=torch.zeros((frames.n_frames, 4), device=dev), graph=None))
         self.graph = graph
         self.steps_done = 0
+
+    @classmethod
+    def from_source(cls, params: UltraGaussParameters, source, batch_size: int, cfg: Optional[TrainConfig] = None,
+                    margin: float = 1.5, prime_batches: int = 4, seed: int = 0, graph: bool = True,
+                    indices: Optional[torch.Tensor] = None) -> "UltraGaussTrainer":
+        """Trains on batches of ``batch_size`` frames of ``source`` (a DeviceFrameSource): each
+        step draws dataset indices on the device (uniformly among ``indices``, all frames by
+        default; the reference draws one frame per step with np.random.choice) and assembles the
+        batch in place with one launch. The instance capacity is the largest of
+        ``prime_batches`` random batches times ``margin``."""
+        dev = source.device
+        pool = (indices if indices is not None else torch.arange(source.n)).to(dev, torch.int64)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(int(seed))
+        table = source.frame_table(batch_size)
+        hw = source.height * source.width
+        pixels = torch.empty((batch_size * hw, 3), device=dev)
+        targets = torch.empty((batch_size * hw,), device=dev)
+        draw = torch.empty((batch_size,), dtype=torch.int64, device=dev)
+        c = cfg or TrainConfig()
+        best = 0
+        for _ in range(max(1, int(prime_batches))):
+            torch.randint(0, pool.numel(), (batch_size,), generator=gen, device=dev, out=draw)
+            source.fill(pool[draw], table, pixels, targets)
+            b = UG.bin_gaussians(params.means, params.raw_precision_tril, params.raw_opacities.reshape(-1),
+                                 params.raw_intensities.reshape(-1), table, c.chi2_threshold, c.diag_beta,
+                                 c.sort_by_depth, slice_cull_pixels=pixels, logit_attributes=True)
+            best = max(best, b.total)
+        self = cls(params, [(table, pixels, targets)], c, margin=1.0, graph=graph)
+        self._batches[0]["capacity"] = int(best * margin) + 1024
+        self.source = dict(source=source, pool=pool, gen=gen, draw=draw)
+        return self
 
     def _render_args(self):
         p = self.params
@@ -176,6 +210,11 @@ class UltraGaussTrainer:
         a CUDA graph once captured) and the Adam update (one launch; its step count and bias
         corrections change every step, so it runs outside the graph)."""
         bt = self._batches[batch_index]
+        if self.source is not None:
+            sc = self.source
+            torch.randint(0, sc["pool"].numel(), sc["draw"].shape, generator=sc["gen"], device=sc["draw"].device,
+                          out=sc["draw"])
+            sc["source"].fill(sc["pool"][sc["draw"]], bt["frames"], bt["pixels"], bt["targets"])
         if not self.graph:
             self._forward_backward(bt)
         elif bt["graph"] is None:
@@ -195,6 +234,8 @@ class UltraGaussTrainer:
         return self._batches[batch_index]["stats"].cpu()
 
     def check(self) -> None:
+        if self.source is not None:
+            self.source["source"].check()
         for k, bt in enumerate(self._batches):
             if bt["binning"] is None:
                 continue
