@@ -89,3 +89,32 @@ def test_shard_frames_partition():
             assert max(map(len, parts)) - min(map(len, parts)) <= 1
     with pytest.raises(ValueError):
         shard_frames(4, 2, 2)
+
+
+def test_device_frame_source_records_on_host():
+    """The frame records a DeviceFrameSource keeps (built without a GPU on the CPU device):
+    the reference's axis normalisation, spacings, lateral centring and the frame size in the
+    us3d_slice_frame layout; 8-bit images scaled by 1/255 when their maximum exceeds 1.5."""
+    import numpy as np
+    import torch
+
+    from us3d_b200 import _lib
+    from us3d_b200.frames import DeviceFrameSource
+
+    rng = np.random.default_rng(0)
+    images = rng.integers(0, 256, (4, 10, 12), dtype=np.uint8)
+    lat = rng.normal(size=(4, 3)).astype(np.float32)
+    src = DeviceFrameSource(images, np.zeros(3, np.float32), lat, [0, 2, 0], None, 0.25, 0.5, 1.5, True,
+                            device=torch.device("cpu"))
+    assert src.image_format == _lib.IMAGES_U8_DIV255
+    rec = src.records
+    assert rec.shape == (4, 24)
+    ref_lat = torch.from_numpy(lat) / torch.linalg.norm(torch.from_numpy(lat), dim=1, keepdim=True).clamp(min=1e-8)
+    assert torch.allclose(rec[:, 3:6], ref_lat, rtol=0, atol=1e-7)
+    assert torch.equal(rec[:, 6:9], torch.tensor([[0.0, 1.0, 0.0]]).expand(4, 3))
+    assert torch.equal(rec[:, 9:12], torch.tensor([[0.0, 0.0, 1.0]]).expand(4, 3))
+    assert torch.equal(rec[0, 12:16], torch.tensor([0.25, 0.5, 1.5, 5.5]))
+    assert rec[0, 16:18].view(torch.int32).tolist() == [10, 12]
+    flat = DeviceFrameSource(images.astype(np.float32) / 255.0, None, None, None, None, 1.0, 1.0,
+                             device=torch.device("cpu"))
+    assert flat.image_format == _lib.IMAGES_F32
