@@ -344,6 +344,7 @@ def run_b200(a):
 
     if rank == 0 and world == 1 and not a.no_cpu:
         out["cpu_baseline"] = cpu_baseline(a, sc, specs)
+        out["cpu_baseline_dense_fallback"] = cpu_baseline_dense()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -500,6 +501,36 @@ def cpu_baseline(a, sc, specs, frames: int = 1):
     return {"value": round(frames / dt, 5), "unit": UNIT, "cores": nt, "kind": "port",
             "sample": f"{frames} full frame(s) of the workload ({a.gaussians} Gaussians, {a.size}^2 px): "
                       f"C oracle mapper + per-pixel candidate lists + forward + backward, {dt:.1f} s"}
+
+
+def cpu_baseline_dense(frames: int = 2):
+    """The reference's own CPU path for UltraGauss (its dense PyTorch fallback, restated in
+    oracle/ultragauss_dense_fallback.py) with autograd backward and an L1 loss, on all host
+    threads, at the survey's config-1 size (4,096 Gaussians, 128x128 frames at 0.3 mm):
+    `frames` frames are timed."""
+    import torch
+
+    from oracle.ultragauss_dense_fallback import render_dense
+    from us3d_b200 import scenes
+
+    nt = os.cpu_count() or 1
+    torch.set_num_threads(nt)
+    sc = scenes.make_scene(4096, seed=0)
+    sweep = scenes.linear_sweep(16, 128, 128, 0.3, seed=0)
+    ps = [sc.means.clone(), sc.precision_tril.clone(),
+          torch.logit(sc.opacities.clamp(1e-6, 1 - 1e-6)).reshape(-1, 1),
+          torch.logit(sc.intensities.clamp(1e-6, 1 - 1e-6)).reshape(-1, 1)]
+    ps = [p.requires_grad_(True) for p in ps]
+    tgt = torch.rand((16, 128 * 128), generator=torch.Generator().manual_seed(1))
+    t0 = time.perf_counter()
+    for f in range(frames):
+        img, _ = render_dense(*ps, sweep[f].pixels, 1e-4, 128, 128)
+        loss = (img.reshape(-1) - tgt[f]).abs().mean()
+        loss.backward()
+    dt = time.perf_counter() - t0
+    return {"value": round(frames / dt, 4), "unit": UNIT, "cores": nt, "kind": "port",
+            "sample": f"{frames} frames at config-1 size (4096 Gaussians, 128^2 px): the reference's dense PyTorch "
+                      f"CPU fallback (restated) + autograd backward, {dt:.1f} s"}
 
 
 def run_reference(a):
