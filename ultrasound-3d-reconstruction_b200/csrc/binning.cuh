@@ -63,6 +63,127 @@ static __device__ void bitonic_sort(unsigned long long* k, int* v, int n) {
     }
 }
 
+// ------------------------------------------------------------------------------------
+// Bucket filling for renderers whose element g has the instances of a half-open rectangle
+// (x0, y0, x1, y1) of a gx-wide bucket grid, enumerated row by row (nothing when x0 >= x1 or
+// y0 >= y1). When the grid has at most BLOCK_BUCKETS_MAX buckets, a block first counts in
+// shared memory and touches each global counter once per bucket it fills, so that a few buckets
+// receiving many instances (a small image, large splats) do not serialise on same-address
+// global atomics.
+// ------------------------------------------------------------------------------------
+constexpr int BUCKET_THREADS = 256;
+constexpr int BLOCK_BUCKETS_MAX = 4096;
+
+struct RectOf4 {
+    const int4* r;
+    __device__ __forceinline__ int4 operator()(int64_t g) const { return r[g]; }
+};
+
+// An inclusive 1D range (r0, r1) as the rectangle (r0, 0, r1 + 1, 1).
+struct RangeOf2 {
+    const int2* r;
+    __device__ __forceinline__ int4 operator()(int64_t g) const {
+        const int2 v = r[g];
+        return make_int4(v.x, 0, v.y + 1, 1);
+    }
+};
+
+static inline bool bucket_counts_in_smem(int64_t n_buckets) { return n_buckets <= BLOCK_BUCKETS_MAX; }
+
+// Instances per bucket (count[] must be zero on entry). Dynamic shared memory: n_buckets ints
+// when bucket_counts_in_smem(n_buckets), else none.
+template <class Rect>
+static __global__ void __launch_bounds__(BUCKET_THREADS)
+rect_count_kernel(int64_t n, int gx, int n_buckets, int use_smem, Rect rect, int* __restrict__ count) {
+    extern __shared__ int s_cnt[];
+    if (use_smem) {
+        for (int i = threadIdx.x; i < n_buckets; i += blockDim.x) s_cnt[i] = 0;
+        __syncthreads();
+    }
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < n) {
+        const int4 r = rect(g);
+        for (int y = r.y; y < r.w; ++y)
+            for (int x = r.x; x < r.z; ++x) atomicAdd(use_smem ? &s_cnt[y * gx + x] : &count[y * gx + x], 1);
+    }
+    if (use_smem) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < n_buckets; i += blockDim.x)
+            if (s_cnt[i] != 0) atomicAdd(&count[i], s_cnt[i]);
+    }
+}
+
+// Writes element g's instances into their buckets: key (dkey[g] << 32 | g) (dkey NULL: 0),
+// instance id inst_offset[g] + ordinal in enumeration order. A slot never leaves its bucket.
+// Dynamic shared memory: 2 * n_buckets ints when use_smem (slots reserved once per block and
+// bucket), else none.
+template <class Rect>
+static __global__ void __launch_bounds__(BUCKET_THREADS)
+rect_scatter_kernel(int64_t n, int gx, int n_buckets, int use_smem, Rect rect, const uint32_t* __restrict__ dkey,
+                    const int* __restrict__ inst_offset, const int* __restrict__ start, int* __restrict__ cursor,
+                    const long long* __restrict__ header, unsigned long long* __restrict__ keys,
+                    int* __restrict__ slot_inst) {
+    extern __shared__ int s_buf[];
+    if (header[H_FLAGS] != 0) return;
+    int* s_cnt = s_buf;
+    int* s_base = s_buf + n_buckets;
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int4 r = g < n ? rect(g) : make_int4(0, 0, 0, 0);
+    if (use_smem) {
+        for (int i = threadIdx.x; i < n_buckets; i += blockDim.x) s_cnt[i] = 0;
+        __syncthreads();
+        for (int y = r.y; y < r.w; ++y)
+            for (int x = r.x; x < r.z; ++x) atomicAdd(&s_cnt[y * gx + x], 1);
+        __syncthreads();
+        for (int i = threadIdx.x; i < n_buckets; i += blockDim.x)
+            if (s_cnt[i] != 0) {
+                s_base[i] = atomicAdd(&cursor[i], s_cnt[i]);
+                s_cnt[i] = 0;
+            }
+        __syncthreads();
+    }
+    if (r.x >= r.z || r.y >= r.w) return;
+    const unsigned long long key =
+        ((unsigned long long)(dkey ? dkey[g] : 0u) << 32) | (unsigned long long)(uint32_t)g;
+    int inst = inst_offset[g];
+    for (int y = r.y; y < r.w; ++y)
+        for (int x = r.x; x < r.z; ++x) {
+            const int t = y * gx + x;
+            const int within = use_smem ? s_base[t] + atomicAdd(&s_cnt[t], 1) : atomicAdd(&cursor[t], 1);
+            const int slot = start[t] + within;
+            if (slot < start[t + 1]) {
+                keys[slot] = key;
+                slot_inst[slot] = inst;
+            }
+            ++inst;
+        }
+}
+
+// Launches rect_count_kernel / rect_scatter_kernel with their shared memory.
+template <class Rect>
+static inline cudaError_t launch_rect_count(int64_t n, int gx, int64_t n_buckets, Rect rect, int* count,
+                                            cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const int sm = bucket_counts_in_smem(n_buckets) ? 1 : 0;
+    rect_count_kernel<Rect><<<(unsigned)((n + BUCKET_THREADS - 1) / BUCKET_THREADS), BUCKET_THREADS,
+                              sm ? (size_t)n_buckets * sizeof(int) : 0, stream>>>(n, gx, (int)n_buckets, sm, rect,
+                                                                                  count);
+    return cudaGetLastError();
+}
+
+template <class Rect>
+static inline cudaError_t launch_rect_scatter(int64_t n, int gx, int64_t n_buckets, Rect rect, const uint32_t* dkey,
+                                              const int* inst_offset, const int* start, int* cursor,
+                                              const long long* header, unsigned long long* keys, int* slot_inst,
+                                              cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const int sm = bucket_counts_in_smem(n_buckets) ? 1 : 0;
+    rect_scatter_kernel<Rect><<<(unsigned)((n + BUCKET_THREADS - 1) / BUCKET_THREADS), BUCKET_THREADS,
+                                sm ? (size_t)n_buckets * 2 * sizeof(int) : 0, stream>>>(
+        n, gx, (int)n_buckets, sm, rect, dkey, inst_offset, start, cursor, header, keys, slot_inst);
+    return cudaGetLastError();
+}
+
 // Register-resident part of the shared-memory sort. A warp owns a 64-element segment; lane
 // l holds its elements 2l (x0) and 2l + 1 (x1). A compare-exchange of stride h >= 2 pairs
 // lane l with lane l ^ h/2 (same slot); a mirror pass over blocks of `size` pairs element
@@ -237,8 +358,9 @@ tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long*
 }
 
 // Second pass: buckets of SORT_SMEM_CAP < n <= SORT_BIG_CAP keys with 96 KB of shared
-// memory. Each block inspects SORT_BIG_TILES consecutive tiles and orders its large ones.
-constexpr int SORT_BIG_TILES = 16;
+// memory. Block b owns a contiguous range of tiles; it inspects them SORT_THREADS at a time
+// and orders the large ones it finds, one after another.
+constexpr int SORT_BIG_GRID = 2 * 148;  // two 96 KB blocks per SM
 
 static __global__ void __launch_bounds__(SORT_THREADS)
 tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
@@ -247,29 +369,30 @@ tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long l
                      const unsigned char* __restrict__ slot_mask, unsigned char* __restrict__ sorted_mask) {
     extern __shared__ __align__(16) unsigned long long s_big_keys[];
     int* s_big_idx = reinterpret_cast<int*>(s_big_keys + SORT_BIG_CAP);
+    __shared__ int s_list[SORT_THREADS];
+    __shared__ int s_n;
     if (header[H_FLAGS] != 0) return;
-    const int64_t t0 = (int64_t)blockIdx.x * SORT_BIG_TILES;
-    const int64_t t = t0 + threadIdx.x;
-    bool big = false;
-    if (threadIdx.x < SORT_BIG_TILES && t < T) {
-        const int n = tile_start[t + 1] - tile_start[t];
-        big = n > SORT_SMEM_CAP && n <= SORT_BIG_CAP;
-    }
-    __shared__ unsigned s_mask;
-    if (threadIdx.x < 32) {
-        const unsigned m = __ballot_sync(0xffffffffu, big);
-        if (threadIdx.x == 0) s_mask = m;
-    }
-    __syncthreads();
-    unsigned mask = s_mask;
-    while (mask != 0u) {
-        const int j = __ffs(mask) - 1;
-        mask &= mask - 1u;
-        const int s0 = tile_start[t0 + j];
-        const int n = tile_start[t0 + j + 1] - s0;
-        sort_bucket_smem(s_big_keys, s_big_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask,
-                         sorted_mask);
+    const int64_t per = (T + gridDim.x - 1) / gridDim.x;
+    const int64_t t0 = (int64_t)blockIdx.x * per;
+    const int64_t t1 = t0 + per < T ? t0 + per : T;
+    for (int64_t c0 = t0; c0 < t1; c0 += SORT_THREADS) {
+        if (threadIdx.x == 0) s_n = 0;
         __syncthreads();
+        const int64_t t = c0 + threadIdx.x;
+        if (t < t1) {
+            const int n = tile_start[t + 1] - tile_start[t];
+            if (n > SORT_SMEM_CAP && n <= SORT_BIG_CAP) s_list[atomicAdd(&s_n, 1)] = threadIdx.x;
+        }
+        __syncthreads();
+        const int count = s_n;
+        for (int k = 0; k < count; ++k) {
+            const int64_t tt = c0 + s_list[k];
+            const int s0 = tile_start[tt];
+            const int n = tile_start[tt + 1] - s0;
+            sort_bucket_smem(s_big_keys, s_big_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask,
+                             sorted_mask);
+            __syncthreads();
+        }
     }
 }
 
@@ -298,7 +421,7 @@ static inline cudaError_t launch_tile_sort(int64_t T, const int* tile_start, con
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 128) attr_done[dev] = true;
     }
-    const unsigned grid = (unsigned)((T + SORT_BIG_TILES - 1) / SORT_BIG_TILES);
+    const unsigned grid = (unsigned)(T < SORT_BIG_GRID ? T : SORT_BIG_GRID);
     tile_sort_big_kernel<<<grid, SORT_THREADS, tile_sort_big_smem_bytes(), stream>>>(
         T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
     return cudaGetLastError();

@@ -306,8 +306,7 @@ preprocess_kernel(int64_t G, int H, int W, int tile, int tiles_x, int tiles_y, f
     rects[g] = make_int4(x0, y0, x1, y1);
     dkey[g] = sort_by_v ? f32_to_u32_sat((v_pix + 500.0f) * 1000.0f) : 0u;
     touched[g] = (x1 - x0) * (y1 - y0);
-    for (int y = y0; y < y1; ++y)
-        for (int x = x0; x < x1; ++x) atomicAdd(&tile_count[y * tiles_x + x], 1);
+    (void)tile_count;  // counted per block by rect_count_kernel
     // Forward candidate, computed with the forward's own near plane (the grid pack's);
     // the mapper's footprint is reused when the two near planes agree.
     Footprint Ff = F;
@@ -339,25 +338,6 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
     header[H_FLAGS] = flags;
 }
 
-__global__ void __launch_bounds__(256)
-scatter_kernel(int64_t G, int tiles_x, const int4* __restrict__ rects, const uint32_t* __restrict__ dkey,
-               const int* __restrict__ inst_offset, const int* __restrict__ tile_start, int* __restrict__ tile_cursor,
-               const long long* __restrict__ header, unsigned long long* __restrict__ keys,
-               int* __restrict__ slot_inst) {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= G || header[H_FLAGS] != 0) return;
-    const int4 r = rects[g];
-    if (r.x >= r.z || r.y >= r.w) return;
-    const unsigned long long key = ((unsigned long long)dkey[g] << 32) | (unsigned long long)(uint32_t)g;
-    int inst = inst_offset[g];
-    for (int y = r.y; y < r.w; ++y)
-        for (int x = r.x; x < r.z; ++x) {
-            const int t = y * tiles_x + x;
-            const int slot = tile_start[t] + atomicAdd(&tile_cursor[t], 1);
-            keys[slot] = key;
-            slot_inst[slot] = inst++;
-        }
-}
 
 // ------------------------------------------------------------------------------------
 // Forward
@@ -731,16 +711,13 @@ finalize_kernel(int64_t G, float k_sigma, const int* __restrict__ inst_offset, c
     pp[9] = -g_delta.x; pp[10] = -g_delta.y; pp[11] = -g_delta.z;
 }
 
-// Sums the per-Gaussian pose contributions in a fixed order (one block).
-__global__ void __launch_bounds__(256)
-pose_reduce_kernel(int64_t G, const float* __restrict__ pose_partial, float* __restrict__ d_pose) {
+// Sums the per-Gaussian pose contributions in a fixed order, in two launches: block b of
+// POSE_BLOCKS reduces the contiguous chunk b of Gaussians and leaves its 12 sums in the chunk's
+// first slot of pose_partial; one block then adds the chunk sums in block order.
+constexpr int POSE_BLOCKS = 512;
+
+__device__ __forceinline__ void pose_block_sum(float a[12]) {
     __shared__ float red[256][13];
-    float a[12];
-#pragma unroll
-    for (int i = 0; i < 12; ++i) a[i] = 0.f;
-    for (int64_t g = threadIdx.x; g < G; g += blockDim.x)
-#pragma unroll
-        for (int i = 0; i < 12; ++i) a[i] += pose_partial[12 * g + i];
 #pragma unroll
     for (int i = 0; i < 12; ++i) red[threadIdx.x][i] = a[i];
     __syncthreads();
@@ -750,10 +727,39 @@ pose_reduce_kernel(int64_t G, const float* __restrict__ pose_partial, float* __r
             for (int i = 0; i < 12; ++i) red[threadIdx.x][i] += red[threadIdx.x + stride][i];
         __syncthreads();
     }
+#pragma unroll
+    for (int i = 0; i < 12; ++i) a[i] = red[0][i];
+}
+
+__global__ void __launch_bounds__(256)
+pose_chunk_kernel(int64_t G, int64_t chunk, float* __restrict__ pose_partial) {
+    const int64_t g0 = (int64_t)blockIdx.x * chunk;
+    if (g0 >= G) return;
+    const int64_t g1 = g0 + chunk < G ? g0 + chunk : G;
+    float a[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) a[i] = 0.f;
+    for (int64_t g = g0 + threadIdx.x; g < g1; g += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < 12; ++i) a[i] += pose_partial[12 * g + i];
+    pose_block_sum(a);  // ends with every read of the chunk done
+    if (threadIdx.x < 12) pose_partial[12 * g0 + threadIdx.x] = a[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(256)
+pose_final_kernel(int64_t G, int64_t chunk, const float* __restrict__ pose_partial, float* __restrict__ d_pose) {
+    const int nb = (int)((G + chunk - 1) / chunk);
+    float a[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) a[i] = 0.f;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < 12; ++i) a[i] += pose_partial[12 * (int64_t)b * chunk + i];
+    pose_block_sum(a);
     if (threadIdx.x == 0) {
         const int idx[12] = {0, 4, 8, 1, 5, 9, 2, 6, 10, 3, 7, 11};
         for (int i = 0; i < 16; ++i) d_pose[i] = 0.f;
-        for (int i = 0; i < 12; ++i) d_pose[idx[i]] = red[0][i];
+        for (int i = 0; i < 12; ++i) d_pose[idx[i]] = a[i];
     }
 }
 
@@ -823,12 +829,12 @@ extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t 
                                                   intensities, pose, grid_pack, focus_params, w.rects, w.dkey,
                                                   w.touched, w.tile_count, w.cand);
     US3D_CHECK_LAUNCH("gp preprocess");
+    US3D_CHECK_CUDA(launch_rect_count(n_gauss, tx, T, RectOf4{w.rects}, w.tile_count, stream));
     US3D_CHECK_CUDA(exclusive_scan(w.touched, n_gauss, w.inst_offset, w.bs_g, w.header + H_SCAN_G, stream));
     US3D_CHECK_CUDA(exclusive_scan(w.tile_count, T, w.tile_start, w.bs_t, w.header + H_SCAN_T, stream));
     check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
-    if (n_gauss > 0)
-        scatter_kernel<<<gb, 256, 0, stream>>>(n_gauss, tx, w.rects, w.dkey, w.inst_offset, w.tile_start,
-                                               w.tile_cursor, w.header, w.keys, w.slot_inst);
+    US3D_CHECK_CUDA(launch_rect_scatter(n_gauss, tx, T, RectOf4{w.rects}, w.dkey, w.inst_offset, w.tile_start,
+                                        w.tile_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_gp_sort_attr, stream));
     forward_kernel<<<(unsigned)T, tile_size * tile_size, 0, stream>>>(H, W, tile_size, tx, grid_pack, focus_params,
@@ -836,7 +842,7 @@ extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t 
                                                                      out_image);
     US3D_CHECK_LAUNCH("gp forward");
     prof_end(prof, stream);
-    count_launches(1 + (n_gauss > 0) * 2 + 6 + 1 + TILE_SORT_LAUNCHES + 1);
+    count_launches(1 + (n_gauss > 0) * 3 + 6 + 1 + TILE_SORT_LAUNCHES + 1);
     return US3D_OK;
 }
 
@@ -888,7 +894,13 @@ extern "C" int us3d_gp_backward(void* workspace, int64_t n_gauss, const float* m
         ++launches;
     }
     if (pose_grad) {
-        pose_reduce_kernel<<<1, 256, 0, stream>>>(n_gauss, pose_partial, d_pose);
+        const int64_t chunk = std::max<int64_t>(1, (n_gauss + POSE_BLOCKS - 1) / POSE_BLOCKS);
+        if (n_gauss > 0) {
+            pose_chunk_kernel<<<(unsigned)((n_gauss + chunk - 1) / chunk), 256, 0, stream>>>(n_gauss, chunk,
+                                                                                             pose_partial);
+            ++launches;
+        }
+        pose_final_kernel<<<1, 256, 0, stream>>>(n_gauss, chunk, pose_partial, d_pose);
         US3D_CHECK_LAUNCH("gp pose reduce");
         ++launches;
     }

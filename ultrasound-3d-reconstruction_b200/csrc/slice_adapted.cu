@@ -121,8 +121,7 @@ preprocess_kernel(int64_t N, int H, int W, int gw, int gh, float hw, float hh, f
     if (x0 >= x1 || y0 >= y1) return;
     rects[g] = make_int4(x0, y0, x1, y1);
     touched[g] = (x1 - x0) * (y1 - y0);
-    for (int y = y0; y < y1; ++y)
-        for (int x = x0; x < x1; ++x) atomicAdd(&tile_count[y * gw + x], 1);
+    (void)tile_count;  // counted per block by rect_count_kernel
 }
 
 __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
@@ -134,23 +133,6 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
     header[H_FLAGS] = flags;
 }
 
-__global__ void __launch_bounds__(256)
-scatter_kernel(int64_t N, int gw, const int4* __restrict__ rects, const int* __restrict__ inst_offset,
-               const int* __restrict__ tile_start, int* __restrict__ tile_cursor, const long long* __restrict__ header,
-               unsigned long long* __restrict__ keys, int* __restrict__ slot_inst) {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= N || header[H_FLAGS] != 0) return;
-    const int4 r = rects[g];
-    if (r.x >= r.z || r.y >= r.w) return;
-    int inst = inst_offset[g];
-    for (int y = r.y; y < r.w; ++y)
-        for (int x = r.x; x < r.z; ++x) {
-            const int t = y * gw + x;
-            const int slot = tile_start[t] + atomicAdd(&tile_cursor[t], 1);
-            keys[slot] = (unsigned long long)(uint32_t)g;
-            slot_inst[slot] = inst++;
-        }
-}
 
 // One block of 16x16 threads per tile, staged Gaussians, per-pixel sums in tile-list order
 // (reference render.cu:354-426).
@@ -464,12 +446,12 @@ extern "C" int us3d_sa_bounded_forward(void* workspace, size_t workspace_bytes, 
     if (n > 0)
         preprocess_kernel<<<gb, 256, 0, stream>>>(n, H, W, gw, gh, half_width, half_height, radius_sigma, m2, iv,
                                                   w.rects, w.bbox, w.touched, w.tile_count);
+    US3D_CHECK_CUDA(launch_rect_count(n, gw, T, RectOf4{w.rects}, w.tile_count, stream));
     US3D_CHECK_CUDA(exclusive_scan(w.touched, n, w.inst_offset, w.bs_g, w.header + H_SCAN_G, stream));
     US3D_CHECK_CUDA(exclusive_scan(w.tile_count, T, w.tile_start, w.bs_t, w.header + H_SCAN_T, stream));
     check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
-    if (n > 0)
-        scatter_kernel<<<gb, 256, 0, stream>>>(n, gw, w.rects, w.inst_offset, w.tile_start, w.tile_cursor, w.header,
-                                               w.keys, w.slot_inst);
+    US3D_CHECK_CUDA(launch_rect_scatter(n, gw, T, RectOf4{w.rects}, nullptr, w.inst_offset, w.tile_start,
+                                        w.tile_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_sa_sort_attr, stream));
     forward_kernel<<<(unsigned)T, TILE * TILE, 0, stream>>>(H, W, gw, half_width, half_height, radius_sigma, m2, iv,
@@ -477,7 +459,7 @@ extern "C" int us3d_sa_bounded_forward(void* workspace, size_t workspace_bytes, 
                                                             out_image, out_alpha);
     US3D_CHECK_LAUNCH("sa forward");
     prof_end(prof, stream);
-    count_launches(1 + 2 * (n > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
+    count_launches(1 + 3 * (n > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
     return US3D_OK;
 }
 

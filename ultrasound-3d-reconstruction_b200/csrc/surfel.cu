@@ -376,8 +376,7 @@ preprocess_kernel(Params p, int* __restrict__ radii, float4* __restrict__ rec, f
     o[4] = make_float4(rgb[1], rgb[2], 0.f, 0.f);
     rect_out[g] = make_int4(x0, y0, x1, y1);
     touched[g] = (x1 - x0) * (y1 - y0);
-    for (int y = y0; y < y1; ++y)
-        for (int x = x0; x < x1; ++x) atomicAdd(&tile_count[y * p.gx + x], 1);
+    (void)tile_count;  // counted per block by rect_count_kernel
 }
 
 __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
@@ -389,26 +388,6 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
     header[H_FLAGS] = flags;
 }
 
-// Instances in the reference's enumeration order (tile rows, then columns) with key
-// (depth bits << 32 | g) in the tile's bucket (rasterizer_impl.cu:70-113).
-__global__ void __launch_bounds__(256)
-scatter_kernel(int G, int gx, const int4* __restrict__ rect, const float* __restrict__ depth,
-               const int* __restrict__ inst_offset, const int* __restrict__ tile_start, int* __restrict__ tile_cursor,
-               const long long* __restrict__ header, unsigned long long* __restrict__ keys, int* __restrict__ slot_inst) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= G || header[H_FLAGS] != 0) return;
-    const int4 rc = rect[g];
-    if ((rc.z - rc.x) * (rc.w - rc.y) == 0) return;
-    const unsigned long long key = ((unsigned long long)__float_as_uint(depth[g]) << 32) | (unsigned long long)(uint32_t)g;
-    int inst = inst_offset[g];
-    for (int y = rc.y; y < rc.w; ++y)
-        for (int x = rc.x; x < rc.z; ++x) {
-            const int t = y * gx + x;
-            const int slot = tile_start[t] + atomicAdd(&tile_cursor[t], 1);
-            keys[slot] = key;
-            slot_inst[slot] = inst++;
-        }
-}
 
 // ------------------------------------------------------------------------------------
 // Forward compositing
@@ -580,6 +559,7 @@ backward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const 
     __shared__ float4 s_rec[REC_F4][BWD_BATCH];
     __shared__ int s_inst[BWD_BATCH];
     __shared__ float s_red[BWD_BATCH][BLOCK / 32][NGRAD];
+    __shared__ int s_last;
     if (header[H_FLAGS] != 0) return;
     const int tile = blockIdx.x;
     const int tx = tile % gx, ty = tile / gx;
@@ -594,8 +574,21 @@ backward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const 
 
     const float T_final = inside ? accum[pix] : 0.f;
     float T = T_final;
-    uint32_t contributor = (uint32_t)n;
     const int last_contributor = inside ? (int)n_contrib[pix] : 0;
+    // No pixel of the tile has a contributor at or beyond the largest last contributor: the
+    // back-to-front replay starts there (its state changes only at contributors), and the
+    // instances behind it get zero partials.
+    if (threadIdx.x == 0) s_last = 0;
+    __syncthreads();
+    if (last_contributor > 0) atomicMax(&s_last, last_contributor);
+    __syncthreads();
+    const int n_live = min(s_last, n);
+    for (int k = n_live + threadIdx.x; k < n; k += BLOCK) {
+        float4* out = partial + (int64_t)PARTIAL_F4 * sorted_inst[s0 + k];
+#pragma unroll
+        for (int f = 0; f < PARTIAL_F4; ++f) out[f] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    uint32_t contributor = (uint32_t)n_live;
     const int median_contributor = inside ? (int)n_contrib[pix + HW] : 0;
     float dpix[3] = {0.f, 0.f, 0.f};
     float dd_depth = 0.f, dd_accum = 0.f, dd_reg = 0.f, dd_median = 0.f;
@@ -620,13 +613,13 @@ backward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const 
     const float bg_dot_dpixel = bg[0] * dpix[0] + bg[1] * dpix[1] + bg[2] * dpix[2];
     const float mscale = FAR_N / (FAR_N - NEAR_N);
 
-    for (int b0 = 0; b0 < n; b0 += BWD_BATCH) {
-        const int nb = min(BWD_BATCH, n - b0);
+    for (int b0 = 0; b0 < n_live; b0 += BWD_BATCH) {
+        const int nb = min(BWD_BATCH, n_live - b0);
         __syncthreads();
-        // stage from the back of the tile list
+        // stage from the back of the tile list's live part
         for (int q = threadIdx.x; q < nb * REC_F4; q += BLOCK) {
             const int jj = q / REC_F4, f = q - jj * REC_F4;
-            const int slot = s0 + n - 1 - (b0 + jj);
+            const int slot = s0 + n_live - 1 - (b0 + jj);
             s_rec[f][jj] = rec[(int64_t)REC_F4 * sorted_gid[slot] + f];
             if (f == 0) s_inst[jj] = sorted_inst[slot];
         }
@@ -1055,19 +1048,20 @@ extern "C" int us3d_gs_forward(void* workspace, size_t workspace_bytes, int64_t 
         preprocess_kernel<<<gb, 256, 0, stream>>>(p, out_radii, w.rec, w.depth, w.rect, w.clamped, w.touched,
                                                   w.tile_count, w.header);
     US3D_CHECK_LAUNCH("gs preprocess");
+    US3D_CHECK_CUDA(launch_rect_count(n_gauss, p.gx, T, RectOf4{w.rect}, w.tile_count, stream));
     US3D_CHECK_CUDA(exclusive_scan(w.touched, n_gauss, w.inst_offset, w.bs_g, w.header + H_SCAN_G, stream));
     US3D_CHECK_CUDA(exclusive_scan(w.tile_count, T, w.tile_start, w.bs_t, w.header + H_SCAN_T, stream));
     check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
-    if (n_gauss > 0)
-        scatter_kernel<<<gb, 256, 0, stream>>>((int)n_gauss, p.gx, w.rect, w.depth, w.inst_offset, w.tile_start,
-                                               w.tile_cursor, w.header, w.keys, w.slot_inst);
+    US3D_CHECK_CUDA(launch_rect_scatter(n_gauss, p.gx, T, RectOf4{w.rect}, reinterpret_cast<const uint32_t*>(w.depth),
+                                        w.inst_offset, w.tile_start, w.tile_cursor, w.header, w.keys, w.slot_inst,
+                                        stream));
     US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_gs_sort_attr, stream));
     forward_kernel<<<(unsigned)T, BLOCK, 0, stream>>>(width, height, p.gx, w.tile_start, w.sorted_gid, w.header, w.rec,
                                                       background, out_color, out_others, w.accum, w.n_contrib);
     US3D_CHECK_LAUNCH("gs forward");
     prof_end(prof, stream);
-    count_launches(1 + 2 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
+    count_launches(1 + 3 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
     return US3D_OK;
 }
 

@@ -263,7 +263,7 @@ preprocess_kernel(int64_t G, int W, float pixel_spacing, float col_off, float ne
     touched[g] = r1 - r0 + 1;
     ray_range[g] = make_int2(r0, r1);
     dkey[g] = f32_to_u32_sat(fmaxf(0.0f, pz) * 1000.0f);
-    for (int x = r0; x <= r1; ++x) atomicAdd(&ray_count[x], 1);
+    (void)ray_count;  // counted per block by rect_count_kernel
 }
 
 __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
@@ -275,22 +275,6 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
     header[H_FLAGS] = flags;
 }
 
-__global__ void __launch_bounds__(256)
-scatter_kernel(int64_t G, const int2* __restrict__ ray_range, const uint32_t* __restrict__ dkey,
-               const int* __restrict__ inst_offset, const int* __restrict__ ray_start, int* __restrict__ ray_cursor,
-               const long long* __restrict__ header, unsigned long long* __restrict__ keys, int* __restrict__ slot_inst) {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= G || header[H_FLAGS] != 0) return;
-    const int2 r = ray_range[g];
-    if (r.x > r.y) return;
-    const unsigned long long key = ((unsigned long long)dkey[g] << 32) | (unsigned long long)(uint32_t)g;
-    int inst = inst_offset[g];
-    for (int x = r.x; x <= r.y; ++x) {
-        const int slot = ray_start[x] + atomicAdd(&ray_cursor[x], 1);
-        keys[slot] = key;
-        slot_inst[slot] = inst++;
-    }
-}
 
 // ------------------------------------------------------------------------------------
 // Forward
@@ -679,12 +663,12 @@ extern "C" int us3d_ugr_forward(void* workspace, size_t workspace_bytes, int64_t
                                                   axis_lat, axis_ele, axis_ax, w.ray_range, w.dkey, w.touched,
                                                   w.ray_count, w.rec);
     US3D_CHECK_LAUNCH("ugr preprocess");
+    US3D_CHECK_CUDA(launch_rect_count(n_gauss, W, W, RangeOf2{w.ray_range}, w.ray_count, stream));
     US3D_CHECK_CUDA(exclusive_scan(w.touched, n_gauss, w.inst_offset, w.bs_g, w.header + H_SCAN_G, stream));
     US3D_CHECK_CUDA(exclusive_scan(w.ray_count, W, w.ray_start, w.bs_t, w.header + H_SCAN_T, stream));
     check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
-    if (n_gauss > 0)
-        scatter_kernel<<<gb, 256, 0, stream>>>(n_gauss, w.ray_range, w.dkey, w.inst_offset, w.ray_start, w.ray_cursor,
-                                               w.header, w.keys, w.slot_inst);
+    US3D_CHECK_CUDA(launch_rect_scatter(n_gauss, W, W, RangeOf2{w.ray_range}, w.dkey, w.inst_offset, w.ray_start,
+                                        w.ray_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(W, w.ray_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_ugr_sort_attr, stream));
     forward_kernel<<<(unsigned)W, 256, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions,
@@ -693,7 +677,7 @@ extern "C" int us3d_ugr_forward(void* workspace, size_t workspace_bytes, int64_t
                                                     local_max_window_mm, out_image, w.pixel_state);
     US3D_CHECK_LAUNCH("ugr forward");
     prof_end(prof, stream);
-    count_launches(1 + 2 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
+    count_launches(1 + 3 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
     return US3D_OK;
 }
 
