@@ -105,3 +105,21 @@ def test_gaussianpile_dropin_api(cuda_device):
     assert rel_l2(img.detach().cpu().numpy(), fx["ref_image"]) <= 1e-5
     assert rel_l2(means.grad.cpu().numpy(), fx["ref_d_means"]) <= 1e-4
     assert rel_l2(pose.grad.cpu().numpy(), fx["ref_d_pose"]) <= 1e-4
+
+
+@pytest.mark.parametrize("tile", [7, 12, 32])
+def test_gaussianpile_tile_sizes_same_image(tile, cuda_device):
+    """Tile lists hold candidates in Gaussian order whatever the tile size, and each pixel
+    applies the same box and weight tests, so the image does not depend on tile_size_px
+    (including sizes whose blocks end in a partial warp)."""
+    fx = load_gp((gp_golden_names() or ["c1"])[0])
+    from us3d_b200 import gaussianpile as GP
+
+    dev = cuda_device
+    t = lambda k: torch.as_tensor(fx[k]).to(dev).float().contiguous()  # noqa: E731
+    m = fx["meta"].tolist()
+    args = (t("means"), t("scales"), t("quats"), t("opacities").reshape(-1), t("intensities").reshape(-1),
+            t("pose").reshape(16), t("grid"), t("params"), int(fx["H"]), int(fx["W"]), m[2], m[3], m[4])
+    ref, _ = GP.forward(*args, 16, m[8], bool(m[9]))
+    img, _ = GP.forward(*args, tile, m[8], bool(m[9]))
+    assert torch.equal(img, ref)

@@ -114,14 +114,14 @@ def test_live_reference_parity(G, H, W, spacing, seed, sort, cuda_device):
 
 
 def test_live_reference_parity_dense_tiles(cuda_device):
-    """60000 Gaussians in a 16 mm cube under a 96x96 slice: tile buckets of every size class
-    of the tile sort (in-register segments, the 48 KB shared-memory pass, the 96 KB pass above
-    4096 keys, the global-memory network above 8192) against the reference's own binning."""
+    """120000 Gaussians in a 16 mm cube under a 96x96 slice: tile buckets of every size class
+    of the tile sort (in-register segments, the 48 KB shared-memory pass, the 192 KB pass above
+    4096 keys, the global-memory network above 16384) against the reference's own binning."""
     REF, REFK = _reference_modules()
-    fx = _scene_case(60000, 96, 96, 0.25, 5, frame=1, cube_mm=16.0)
+    fx = _scene_case(120000, 96, 96, 0.25, 5, frame=1, cube_mm=16.0)
     fx.update(_reference_run(REF, REFK, fx, cuda_device))
     n = fx["ref_range_end"] - fx["ref_range_start"]
-    assert n.max() > 8192 and ((n > 4096) & (n <= 8192)).any() and ((n > 64) & (n <= 2048)).any()
+    assert n.max() > 16384 and ((n > 4096) & (n <= 16384)).any() and ((n > 64) & (n <= 2048)).any()
     out = run_b200(fx, cuda_device)
     _assert_case(out, fx)
 

@@ -11,9 +11,10 @@ namespace us3d {
 constexpr int SORT_THREADS = 512;
 // Tiles of up to SORT_SMEM_CAP keys are ordered in shared memory by the first sort pass
 // (48 KB, four 512-thread blocks per SM); larger ones, up to SORT_BIG_CAP, by a second pass
-// with 96 KB; beyond that the network runs on global memory (one block per tile).
+// with 192 KB (one block per SM); beyond that the network runs on global memory (one block
+// per tile).
 constexpr int SORT_SMEM_CAP = 4096;
-constexpr int SORT_BIG_CAP = 8192;
+constexpr int SORT_BIG_CAP = 16384;
 constexpr int SORT_MIN_BLOCKS = 4;
 // Above every real key: a key's low word is a Gaussian (or instance) index below 2^31.
 constexpr unsigned long long SORT_PAD_KEY = ~0ull;
@@ -357,10 +358,10 @@ tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long*
     }
 }
 
-// Second pass: buckets of SORT_SMEM_CAP < n <= SORT_BIG_CAP keys with 96 KB of shared
+// Second pass: buckets of SORT_SMEM_CAP < n <= SORT_BIG_CAP keys with 192 KB of shared
 // memory. Block b owns a contiguous range of tiles; it inspects them SORT_THREADS at a time
 // and orders the large ones it finds, one after another.
-constexpr int SORT_BIG_GRID = 2 * 148;  // two 96 KB blocks per SM
+constexpr int SORT_BIG_GRID = 148;  // one 192 KB block per SM
 
 static __global__ void __launch_bounds__(SORT_THREADS)
 tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,

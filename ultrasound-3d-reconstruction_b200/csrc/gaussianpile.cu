@@ -357,7 +357,8 @@ __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float*
     const int tx = t % tiles_x, ty = t / tiles_x;
     const int lx = threadIdx.x % tile, ly = threadIdx.x / tile;
     const int x = tx * tile + lx, y = ty * tile + ly;
-    const bool valid = (x < W) && (y < H);
+    // blocks are whole warps (tile x tile rounded up to 32 threads): the extra threads own no pixel
+    const bool valid = (int)threadIdx.x < tile * tile && (x < W) && (y < H);
     const float weight_min = params[UF_WEIGHT_MIN];
     float xi_lat = 0.f, xi_ax = 0.f;
     if (valid) {
@@ -367,6 +368,18 @@ __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float*
     const int s0 = tile_start[t], n = tile_start[t + 1] - s0;
     float accum = 0.f;
     const int nthreads = blockDim.x;
+    // The warp's pixel extent in mm: a candidate whose box misses it (with a margin for the
+    // rounding of the per-pixel test) is skipped by the whole warp.
+    const int lane = threadIdx.x & 31;
+    float lat_lo = valid ? xi_lat : 3.0e38f, lat_hi = valid ? xi_lat : -3.0e38f;
+    float ax_lo = valid ? xi_ax : 3.0e38f, ax_hi = valid ? xi_ax : -3.0e38f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lat_lo = fminf(lat_lo, __shfl_xor_sync(0xffffffffu, lat_lo, o));
+        lat_hi = fmaxf(lat_hi, __shfl_xor_sync(0xffffffffu, lat_hi, o));
+        ax_lo = fminf(ax_lo, __shfl_xor_sync(0xffffffffu, ax_lo, o));
+        ax_hi = fmaxf(ax_hi, __shfl_xor_sync(0xffffffffu, ax_hi, o));
+    }
     for (int b0 = 0; b0 < n; b0 += FWD_BATCH) {
         const int nb = min(FWD_BATCH, n - b0);
         __syncthreads();
@@ -378,10 +391,23 @@ __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float*
             sc2[j] = make_float2(c2.x, c2.y);
         }
         __syncthreads();
-        if (valid) {
-            for (int j = 0; j < nb; ++j) {
+        for (int jc = 0; jc < nb; jc += 32) {
+            bool near = false;
+            if (jc + lane < nb) {
+                const float2 c2 = sc2[jc + lane];
+                const float4 c0 = sc0[jc + lane];
+                const float rl = sc1[jc + lane].w;
+                const float ml = 1e-5f * (fabsf(c0.z) + rl + fabsf(lat_lo) + fabsf(lat_hi)) + 1e-30f;
+                const float ma = 1e-5f * (fabsf(c0.w) + c2.x + fabsf(ax_lo) + fabsf(ax_hi)) + 1e-30f;
+                near = c2.y != 0.f && lat_hi >= c0.z - rl - ml && lat_lo <= c0.z + rl + ml &&
+                       ax_hi >= c0.w - c2.x - ma && ax_lo <= c0.w + c2.x + ma;
+            }
+            unsigned bits = __ballot_sync(0xffffffffu, near);
+            if (!valid) continue;
+            while (bits != 0u) {
+                const int j = jc + __ffs(bits) - 1;
+                bits &= bits - 1u;
                 const float2 c2 = sc2[j];
-                if (c2.y == 0.f) continue;
                 const float4 c0 = sc0[j];
                 const float4 c1 = sc1[j];
                 if (fabsf(xi_lat - c0.z) > c1.w || fabsf(xi_ax - c0.w) > c2.x) continue;
@@ -837,7 +863,7 @@ extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t 
                                         w.tile_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_gp_sort_attr, stream));
-    forward_kernel<<<(unsigned)T, tile_size * tile_size, 0, stream>>>(H, W, tile_size, tx, grid_pack, focus_params,
+    forward_kernel<<<(unsigned)T, (tile_size * tile_size + 31) / 32 * 32, 0, stream>>>(H, W, tile_size, tx, grid_pack, focus_params,
                                                                      w.tile_start, w.sorted_gid, w.header, w.cand,
                                                                      out_image);
     US3D_CHECK_LAUNCH("gp forward");
