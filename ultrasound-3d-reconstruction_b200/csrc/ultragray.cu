@@ -125,8 +125,10 @@ __device__ __forceinline__ float4 quat_grad(const float4 q, const float* g) {
 
 // Gauss-Legendre (3 points) integral of the canonical Gaussian along the ray over [0, l],
 // restricted to a window of radius wr around the closest approach (reference shared.cuh:27-85).
+// With wr > 0 the integral ends at min(l, tc + wr): for every pixel depth l >= tc + wr it is
+// one value per (ray, Gaussian), which *tcw_out (if not NULL) receives as tc + wr.
 __device__ __forceinline__ float ray_integral(const float3 ro, const float3 rd, const float3 mu, const float3 s,
-                                              const float* R, float l, float wr) {
+                                              const float* R, float l, float wr, float* tcw_out = nullptr) {
     if (l <= 0.0f) return 0.0f;
     const float3 diff = v_sub(ro, mu);
     float3 ol, dl;
@@ -144,6 +146,7 @@ __device__ __forceinline__ float ray_integral(const float3 ro, const float3 rd, 
     if (wr > 0.0f) {
         t0s = fmaxf(0.0f, tc - wr);
         t1s = fminf(l, tc + wr);
+        if (tcw_out) *tcw_out = tc + wr;
     }
     if (t1s <= t0s) return 0.0f;
     const float half = 0.5f * (t1s - t0s);
@@ -312,11 +315,14 @@ forward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __res
     __shared__ float4 s_rec[BATCH * REC_F4];
     __shared__ float s_tg[BATCH];
     __shared__ float s_depth[BATCH];
+    __shared__ float s_tcw[BATCH];   // window end tc + wr of the transmission integral (+inf: none)
+    __shared__ float s_far[BATCH];   // its factor tau + (1 - tau) exp(-psi) for pixels at or past it
     if (header[H_FLAGS] != 0) return;
     const int x = blockIdx.x;
     const int s0 = ray_start[x], n = ray_start[x + 1] - s0;
     const RayGeo rg = ray_geo(x, ray_o, ray_d, a_ele, pert);
-    for (int y0 = 0; y0 < H; y0 += blockDim.x) {
+    // blockIdx.y: which blockDim.x samples of the ray this block shades
+    for (int y0 = blockIdx.y * blockDim.x; y0 < H; y0 += gridDim.y * blockDim.x) {
         const int y = y0 + threadIdx.x;
         const bool valid = y < H;
         float3 p = make_float3(0.f, 0.f, 0.f);
@@ -338,6 +344,15 @@ forward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __res
                 const float4 a = s_rec[k * REC_F4];
                 s_tg[k] = v_dot(v_sub(make_float3(a.x, a.y, a.z), rg.o), rg.d);
                 s_depth[k] = (float)dkey[sorted_gid[s0 + b0 + k]] * 0.001f;
+                float tcw = 3.0e38f, far = 1.0f;
+                if (wr > 0.0f) {
+                    Rec r;
+                    load_rec(s_rec + k * REC_F4, r);
+                    const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, 3.0e38f, wr, &tcw);
+                    far = r.tau + (1.0f - r.tau) * __expf(-psi);
+                }
+                s_tcw[k] = tcw;
+                s_far[k] = far;
             }
             __syncthreads();
             if (!valid || n == 0) continue;
@@ -350,11 +365,20 @@ forward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __res
                 if (local_only) need_t = need_t && ((t_pixel - t_gauss) <= depth_radius + wr);
                 const bool need_e = fabsf(t_gauss - t_pixel) <= depth_radius;
                 if (!need_t && !need_e) continue;
+                // past the window end the factor is the ray's per-Gaussian constant
+                if (need_t && !need_e && t_pixel > 0.0f && t_pixel >= s_tcw[k]) {
+                    trans *= s_far[k];
+                    continue;
+                }
                 Rec r;
                 load_rec(s_rec + k * REC_F4, r);
                 if (need_t) {
-                    const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, t_pixel, wr);
-                    trans *= r.tau + (1.0f - r.tau) * __expf(-psi);
+                    if (t_pixel > 0.0f && t_pixel >= s_tcw[k]) {
+                        trans *= s_far[k];
+                    } else {
+                        const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, t_pixel, wr);
+                        trans *= r.tau + (1.0f - r.tau) * __expf(-psi);
+                    }
                 }
                 if (need_e) {
                     const float wgt = gauss_weight(p, r.mu, r.P);
@@ -374,6 +398,63 @@ forward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __res
         }
         image[(int64_t)y * W + x] = out;
         pixel_state[(int64_t)x * H + y] = make_float4(trans, num, den, sacc);
+    }
+}
+
+// VJP of ray_integral w.r.t. the Gaussian (mean, scales, rotation), the quadrature nodes held
+// fixed (reference backward.cu:26-108), accumulated into ds, dmu, dR; l is the pixel depth.
+// With wr > 0, *tcw_out (if not NULL) receives the window end tc + wr it uses.
+__device__ __forceinline__ void psi_vjp(const RayGeo& rg, const Rec& r, float t_pixel, float wr, float dpsi,
+                                        float ds[3], float dmu[3], float dR[9], float* tcw_out = nullptr) {
+    if (t_pixel > 0.0f) {
+        const float3 diff = v_sub(rg.o, r.mu);
+        float3 ol, dl;
+        ol.x = r.R[0] * diff.x + r.R[3] * diff.y + r.R[6] * diff.z;
+        ol.y = r.R[1] * diff.x + r.R[4] * diff.y + r.R[7] * diff.z;
+        ol.z = r.R[2] * diff.x + r.R[5] * diff.y + r.R[8] * diff.z;
+        dl.x = r.R[0] * rg.d.x + r.R[3] * rg.d.y + r.R[6] * rg.d.z;
+        dl.y = r.R[1] * rg.d.x + r.R[4] * rg.d.y + r.R[7] * rg.d.z;
+        dl.z = r.R[2] * rg.d.x + r.R[5] * rg.d.y + r.R[8] * rg.d.z;
+        const float3 is = make_float3(1.0f / r.s.x, 1.0f / r.s.y, 1.0f / r.s.z);
+        const float3 og = make_float3(ol.x * is.x, ol.y * is.y, ol.z * is.z);
+        const float3 dg = make_float3(dl.x * is.x, dl.y * is.y, dl.z * is.z);
+        const float dg2 = v_dot(dg, dg);
+        const float tc = -v_dot(og, dg) / (dg2 + 1e-8f);
+        float ta0 = 0.0f, ta1 = t_pixel;
+        if (wr > 0.0f) {
+            ta0 = fmaxf(0.0f, tc - wr);
+            ta1 = fminf(t_pixel, tc + wr);
+            if (tcw_out) *tcw_out = tc + wr;
+        }
+        if (ta1 > ta0 && dpsi != 0.0f) {
+            const float half = 0.5f * (ta1 - ta0), c = 0.5f * (ta1 + ta0);
+            const float tn[3] = {half * -0.7745966692f + c, half * 0.0f + c, half * 0.7745966692f + c};
+            const float wn[3] = {0.5555555556f, 0.8888888889f, 0.5555555556f};
+            const float coeff = dpsi * half;
+            float3 gog = make_float3(0.f, 0.f, 0.f), gdg = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+            for (int qn = 0; qn < 3; ++qn) {
+                const float3 xq = v_add(og, v_mul(dg, tn[qn]));
+                const float f = __expf(-0.5f * v_dot(xq, xq));
+                gog = v_add(gog, v_mul(xq, -coeff * wn[qn] * f));
+                gdg = v_add(gdg, v_mul(xq, -coeff * wn[qn] * f * tn[qn]));
+            }
+            const float3 gol = make_float3(gog.x * is.x, gog.y * is.y, gog.z * is.z);
+            const float3 gdl = make_float3(gdg.x * is.x, gdg.y * is.y, gdg.z * is.z);
+            ds[0] += gog.x * (-og.x * is.x) + gdg.x * (-dg.x * is.x);
+            ds[1] += gog.y * (-og.y * is.y) + gdg.y * (-dg.y * is.y);
+            ds[2] += gog.z * (-og.z * is.z) + gdg.z * (-dg.z * is.z);
+            dmu[0] += -(r.R[0] * gol.x + r.R[1] * gol.y + r.R[2] * gol.z);
+            dmu[1] += -(r.R[3] * gol.x + r.R[4] * gol.y + r.R[5] * gol.z);
+            dmu[2] += -(r.R[6] * gol.x + r.R[7] * gol.y + r.R[8] * gol.z);
+            const float dv[3] = {diff.x, diff.y, diff.z}, rv[3] = {rg.d.x, rg.d.y, rg.d.z};
+#pragma unroll
+            for (int rr = 0; rr < 3; ++rr) {
+                dR[rr * 3 + 0] += gol.x * dv[rr] + gdl.x * rv[rr];
+                dR[rr * 3 + 1] += gol.y * dv[rr] + gdl.y * rv[rr];
+                dR[rr * 3 + 2] += gol.z * dv[rr] + gdl.z * rv[rr];
+            }
+        }
     }
 }
 
@@ -411,12 +492,20 @@ backward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __re
             dP[i] = 0.f;
         }
         float t_gauss = 0.f, depth_radius = -1.f, depth = 0.f;
+        // far field (wr > 0, pixel past both window ends): constant factor and VJP
+        float far_tcw = 3.0e38f, far_tcw_vjp = 3.0e38f, far_T = 1.0f, far_exp = 1.0f, far_dT = 0.0f;
         if (own) {
             const int gk = sorted_gid[s0 + k];
             load_rec(rec + (int64_t)REC_F4 * gk, r);
             depth = (float)dkey[gk] * 0.001f;
             t_gauss = v_dot(v_sub(r.mu, rg.o), rg.d);
             depth_radius = r.smax * k_sigma;
+            if (wr > 0.0f) {
+                const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, 3.0e38f, wr, &far_tcw);
+                far_exp = __expf(-psi);
+                far_T = r.tau + (1.0f - r.tau) * far_exp;
+                psi_vjp(rg, r, 3.0e38f, wr, 0.0f, ds, dmu, dR, &far_tcw_vjp);
+            }
         }
         for (int y0 = 0; y0 < H; y0 += PIX_CHUNK) {
             const int ny = min(PIX_CHUNK, H - y0);
@@ -455,7 +544,11 @@ backward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __re
                 const bool need_e = fabsf(t_gauss - t_pixel) <= depth_radius;
                 if (!need_t && !need_e) continue;
                 const float4 cf = s_c[j];
-                if (need_t) {
+                if (need_t && t_pixel > 0.0f && t_pixel >= far_tcw && t_pixel >= far_tcw_vjp) {
+                    // past both window ends: the factor and its VJP are the instance's constants,
+                    // so only the scalar adjoint is summed here (applied once after the sweep)
+                    if (far_T > 1e-6f) far_dT += cf.x * (cf.y / far_T);
+                } else if (need_t) {
                     const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, t_pixel, wr);
                     const float exp_psi = __expf(-psi);
                     const float T_i = r.tau + (1.0f - r.tau) * exp_psi;
@@ -464,55 +557,7 @@ backward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __re
                     dtau_raw += dTi * (1.0f - exp_psi) * (r.tau * (1.0f - r.tau));
                     const float dpsi = dTi * (1.0f - r.tau) * exp_psi * (-1.0f);
                     // integral VJP with the quadrature nodes held fixed (reference backward.cu:26-108)
-                    if (t_pixel > 0.0f) {
-                        const float3 diff = v_sub(rg.o, r.mu);
-                        float3 ol, dl;
-                        ol.x = r.R[0] * diff.x + r.R[3] * diff.y + r.R[6] * diff.z;
-                        ol.y = r.R[1] * diff.x + r.R[4] * diff.y + r.R[7] * diff.z;
-                        ol.z = r.R[2] * diff.x + r.R[5] * diff.y + r.R[8] * diff.z;
-                        dl.x = r.R[0] * rg.d.x + r.R[3] * rg.d.y + r.R[6] * rg.d.z;
-                        dl.y = r.R[1] * rg.d.x + r.R[4] * rg.d.y + r.R[7] * rg.d.z;
-                        dl.z = r.R[2] * rg.d.x + r.R[5] * rg.d.y + r.R[8] * rg.d.z;
-                        const float3 is = make_float3(1.0f / r.s.x, 1.0f / r.s.y, 1.0f / r.s.z);
-                        const float3 og = make_float3(ol.x * is.x, ol.y * is.y, ol.z * is.z);
-                        const float3 dg = make_float3(dl.x * is.x, dl.y * is.y, dl.z * is.z);
-                        const float dg2 = v_dot(dg, dg);
-                        const float tc = -v_dot(og, dg) / (dg2 + 1e-8f);
-                        float ta0 = 0.0f, ta1 = t_pixel;
-                        if (wr > 0.0f) {
-                            ta0 = fmaxf(0.0f, tc - wr);
-                            ta1 = fminf(t_pixel, tc + wr);
-                        }
-                        if (ta1 > ta0) {
-                            const float half = 0.5f * (ta1 - ta0), c = 0.5f * (ta1 + ta0);
-                            const float tn[3] = {half * -0.7745966692f + c, half * 0.0f + c, half * 0.7745966692f + c};
-                            const float wn[3] = {0.5555555556f, 0.8888888889f, 0.5555555556f};
-                            const float coeff = dpsi * half;
-                            float3 gog = make_float3(0.f, 0.f, 0.f), gdg = make_float3(0.f, 0.f, 0.f);
-#pragma unroll
-                            for (int qn = 0; qn < 3; ++qn) {
-                                const float3 xq = v_add(og, v_mul(dg, tn[qn]));
-                                const float f = __expf(-0.5f * v_dot(xq, xq));
-                                gog = v_add(gog, v_mul(xq, -coeff * wn[qn] * f));
-                                gdg = v_add(gdg, v_mul(xq, -coeff * wn[qn] * f * tn[qn]));
-                            }
-                            const float3 gol = make_float3(gog.x * is.x, gog.y * is.y, gog.z * is.z);
-                            const float3 gdl = make_float3(gdg.x * is.x, gdg.y * is.y, gdg.z * is.z);
-                            ds[0] += gog.x * (-og.x * is.x) + gdg.x * (-dg.x * is.x);
-                            ds[1] += gog.y * (-og.y * is.y) + gdg.y * (-dg.y * is.y);
-                            ds[2] += gog.z * (-og.z * is.z) + gdg.z * (-dg.z * is.z);
-                            dmu[0] += -(r.R[0] * gol.x + r.R[1] * gol.y + r.R[2] * gol.z);
-                            dmu[1] += -(r.R[3] * gol.x + r.R[4] * gol.y + r.R[5] * gol.z);
-                            dmu[2] += -(r.R[6] * gol.x + r.R[7] * gol.y + r.R[8] * gol.z);
-                            const float dv[3] = {diff.x, diff.y, diff.z}, rv[3] = {rg.d.x, rg.d.y, rg.d.z};
-#pragma unroll
-                            for (int rr = 0; rr < 3; ++rr) {
-                                dR[rr * 3 + 0] += gol.x * dv[rr] + gdl.x * rv[rr];
-                                dR[rr * 3 + 1] += gol.y * dv[rr] + gdl.y * rv[rr];
-                                dR[rr * 3 + 2] += gol.z * dv[rr] + gdl.z * rv[rr];
-                            }
-                        }
-                    }
+                    psi_vjp(rg, r, t_pixel, wr, dpsi, ds, dmu, dR);
                 }
                 if (need_e) {
                     const float3 p = make_float3(pt.x, pt.y, pt.z);
@@ -540,6 +585,10 @@ backward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __re
             }
         }
         if (!own) continue;
+        if (far_dT != 0.0f) {
+            dtau_raw += far_dT * (1.0f - far_exp) * (r.tau * (1.0f - r.tau));
+            psi_vjp(rg, r, 3.0e38f, wr, far_dT * (1.0f - r.tau) * far_exp * (-1.0f), ds, dmu, dR);
+        }
         // dL/dP (symmetric sum over pixels) -> dL/dR, dL/ds; dL/dR -> dL/dq.
         dP[3] = dP[1];
         dP[6] = dP[2];
@@ -671,7 +720,7 @@ extern "C" int us3d_ugr_forward(void* workspace, size_t workspace_bytes, int64_t
                                         w.ray_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(W, w.ray_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_ugr_sort_attr, stream));
-    forward_kernel<<<(unsigned)W, 256, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions,
+    forward_kernel<<<dim3((unsigned)W, (unsigned)((H + 255) / 256)), 256, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions,
                                                     ray_origins, ray_dirs, axis_ele, ray_perturbations, w.dkey,
                                                     k_sigma, quadrature_window_radius_mm, local_window_only ? 1 : 0,
                                                     local_max_window_mm, out_image, w.pixel_state);
