@@ -303,9 +303,14 @@ __device__ __forceinline__ RayGeo ray_geo(int x, const float* __restrict__ ray_o
     return r;
 }
 
-// One block per ray; threads own pixels of the ray (row y of column x), instances of the
-// ray are staged in shared memory and walked in list order (reference forward.cu:22-119).
-__global__ void __launch_bounds__(256)
+// Block (x, y) shades samples [FWD_SAMPLES y, FWD_SAMPLES (y + 1)) of ray x, one per thread;
+// the ray's instances are staged in shared memory and walked in list order (reference
+// forward.cu:22-119).
+#ifndef US3D_UGR_FWD_SAMPLES
+#define US3D_UGR_FWD_SAMPLES 64
+#endif
+constexpr int FWD_SAMPLES = US3D_UGR_FWD_SAMPLES;
+__global__ void __launch_bounds__(FWD_SAMPLES)
 forward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __restrict__ sorted_gid,
                const long long* __restrict__ header, const float4* __restrict__ rec,
                const float* __restrict__ pixels, const float* __restrict__ ray_o, const float* __restrict__ ray_d,
@@ -462,8 +467,9 @@ __device__ __forceinline__ void psi_vjp(const RayGeo& rg, const Rec& r, float t_
 // Backward
 // ------------------------------------------------------------------------------------
 
-// One block per ray; thread k owns instance k of the ray and sweeps the ray's pixels in
-// chunks whose adjoint coefficients are staged in shared memory (reference backward.cu:138-325).
+// Blocks (x, *) share ray x's instances; a thread owns one instance at a time and sweeps
+// the ray's pixels in chunks whose adjoint coefficients are staged in shared memory
+// (reference backward.cu:138-325).
 __global__ void __launch_bounds__(128)
 backward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __restrict__ sorted_gid,
                 const int* __restrict__ sorted_inst, const long long* __restrict__ header,
@@ -480,7 +486,8 @@ backward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __re
     const int s0 = ray_start[x], n = ray_start[x + 1] - s0;
     if (n <= 0) return;
     const RayGeo rg = ray_geo(x, ray_o, ray_d, a_ele, pert);
-    for (int kb = 0; kb < n; kb += blockDim.x) {
+    // blocks (x, y) share ray x's instances: block y takes rounds y, y + gridDim.y, ...
+    for (int kb = blockIdx.y * blockDim.x; kb < n; kb += gridDim.y * blockDim.x) {
         const int k = kb + threadIdx.x;
         const bool own = k < n;
         Rec r;
@@ -720,7 +727,7 @@ extern "C" int us3d_ugr_forward(void* workspace, size_t workspace_bytes, int64_t
                                         w.ray_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(W, w.ray_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_ugr_sort_attr, stream));
-    forward_kernel<<<dim3((unsigned)W, (unsigned)((H + 255) / 256)), 256, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions,
+    forward_kernel<<<dim3((unsigned)W, (unsigned)((H + FWD_SAMPLES - 1) / FWD_SAMPLES)), FWD_SAMPLES, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions,
                                                     ray_origins, ray_dirs, axis_ele, ray_perturbations, w.dkey,
                                                     k_sigma, quadrature_window_radius_mm, local_window_only ? 1 : 0,
                                                     local_max_window_mm, out_image, w.pixel_state);
@@ -759,7 +766,9 @@ extern "C" int us3d_ugr_backward(void* workspace, int64_t n_gauss, const float* 
     cudaStream_t stream = (cudaStream_t)stream_;
     float4* partial = reinterpret_cast<float4*>(scratch);
     const int prof = prof_begin("ugr_backward", stream);
-    backward_kernel<<<(unsigned)W, 128, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.sorted_inst, w.header, w.rec,
+    // enough blocks per ray to give every SM several (a frame has few rays)
+    const unsigned by = (unsigned)std::max<int64_t>(1, std::min<int64_t>(64, (148 * 8 + W - 1) / std::max<int64_t>(W, 1)));
+    backward_kernel<<<dim3((unsigned)W, by), 128, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.sorted_inst, w.header, w.rec,
                                                      quats, pixel_positions, ray_origins, ray_dirs, axis_ele,
                                                      ray_perturbations, w.dkey, w.pixel_state, grad_image, k_sigma,
                                                      quadrature_window_radius_mm, local_window_only ? 1 : 0,
