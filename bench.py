@@ -224,6 +224,12 @@ def run_b200(a):
         barrier()
         return max_over_ranks(st.elapsed_time(en), device=dev)
 
+    # -- launch-shape autotuning on the first batch (untimed; changes no result) --
+    from us3d_b200.batch import autotune_launch
+
+    tuned = autotune_launch(batches[0][0], params, batches[0][1])
+    launch_shape = min(tuned, key=tuned.get)
+
     # -- warm-up + stage selection for the roofline (untimed) --
     stage_ms = {}
     for stage in ("ug_bin", "ug_forward", "ug_backward"):
@@ -305,6 +311,8 @@ def run_b200(a):
         "config": workload_config(a, world), "instances_per_frame": round(I, 1), "roofline": roofline,
         "clocks": clocks, "gpu_launches": gpu_launches,
         "batched_form": "CUDA-graph replay of bin + forward + L1 gradient + backward per 16-frame batch",
+        "launch_config": {"forward_batch": launch_shape[0], "backward_threads": launch_shape[1],
+                          "autotune_ms_per_step": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in tuned.items()}},
         "uncaptured": {"value": round(uncaptured_value, 3), "unit": UNIT,
                        "note": "same step launched from Python with one instance-total readback; "
                                "the roofline stage times come from this run's CUDA events"},

@@ -192,6 +192,17 @@ US3D_API int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames_de
                      float* d_intensities, void* stream);
 
 /*
+ * Launch shapes of the UltraGauss shading kernels, process-wide (read at every launch; set
+ * them before capturing a CUDA graph): Gaussians staged per forward batch (128, 256 or 512)
+ * and threads per backward CTA (128 or 256). Results do not depend on them. The defaults
+ * (512, 256) are the fastest measured on the headline scene; us3d_b200.batch.autotune_launch
+ * times every pair on a caller's workload and keeps the fastest. No counterpart in the
+ * reference (its kernels have fixed launch shapes).
+ */
+US3D_API int us3d_ug_set_launch_config(int32_t forward_batch, int32_t backward_threads);
+US3D_API int us3d_ug_get_launch_config(int32_t* forward_batch, int32_t* backward_threads);
+
+/*
  * Per-frame image loss of the reference's training step (image_loss in
  * pipeline_god_file.py:606-617 with simple_ssim at :627-637): for each frame f of the table,
  * loss_f = l1_weight * mean|x - y| + ssim_weight * (1 - SSIM_f), SSIM_f the global SSIM of

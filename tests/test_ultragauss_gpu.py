@@ -417,3 +417,31 @@ def test_graphed_training_step_matches_eager(cuda_device):
         for a_, b_ in zip(got, ref):
             assert torch.equal(a_, b_), it
         params[0].add_(0.01)  # in-place update seen by the next replay
+
+
+def test_launch_shapes_same_results_and_autotune(cuda_device):
+    """Every launch shape of the shading kernels (forward batch 128/256/512, backward CTA
+    128/256 threads) gives bit-identical images and gradients; the autotuner times all of them
+    and keeps the fastest."""
+    from us3d_b200 import batch as B
+    from us3d_b200 import ultragauss as UG
+
+    args, ft, pix, grads = _cull_case(cuda_device, G=60000)
+    default = B.get_launch_config()
+    outs = {}
+    try:
+        for shape in B.LAUNCH_SHAPES:
+            B.set_launch_config(*shape)
+            b = UG.bin_gaussians(*args, ft, 7.815, 1e-4, True, slice_cull_pixels=pix)
+            img, alpha, depth, _ = UG.forward(b, pix, 1e-6, 0.0, want_counts=False)
+            g = UG.backward(b, pix, grads[0], grads[1], grads[2], alpha, 1e-6, 0.0)
+            outs[shape] = [x.cpu().numpy() for x in (img, alpha, depth, *g)]
+        ref = outs[default]
+        for shape, o in outs.items():
+            for x, y in zip(o, ref):
+                assert np.array_equal(x, y), shape
+        timings = B.autotune_launch(ft, list(args), pix, reps=1)
+        assert set(timings) == set(B.LAUNCH_SHAPES)
+        assert B.get_launch_config() == min(timings, key=timings.get)
+    finally:
+        B.set_launch_config(*default)

@@ -24,6 +24,8 @@
 // counts agree bit for bit.
 #include <algorithm>
 
+#include <atomic>
+
 #include "us3d_common.cuh"
 #include "scan.cuh"
 #include "binning.cuh"
@@ -31,25 +33,19 @@
 namespace us3d {
 namespace ug {
 
-// Threads of a backward CTA, and resident CTAs per SM the shading kernels are compiled for
-// (register budget 65536 / (threads x n)); Gaussians staged per forward batch.
-#ifndef US3D_UG_BWD_THREADS
-#define US3D_UG_BWD_THREADS 256
-#endif
+// Resident CTAs per SM the forward is compiled for (register budget 65536 / (256 x n)).
 #ifndef US3D_UG_FWD_MIN_CTAS
 #define US3D_UG_FWD_MIN_CTAS 5
-#endif
-#ifndef US3D_UG_BWD_MIN_CTAS
-#define US3D_UG_BWD_MIN_CTAS (1024 / US3D_UG_BWD_THREADS)
-#endif
-#ifndef US3D_UG_FWD_BATCH
-#define US3D_UG_FWD_BATCH 512
 #endif
 
 constexpr int TILE = 16;           // reference SLICE_TILE_SIZE (include/mapper/core.cuh:5)
 constexpr int TILE_PIX = TILE * TILE;
-constexpr int FWD_BATCH = US3D_UG_FWD_BATCH;  // Gaussians staged per shared-memory batch
-constexpr int BWD_THREADS = US3D_UG_BWD_THREADS;
+// Launch shapes the shading kernels are instantiated for (us3d_ug_set_launch_config picks
+// one of each at run time; the defaults are the fastest measured on the headline scene):
+// Gaussians staged per forward batch, and threads of a backward CTA (compiled for 1024 /
+// threads resident CTAs per SM).
+constexpr int FWD_BATCH = 512;
+constexpr int BWD_THREADS = 256;
 // A tile's pixels are shaded by 8 warps, each owning a block of 8 columns x 4 rows; bit
 // (band * 2 + half) of an instance's block mask is set when the Gaussian can reach block
 // (4-row band `band`, 8-column half `half`) of that tile.
@@ -675,6 +671,7 @@ __device__ __forceinline__ int block_row(int k) { return (k >> 6) * BLK_H + ((k 
 
 // One block per tile, one thread per pixel; warp w owns warp block w of the tile and visits
 // only the staged Gaussians whose block mask has bit w (the others reach none of its pixels).
+template <int BATCH>
 __global__ void __launch_bounds__(TILE_PIX, US3D_UG_FWD_MIN_CTAS)
 forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
@@ -682,8 +679,8 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
                const float4* __restrict__ pack, const float* __restrict__ pixels, float chi2, float beta,
                float bg_alpha, float bg_intensity, float* __restrict__ out_image, float* __restrict__ out_alpha,
                float* __restrict__ out_depth, int* __restrict__ out_counts, float2* __restrict__ pixel_aux) {
-    __shared__ Staged sg[FWD_BATCH];
-    __shared__ unsigned char s_blocks[FWD_BATCH];
+    __shared__ Staged sg[BATCH];
+    __shared__ unsigned char s_blocks[BATCH];
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
     const Geo geo = load_geo(frames + tile_frame[t]);
@@ -722,8 +719,8 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     };
     // Without a slice cull every mask is full: plain sweep, same order and sums.
     const bool culled = header[H_MODE] != 0;
-    for (int b0 = 0; b0 < n; b0 += FWD_BATCH) {
-        const int nb = min(FWD_BATCH, n - b0);
+    for (int b0 = 0; b0 < n; b0 += BATCH) {
+        const int nb = min(BATCH, n - b0);
         __syncthreads();
         for (int j = threadIdx.x; j < nb; j += blockDim.x) {
             sg[j] = stage_gaussian(pack, sorted_gid[s0 + b0 + j], geo, chi2, beta);
@@ -766,8 +763,8 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
 // LOSS: dL/dimage comes from the fused per-frame loss (L1 + global SSIM of image against
 // target, coefficients per frame in loss_coef; see us3d_ug_loss) and dL/dalpha = dL/ddepth =
 // 0; otherwise from d_image, d_alpha, d_depth.
-template <bool LOSS>
-__global__ void __launch_bounds__(BWD_THREADS, US3D_UG_BWD_MIN_CTAS)
+template <bool LOSS, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                 const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
                 const int* __restrict__ sorted_inst, const unsigned char* __restrict__ sorted_mask,
@@ -791,7 +788,7 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
     const Geo geo = load_geo(frames + tile_frame[t]);
     int tx, ty;
     find_tile_coords(geo, t, tx, ty);
-    for (int slot = threadIdx.x; slot < TILE_PIX; slot += BWD_THREADS) {
+    for (int slot = threadIdx.x; slot < TILE_PIX; slot += THREADS) {
         const int r = block_row(slot), c = block_col(slot);
         const int e0 = (slot >> 5) * 64 + (slot & 31), e1 = e0 + 32;
         const int64_t p = (int64_t)geo.pix_off + (int64_t)(ty * TILE + r) * geo.W + (tx * TILE + c);
@@ -1029,6 +1026,26 @@ using namespace us3d::ug;
 // Per-device flag: the large-bucket sort kernel's shared-memory limit has been raised.
 static bool g_sort_attr_done[128];
 
+// Launch shapes of the shading kernels (process-wide; read at every launch).
+static std::atomic<int> g_fwd_batch{FWD_BATCH};
+static std::atomic<int> g_bwd_threads{BWD_THREADS};
+
+extern "C" int us3d_ug_set_launch_config(int32_t forward_batch, int32_t backward_threads) {
+    US3D_CHECK_ARG(forward_batch == 128 || forward_batch == 256 || forward_batch == 512,
+                   "forward_batch must be 128, 256 or 512 (got %d)", forward_batch);
+    US3D_CHECK_ARG(backward_threads == 128 || backward_threads == 256,
+                   "backward_threads must be 128 or 256 (got %d)", backward_threads);
+    g_fwd_batch.store(forward_batch);
+    g_bwd_threads.store(backward_threads);
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_get_launch_config(int32_t* forward_batch, int32_t* backward_threads) {
+    if (forward_batch) *forward_batch = g_fwd_batch.load();
+    if (backward_threads) *backward_threads = g_bwd_threads.load();
+    return US3D_OK;
+}
+
 extern "C" size_t us3d_ug_workspace_bytes(int64_t n_gauss, int32_t n_frames, int64_t n_tiles,
                                           int64_t n_pixels, int64_t instance_capacity) {
     (void)n_frames;
@@ -1162,9 +1179,16 @@ extern "C" int us3d_ug_forward(void* workspace, const us3d_slice_frame* frames, 
     if (n_tiles == 0) return US3D_OK;
     cudaStream_t stream = (cudaStream_t)stream_;
     const int prof = prof_begin("ug_forward", stream);
-    forward_kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(
-        n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_mask, w.header, w.pack, pixels,
-        chi2, beta, bg_alpha, bg_intensity, out_image, out_alpha, out_depth, out_counts, w.pixel_aux);
+    auto launch = [&](auto kernel) {
+        kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(
+            n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_mask, w.header, w.pack,
+            pixels, chi2, beta, bg_alpha, bg_intensity, out_image, out_alpha, out_depth, out_counts, w.pixel_aux);
+    };
+    switch (g_fwd_batch.load()) {
+        case 128: launch(forward_kernel<128>); break;
+        case 256: launch(forward_kernel<256>); break;
+        default: launch(forward_kernel<512>); break;
+    }
     US3D_CHECK_LAUNCH("ug forward");
     prof_end(prof, stream);
     count_launches(1);
@@ -1196,16 +1220,17 @@ static int ug_backward_impl(void* workspace, const us3d_slice_frame* frames, int
     float4* partial = reinterpret_cast<float4*>(scratch);
     const int prof = prof_begin("ug_backward", stream);
     if (n_tiles > 0) {
-        if (fused)
-            backward_kernel<true><<<(unsigned)n_tiles, BWD_THREADS, 0, stream>>>(
-                n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_inst, w.sorted_mask,
-                w.header, w.pack, pixels, nullptr, nullptr, nullptr, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha,
-                bg_intensity, loss_image, loss_target, loss_coef, partial);
-        else
-            backward_kernel<false><<<(unsigned)n_tiles, BWD_THREADS, 0, stream>>>(
+        const int threads = g_bwd_threads.load();
+        auto launch = [&](auto kernel, int nthreads) {
+            kernel<<<(unsigned)n_tiles, nthreads, 0, stream>>>(
                 n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_inst, w.sorted_mask,
                 w.header, w.pack, pixels, d_image, d_alpha, d_depth, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha,
-                bg_intensity, nullptr, nullptr, nullptr, partial);
+                bg_intensity, loss_image, loss_target, loss_coef, partial);
+        };
+        if (fused)
+            threads == 128 ? launch(backward_kernel<true, 128>, 128) : launch(backward_kernel<true, 256>, 256);
+        else
+            threads == 128 ? launch(backward_kernel<false, 128>, 128) : launch(backward_kernel<false, 256>, 256);
         US3D_CHECK_LAUNCH("ug backward");
     }
     if (n_gauss > 0) {

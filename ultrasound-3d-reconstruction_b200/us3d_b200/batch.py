@@ -115,3 +115,62 @@ class GraphedTrainingStep:
         if flags:
             raise RuntimeError(f"graphed step: binning flags {flags} ({total} instances, capacity {self.capacity})")
         return total
+
+
+LAUNCH_SHAPES = [(b, t) for b in (128, 256, 512) for t in (128, 256)]
+
+
+def get_launch_config():
+    """(forward batch, backward threads) the UltraGauss shading kernels launch with."""
+    import ctypes
+
+    from . import _lib
+
+    fb, bt = ctypes.c_int32(0), ctypes.c_int32(0)
+    _lib.check(_lib.call("us3d_ug_get_launch_config", ctypes.byref(fb), ctypes.byref(bt)), "us3d_ug_get_launch_config")
+    return int(fb.value), int(bt.value)
+
+
+def set_launch_config(forward_batch: int, backward_threads: int) -> None:
+    from . import _lib
+
+    _lib.check(_lib.call("us3d_ug_set_launch_config", int(forward_batch), int(backward_threads)),
+               "us3d_ug_set_launch_config")
+
+
+def autotune_launch(frames: UG.FrameTable, params, pixels: torch.Tensor, reps: int = 3,
+                    chi2_threshold: float = 7.815, diag_beta: float = 1e-4, bg_alpha: float = 1e-6):
+    """Times the batched step (slice-culled bin, forward, backward with a seeded upstream
+    gradient) on the caller's frames for every launch shape the library is built for, keeps the
+    fastest (set_launch_config) and returns {(forward_batch, backward_threads): ms per step}.
+    The shapes change no result, only speed. Synchronises; run it before capturing graphs."""
+    means, tril, opac, inten = params[0], params[1].contiguous(), params[2].reshape(-1), params[3].reshape(-1)
+    g = torch.Generator(device=pixels.device)
+    g.manual_seed(0)
+    d_image = torch.randn(frames.n_pixels, generator=g, device=pixels.device)
+    zeros = torch.zeros_like(d_image)
+    b = UG.bin_gaussians(means, tril, opac, inten, frames, chi2_threshold, diag_beta, True,
+                         slice_cull_pixels=pixels)
+    cap = b.capacity
+
+    def step():
+        bb = UG.bin_gaussians(means, tril, opac, inten, frames, chi2_threshold, diag_beta, True, capacity=cap,
+                              sync_check=False, slice_cull_pixels=pixels)
+        img, alpha, depth, _ = UG.forward(bb, pixels, bg_alpha, 0.0, want_counts=False)
+        UG.backward(bb, pixels, d_image, zeros, zeros, alpha, bg_alpha, 0.0)
+
+    timings = {}
+    for shape in LAUNCH_SHAPES:
+        set_launch_config(*shape)
+        step()
+        torch.cuda.synchronize(pixels.device)
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st.record()
+        for _ in range(reps):
+            step()
+        en.record()
+        en.synchronize()
+        timings[shape] = st.elapsed_time(en) / reps
+    best = min(timings, key=timings.get)
+    set_launch_config(*best)
+    return timings
