@@ -287,6 +287,16 @@ US3D_API int us3d_frames_gather(const us3d_slice_frame* all_frames, int64_t n_al
                                 float* out_pixel_positions, float* out_targets, int32_t* status, void* stream);
 
 /*
+ * Densification statistics of a training step (the refinement the UltraG-Ray paper
+ * describes, absent from the reference's code): for each of the n_gauss Gaussians,
+ * importance[g] += |dL/dmean_g| (Euclidean norm of its row of grad_means, (G,3)) and
+ * visits[g] += 1 when that norm is non-zero. Never synchronises. No counterpart in the
+ * reference.
+ */
+US3D_API int us3d_ug_refine_stats(const float* grad_means, int64_t n_gauss, float* importance, int32_t* visits,
+                                  void* stream);
+
+/*
  * Per-pixel candidate lists in the reference's CSR layout (pixel_gauss_indices of
  * MapperForwardCUDA, src/mapper/core.cu:237-287): for each pixel, in tile-list order,
  * the Gaussians passing the window test. `offsets` is the exclusive scan of the counts

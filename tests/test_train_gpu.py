@@ -219,3 +219,45 @@ def test_trainer_graph_replay_equals_eager(cuda_device):
         out.append([t.cpu().numpy() for t in params.tensors()])
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+def test_refine_stats_kernel(cuda_device):
+    from us3d_b200.refine import RefineStats
+
+    dev = cuda_device
+    g = torch.Generator().manual_seed(3)
+    grads = torch.randn((5000, 3), generator=g)
+    grads[::7] = 0.0
+    st = RefineStats(5000, dev)
+    for _ in range(3):
+        st.accumulate(grads.to(dev))
+    n = grads.norm(dim=1)
+    assert torch.allclose(st.importance.cpu(), 3 * n, rtol=1e-6, atol=0)
+    assert torch.equal(st.visits.cpu(), 3 * (n > 0).int())
+
+
+def test_trainer_with_refinement(cuda_device):
+    """Densification and pruning inside graph-replayed training: the Gaussian count changes,
+    graphs are captured again, the capacity check holds, and training continues."""
+    from us3d_b200 import scenes
+    from us3d_b200.refine import RefineConfig
+    from us3d_b200.train import TrainConfig, UltraGaussParameters, UltraGaussTrainer
+
+    dev = cuda_device
+    specs, pix = _specs(((96, 128, 0.25), (80, 80, 0.3)), seed=4)
+    pix = pix.to(dev)
+    sc = scenes.make_scene(20000, seed=4, cube_mm=32.0)
+    params = UltraGaussParameters.from_points(sc.means.to(dev), sc.intensities.to(dev), init_scale_mm=0.8)
+    tgt = torch.rand(pix.shape[0], generator=torch.Generator().manual_seed(9)).to(dev)
+    rc = RefineConfig(every=2, start=2, stop=4, grad_threshold=1e-6, split_scale_mm=0.9, max_gaussians=24000)
+    tr = UltraGaussTrainer(params, [(specs, pix, tgt)], TrainConfig(lr=1e-2), refine=rc)
+    for _ in range(6):
+        tr.step(0)
+    tr.check()
+    assert [r["step"] for r in tr.refine_log] == [2, 4]
+    assert params.means.shape[0] == tr.refine_log[-1]["total"] != 20000
+    assert all(r["cloned"] + r["split"] > 0 for r in tr.refine_log)
+    assert params.means.shape[0] <= 24000
+    for t in params.tensors():
+        assert torch.isfinite(t).all()
+    assert torch.isfinite(tr.losses(0)).all()

@@ -99,6 +99,21 @@ __global__ void loss_final_kernel(const us3d_slice_frame* __restrict__ frames, i
     coef[f] = make_float4((float)a, (float)b0, (float)cx, (float)cy);
 }
 
+// Densification statistics: importance[g] += |dL/dmean_g|, visits[g] += 1 if that gradient is
+// non-zero (the Gaussian reached a pixel of the step's frames).
+__global__ void __launch_bounds__(256)
+refine_stats_kernel(int64_t G, const float* __restrict__ grad_means, float* __restrict__ importance,
+                    int* __restrict__ visits) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    const float x = grad_means[3 * g], y = grad_means[3 * g + 1], z = grad_means[3 * g + 2];
+    const float n = sqrtf(x * x + y * y + z * z);
+    if (n > 0.0f) {
+        importance[g] += n;
+        visits[g] += 1;
+    }
+}
+
 struct AdamTable {
     us3d_adam_tensor t[US3D_ADAM_MAX_TENSORS];
     int64_t start[US3D_ADAM_MAX_TENSORS + 1];
@@ -200,6 +215,18 @@ extern "C" int us3d_adam_step(const us3d_adam_tensor* tensors, int32_t n_tensors
                                                                      (float)(1.0 - beta2), (float)eps, step_size,
                                                                      bc2_sqrt);
     US3D_CHECK_LAUNCH("adam");
+    count_launches(1);
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_refine_stats(const float* grad_means, int64_t n_gauss, float* importance, int32_t* visits,
+                                    void* stream_) {
+    US3D_CHECK_ARG(n_gauss >= 0, "negative size");
+    if (n_gauss == 0) return US3D_OK;
+    US3D_CHECK_ARG(grad_means && importance && visits, "pointer is NULL");
+    refine_stats_kernel<<<(unsigned)((n_gauss + 255) / 256), 256, 0, (cudaStream_t)stream_>>>(n_gauss, grad_means,
+                                                                                              importance, visits);
+    US3D_CHECK_LAUNCH("refine stats");
     count_launches(1);
     return US3D_OK;
 }

@@ -132,12 +132,19 @@ class UltraGaussTrainer:
     priming binning times ``margin``; ``check()`` reads the flags of every batch's last replay
     (one synchronisation per batch) and raises if a binning outgrew its capacity. ``losses()``
     returns the last replay's per-frame statistics (synchronises). ``from_source`` trains on
-    random batches drawn on the device from a ``frames.DeviceFrameSource``."""
+    random batches drawn on the device from a ``frames.DeviceFrameSource``. With ``refine``
+    (a refine.RefineConfig) the Gaussians are densified and pruned on its schedule: the
+    statistics are accumulated on the device every step, and after a refinement the parameter
+    and gradient buffers are new, so every batch's graph is captured again and its instance
+    capacity primed again (``refine_log`` lists the counts of each refinement)."""
 
     def __init__(self, params: UltraGaussParameters, batches, cfg: Optional[TrainConfig] = None,
-                 margin: float = 1.25, graph: bool = True):
+                 margin: float = 1.25, graph: bool = True, refine=None):
         self.params = params
         self.cfg = cfg or TrainConfig()
+        self.margin = float(margin)
+        self.refine_cfg = refine
+        self.refine_log = []
         dev = params.means.device
         G = params.means.shape[0]
         self.grads = (torch.empty((G, 3), device=dev), torch.empty((G, 6), device=dev), torch.empty((G,), device=dev),
@@ -156,11 +163,18 @@ class UltraGaussTrainer:
                                       coef=torch.zeros((frames.n_frames, 4), device=dev), graph=None))
         self.graph = graph
         self.steps_done = 0
+        self.refine_stats = None
+        if refine is not None:
+            from .refine import RefineStats
+
+            self.refine_stats = RefineStats(G, dev)
+            self.refine_gen = torch.Generator(device=dev)
+            self.refine_gen.manual_seed(0)
 
     @classmethod
     def from_source(cls, params: UltraGaussParameters, source, batch_size: int, cfg: Optional[TrainConfig] = None,
                     margin: float = 1.5, prime_batches: int = 4, seed: int = 0, graph: bool = True,
-                    indices: Optional[torch.Tensor] = None) -> "UltraGaussTrainer":
+                    indices: Optional[torch.Tensor] = None, refine=None) -> "UltraGaussTrainer":
         """Trains on batches of ``batch_size`` frames of ``source`` (a DeviceFrameSource): each
         step draws dataset indices on the device (uniformly among ``indices``, all frames by
         default; the reference draws one frame per step with np.random.choice) and assembles the
@@ -184,9 +198,10 @@ class UltraGaussTrainer:
                                  params.raw_intensities.reshape(-1), table, c.chi2_threshold, c.diag_beta,
                                  c.sort_by_depth, slice_cull_pixels=pixels, logit_attributes=True)
             best = max(best, b.total)
-        self = cls(params, [(table, pixels, targets)], c, margin=1.0, graph=graph)
+        self = cls(params, [(table, pixels, targets)], c, margin=1.0, graph=graph, refine=refine)
         self._batches[0]["capacity"] = int(best * margin) + 1024
-        self.source = dict(source=source, pool=pool, gen=gen, draw=draw)
+        self.source = dict(source=source, pool=pool, gen=gen, draw=draw, prime_batches=max(1, int(prime_batches)),
+                           margin=float(margin))
         return self
 
     def _render_args(self):
@@ -229,6 +244,38 @@ class UltraGaussTrainer:
             bt["graph"].replay()
         self.optimizer.step(self.grads)
         self.steps_done += 1
+        if self.refine_stats is not None:
+            self.refine_stats.accumulate(self.grads[0])
+            if self.refine_cfg.due(self.steps_done):
+                self._refine()
+
+    def _refine(self) -> None:
+        from .refine import refine
+
+        self.refine_log.append(dict(step=self.steps_done, **refine(self.params, self.optimizer, self.refine_stats,
+                                                                    self.refine_cfg, self.refine_gen)))
+        dev = self.params.means.device
+        G = self.params.means.shape[0]
+        self.grads = (torch.empty((G, 3), device=dev), torch.empty((G, 6), device=dev),
+                      torch.empty((G,), device=dev), torch.empty((G,), device=dev))
+        c = self.cfg
+        for bt in self._batches:
+            bt["graph"] = None  # parameter and gradient buffers moved: capture again
+            bt["binning"] = None
+            if self.source is None:
+                prime = UG.bin_gaussians(*self._render_args(), bt["frames"], c.chi2_threshold, c.diag_beta,
+                                         c.sort_by_depth, slice_cull_pixels=bt["pixels"], logit_attributes=True)
+                bt["capacity"] = int(prime.total * self.margin) + 1024
+        if self.source is not None:
+            sc, bt = self.source, self._batches[0]
+            best = 0
+            for _ in range(sc["prime_batches"]):
+                torch.randint(0, sc["pool"].numel(), sc["draw"].shape, generator=sc["gen"], device=dev, out=sc["draw"])
+                sc["source"].fill(sc["pool"][sc["draw"]], bt["frames"], bt["pixels"], bt["targets"])
+                prime = UG.bin_gaussians(*self._render_args(), bt["frames"], c.chi2_threshold, c.diag_beta,
+                                         c.sort_by_depth, slice_cull_pixels=bt["pixels"], logit_attributes=True)
+                best = max(best, prime.total)
+            bt["capacity"] = int(best * sc["margin"]) + 1024
 
     def losses(self, batch_index: int = 0) -> torch.Tensor:
         return self._batches[batch_index]["stats"].cpu()
