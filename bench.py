@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--frames-per-step", type=int, default=16)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-train", action="store_true", help="skip the training-step measurement")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -318,28 +319,8 @@ def run_b200(a):
                                "the roofline stage times come from this run's CUDA events"},
     }
 
-    # The whole training step of the reference's loop (activations, L1 loss, backward, Adam
-    # over all parameters) on the same batches, forward + loss + backward replayed from a CUDA
-    # graph per batch, Adam one launch; the parameters are raw (logit) copies of the scene's.
-    from us3d_b200.train import TrainConfig, UltraGaussParameters, UltraGaussTrainer
-
-    tp = UltraGaussParameters(params[0].clone(), params[1].clone(), torch.logit(params[2].clamp(1e-6, 1 - 1e-6)),
-                              torch.logit(params[3].clamp(1e-6, 1 - 1e-6)))
-    trainer = UltraGaussTrainer(tp, [(specs[k * F:(k + 1) * F], pix, tgt) for k, (ft, pix, tgt) in enumerate(batches)],
-                                TrainConfig())
-
-    def train_step(i):
-        trainer.step(i % len(batches))
-
-    # every batch's graph is captured during the warm-up (its first step)
-    ms_train = timed(train_step, a.steps, max(a.warmup, len(batches)))
-    trainer.check()
-    out["train_step"] = {"value": round(a.steps * F * world / (ms_train / 1e3), 3), "unit": UNIT,
-                         "ms_per_step": round(ms_train / a.steps, 4),
-                         "step": "bin (logistic activation fused) + forward + per-frame L1 loss + backward with the "
-                                 "fused loss gradient (CUDA-graph replay) + Adam over all 4 parameter tensors "
-                                 "(one launch)"}
-    del trainer, tp
+    if not a.no_train:
+        out["train_step"] = measure_train_step(a, params, specs, batches, F, world, timed)
 
     if not a.no_plain:
         steps_p = max(2, a.steps // 2)
@@ -359,6 +340,34 @@ def run_b200(a):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def measure_train_step(a, params, specs, batches, F, world, timed):
+    """The whole training step of the reference's loop (activations, L1 loss, backward, Adam
+    over all parameters) on the bench's batches: forward + loss + backward replayed from a CUDA
+    graph per batch, Adam one launch; the parameters are raw (logit) copies of the scene's."""
+    import torch
+
+    from us3d_b200.train import TrainConfig, UltraGaussParameters, UltraGaussTrainer
+
+    tp = UltraGaussParameters(params[0].clone(), params[1].clone(), torch.logit(params[2].clamp(1e-6, 1 - 1e-6)),
+                              torch.logit(params[3].clamp(1e-6, 1 - 1e-6)))
+    trainer = UltraGaussTrainer(tp, [(specs[k * F:(k + 1) * F], pix, tgt) for k, (ft, pix, tgt) in enumerate(batches)],
+                                TrainConfig())
+
+    def train_step(i):
+        trainer.step(i % len(batches))
+
+    # every batch's graph is captured during the warm-up (its first step)
+    ms_train = timed(train_step, a.steps, max(a.warmup, len(batches)))
+    trainer.check()
+    result = {"value": round(a.steps * F * world / (ms_train / 1e3), 3), "unit": UNIT,
+              "ms_per_step": round(ms_train / a.steps, 4),
+              "step": "bin (logistic activation fused) + forward + per-frame L1 loss + backward with the fused loss "
+                      "gradient (CUDA-graph replay) + Adam over all 4 parameter tensors (one launch)"}
+    del trainer, tp
+    torch.cuda.synchronize()
+    return result
 
 
 def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
@@ -391,7 +400,11 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
     copy_stream = torch.cuda.Stream(device=dev)
     d2h_stream = torch.cuda.Stream(device=dev)
     compute = torch.cuda.current_stream()
-    slots = [dict(step=-1, ready=torch.cuda.Event(), free=torch.cuda.Event()) for _ in range(2)]
+    # two slots of device input buffers, refilled in place (no allocation per step)
+    slots = [dict(step=-1, ready=torch.cuda.Event(), free=torch.cuda.Event(),
+                  ps=[torch.empty(x.shape, dtype=x.dtype, device=dev) for x in host],
+                  pix=torch.empty((F * P1, 3), device=dev), tgt=torch.empty((F * P1,), device=dev))
+             for _ in range(2)]
 
     def prefetch(i):
         sl = slots[i % 2]
@@ -399,9 +412,10 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
         s = k * F
         with torch.cuda.stream(copy_stream):
             copy_stream.wait_event(sl["free"])
-            sl["ps"] = [x.to(dev, non_blocking=True) for x in host]
-            sl["pix"] = sweep_pix[s * P1:(s + F) * P1].to(dev, non_blocking=True)
-            sl["tgt"] = tgt_host[s * P1:(s + F) * P1].to(dev, non_blocking=True)
+            for d, x in zip(sl["ps"], host):
+                d.copy_(x, non_blocking=True)
+            sl["pix"].copy_(sweep_pix[s * P1:(s + F) * P1], non_blocking=True)
+            sl["tgt"].copy_(tgt_host[s * P1:(s + F) * P1], non_blocking=True)
             sl["ready"].record(copy_stream)
         sl["step"] = i
 
@@ -410,11 +424,9 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
         if sl["step"] != i:
             prefetch(i)
         compute.wait_event(sl["ready"])
-        ps, pix, tgt = sl["ps"], sl["pix"], sl["tgt"]
-        for t in ps + [pix, tgt]:
-            t.record_stream(compute)
+        pix, tgt = sl["pix"], sl["tgt"]
         prefetch(i + 1)
-        ps = [x.requires_grad_(True) for x in ps]
+        ps = [x.detach().requires_grad_(True) for x in sl["ps"]]
         img, alpha, depth = renderers[i % len(renderers)](*ps, pix)
         loss = (img - tgt).abs().mean()
         loss.backward()
@@ -466,7 +478,10 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
     for r in renderers:
         r.params["capacity"] = cap
         r.params["sync_check"] = False
+    ms0 = torch.cuda.memory_stats(dev)
     ms = timed_e2e(a.steps, a.warmup)
+    ms1 = torch.cuda.memory_stats(dev)
+    alloc = {k: int(ms1.get(k, 0) - ms0.get(k, 0)) for k in ("num_device_alloc", "num_device_free", "num_alloc_retries")}
     for r in renderers:
         if "binning" in r.last:
             total, flags = UG.read_status(r.last["binning"])
@@ -477,7 +492,7 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
     return {"value": round(a.steps * F * world / (ms / 1e3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "api": "us3d_b200.batch.UltraGaussBatchRenderer (autograd)",
             "copies": "next step's inputs prefetched on a second stream (double buffered); results read back on a "
-                      "third stream", "pinned_copy_gbs": link}
+                      "third stream", "pinned_copy_gbs": link, "device_allocations_in_timed_steps": alloc}
 
 
 def cpu_baseline(a, sc, specs, frames: int = 1):

@@ -859,9 +859,9 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
             precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
             const float3 m = make_float3(a.x, a.y, a.z);
             const float dterm = f3_dot(f3_sub(m, geo.o), geo.ele);
-            float r_lat, r_ax, r_ele;
-            window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax, r_ele);
             const float o = a.w, ci = c.z;
+            const float cl11 = b.x * b.x + beta, cl12 = b.y, cl13 = b.z;  // precision factor L
+            const float cl22 = b.w * b.w + beta, cl23 = c.x, cl33 = c.y * c.y + beta;
             float acc_c = 0.f, acc_o = 0.f, acc_e = 0.f;
             float sdx = 0.f, sdy = 0.f, sdz = 0.f;
             float sxx = 0.f, sxy = 0.f, sxz = 0.f, syy = 0.f, syz = 0.f, szz = 0.f;
@@ -873,8 +873,13 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
                 for (int jj = 0; jj < 32; ++jj) {
                     const float4 pa = pa_b[jj];
                     const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
-                    if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
-                    const float q = quad_form(d, q1, s12, s22);
+                    // q = |L^T d|^2. The lateral/axial window of the forward is the bounding
+                    // box of the chi-square ellipsoid, so q <= chi2 implies it up to float
+                    // rounding: the backward tests q only.
+                    const float u0 = cl11 * d.x + cl12 * d.y + cl13 * d.z;
+                    const float u1 = cl22 * d.y + cl23 * d.z;
+                    const float u2 = cl33 * d.z;
+                    const float q = u0 * u0 + u1 * u1 + u2 * u2;
                     if (q > chi2) continue;
                     const float2 pb = pb_b[jj];
                     const float w = __expf(-0.5f * q);
