@@ -395,15 +395,17 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
     g = torch.Generator().manual_seed(99 + rank)
     tgt_host = torch.rand((n_pool * P1,), generator=g).pin_memory()
     renderers = [UltraGaussBatchRenderer(specs[s:s + F], dev) for s in range(0, n_pool, F)]
-    grad_host = [torch.empty_like(x).pin_memory() for x in host]
-    loss_host = torch.empty((), dtype=torch.float32).pin_memory()
     copy_stream = torch.cuda.Stream(device=dev)
     d2h_stream = torch.cuda.Stream(device=dev)
     compute = torch.cuda.current_stream()
-    # two slots of device input buffers, refilled in place (no allocation per step)
-    slots = [dict(step=-1, ready=torch.cuda.Event(), free=torch.cuda.Event(),
+    # two slots of device input buffers (refilled in place) and of pinned result buffers; a
+    # step waits on the host until the results of the step two before it have arrived, as a
+    # loop that reads every loss does, which also bounds how far the host runs ahead
+    slots = [dict(step=-1, ready=torch.cuda.Event(), free=torch.cuda.Event(), landed=torch.cuda.Event(),
                   ps=[torch.empty(x.shape, dtype=x.dtype, device=dev) for x in host],
-                  pix=torch.empty((F * P1, 3), device=dev), tgt=torch.empty((F * P1,), device=dev))
+                  pix=torch.empty((F * P1, 3), device=dev), tgt=torch.empty((F * P1,), device=dev),
+                  grad_host=[torch.empty_like(x).pin_memory() for x in host],
+                  loss_host=torch.empty((), dtype=torch.float32).pin_memory())
              for _ in range(2)]
 
     def prefetch(i):
@@ -421,6 +423,7 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
 
     def step(i):
         sl = slots[i % 2]
+        sl["landed"].synchronize()  # step i-2's loss and gradients are on the host
         if sl["step"] != i:
             prefetch(i)
         compute.wait_event(sl["ready"])
@@ -435,11 +438,12 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
         done.record(compute)
         with torch.cuda.stream(d2h_stream):
             d2h_stream.wait_event(done)
-            loss_host.copy_(outs[0], non_blocking=True)
-            for gh, g in zip(grad_host, outs[1:]):
+            sl["loss_host"].copy_(outs[0], non_blocking=True)
+            for gh, g in zip(sl["grad_host"], outs[1:]):
                 gh.copy_(g, non_blocking=True)
             for t in outs:
                 t.record_stream(d2h_stream)
+            sl["landed"].record(d2h_stream)
         sl["free"].record(compute)
 
     def timed_e2e(steps, warm):
@@ -448,13 +452,17 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
         compute.wait_stream(d2h_stream)
         timed_barrier()
         st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0 = torch.cuda.memory_stats(dev)
         st.record(compute)
         for i in range(steps):
             step(warm + i)
         compute.wait_stream(d2h_stream)  # the last step's results have reached the host
         en.record(compute)
+        m1 = torch.cuda.memory_stats(dev)
         timed_barrier()
-        return max_over_ranks(st.elapsed_time(en), device=dev)
+        allocs = {k: int(m1.get(k, 0) - m0.get(k, 0)) for k in ("num_device_alloc", "num_device_free",
+                                                                  "num_alloc_retries")}
+        return max_over_ranks(st.elapsed_time(en), device=dev), allocs
 
     # pinned-memory copy bandwidth of this machine, one transfer of a step's inputs each way
     probe = torch.empty(sum(x.numel() for x in host) + 2 * F * P1 * 4, dtype=torch.float32).pin_memory()
@@ -478,10 +486,7 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
     for r in renderers:
         r.params["capacity"] = cap
         r.params["sync_check"] = False
-    ms0 = torch.cuda.memory_stats(dev)
-    ms = timed_e2e(a.steps, a.warmup)
-    ms1 = torch.cuda.memory_stats(dev)
-    alloc = {k: int(ms1.get(k, 0) - ms0.get(k, 0)) for k in ("num_device_alloc", "num_device_free", "num_alloc_retries")}
+    ms, alloc = timed_e2e(a.steps, a.warmup)
     for r in renderers:
         if "binning" in r.last:
             total, flags = UG.read_status(r.last["binning"])
@@ -492,7 +497,8 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
     return {"value": round(a.steps * F * world / (ms / 1e3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "api": "us3d_b200.batch.UltraGaussBatchRenderer (autograd)",
             "copies": "next step's inputs prefetched on a second stream (double buffered); results read back on a "
-                      "third stream", "pinned_copy_gbs": link, "device_allocations_in_timed_steps": alloc}
+                      "third stream; the host waits for step i-2's results before launching step i",
+            "pinned_copy_gbs": link, "device_allocations_in_timed_steps": alloc}
 
 
 def cpu_baseline(a, sc, specs, frames: int = 1):

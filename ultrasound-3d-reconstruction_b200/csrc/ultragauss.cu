@@ -25,6 +25,7 @@
 #include <algorithm>
 
 #include <atomic>
+#include <type_traits>
 
 #include "us3d_common.cuh"
 #include "scan.cuh"
@@ -602,15 +603,8 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
 // Shading
 // ------------------------------------------------------------------------------------
 
-// Per-Gaussian data staged in shared memory for one frame.
-struct Staged {
-    float4 q0;  // mean.xyz, opacity
-    float4 q1;  // s00 s01 s02 s11 (precision)
-    float4 q2;  // s12 s22 intensity depth_term
-    float4 q3;  // r_lat r_ax
-};
-
-// Precision Lambda = L L^T from the raw factor (reference include/shader/shared.cuh:4-25).
+// Precision Lambda = L L^T from the raw factor (reference include/shader/shared.cuh:4-25):
+// q1 = (L00, L01, L02, L11), s12 = L12, s22 = L22.
 __device__ __forceinline__ void precision_from_raw(float t0, float t1, float t2, float t3, float t4,
                                                    float t5, float beta, float4& q1, float& s12,
                                                    float& s22) {
@@ -628,22 +622,6 @@ __device__ __forceinline__ void precision_from_raw(float t0, float t1, float t2,
     s22 = l13 * l13 + l23 * l23 + l33 * l33;
 }
 
-__device__ __forceinline__ Staged stage_gaussian(const float4* __restrict__ pack, int g, const Geo& F,
-                                                 float chi2, float beta) {
-    const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
-    Staged s;
-    s.q0 = a;
-    float s12, s22;
-    precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, s.q1, s12, s22);
-    const float3 m = make_float3(a.x, a.y, a.z);
-    const float dterm = f3_dot(f3_sub(m, F.o), F.ele);
-    s.q2 = make_float4(s12, s22, c.z, dterm);
-    float r_lat, r_ax, r_ele;
-    window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, F.lat, F.ax, F.ele, r_lat, r_ax, r_ele);
-    s.q3 = make_float4(r_lat, r_ax, 0.0f, 0.0f);
-    return s;
-}
-
 // Reference window test (src/mapper/core.cu:166-182): |(p-m).lat| <= r_lat && |(p-m).ax| <= r_ax.
 __device__ __forceinline__ bool window_hit(const float3 d, const float3 lat, const float3 ax, float r_lat,
                                            float r_ax) {
@@ -652,11 +630,19 @@ __device__ __forceinline__ bool window_hit(const float3 d, const float3 lat, con
     return dl <= r_lat && da <= r_ax;
 }
 
-// Quadratic form d^T Lambda d in the reference's term order (include/shader/shared.cuh:41-52).
+// Quadratic form d^T Lambda d in the reference's term order (include/shader/shared.cuh:41-52),
+// which its forward and backward both use: every kernel here takes the same q <= chi2 decision
+// for a (pixel, Gaussian) pair as the reference.
 __device__ __forceinline__ float quad_form(const float3 d, const float4 q1, const float s12, const float s22) {
     return (q1.x * d.x + q1.y * d.y + q1.z * d.z) * d.x + (q1.y * d.x + q1.w * d.y + s12 * d.z) * d.y +
            (q1.z * d.x + s12 * d.y + s22 * d.z) * d.z;
 }
+
+// When the diagonal of L is at least 1e-10 (beta >= 1e-10), the lateral/axial window of the
+// reference is the bounding box of the chi-square ellipsoid (the clamps inside window_radii only
+// widen it), so q <= chi2 implies the window test up to float rounding and the test can be left
+// out; below that the clamp can cut the ellipsoid and the window is applied.
+__device__ __forceinline__ bool window_implied(float beta) { return beta >= 1e-10f; }
 
 __device__ __forceinline__ int find_tile_coords(const Geo& geo, int64_t t, int& tx, int& ty) {
     const int lt = (int)(t - geo.tile_off);
@@ -670,7 +656,12 @@ __device__ __forceinline__ int block_col(int k) { return ((k >> 5) & 1) * BLK_W 
 __device__ __forceinline__ int block_row(int k) { return (k >> 6) * BLK_H + ((k & 31) >> 3); }
 
 // One block per tile, one thread per pixel; warp w owns warp block w of the tile and visits
-// only the staged Gaussians whose block mask has bit w (the others reach none of its pixels).
+// only the staged Gaussians whose block mask has bit w (the others reach none of its pixels;
+// without a slice cull every mask is full and all staged Gaussians are visited in list order).
+// A staged Gaussian is four float4: mean + opacity, the precision Lambda, intensity + depth term,
+// and the window radii, which are computed and tested only when the window is not implied by the
+// chi-square test. Both binnings therefore run the same arithmetic per pair (bit-identical
+// results); the reference's candidate counts come from pixel_csr_kernel<true>.
 template <int BATCH>
 __global__ void __launch_bounds__(TILE_PIX, US3D_UG_FWD_MIN_CTAS)
 forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
@@ -678,8 +669,8 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
                const unsigned char* __restrict__ sorted_mask, const long long* __restrict__ header,
                const float4* __restrict__ pack, const float* __restrict__ pixels, float chi2, float beta,
                float bg_alpha, float bg_intensity, float* __restrict__ out_image, float* __restrict__ out_alpha,
-               float* __restrict__ out_depth, int* __restrict__ out_counts, float2* __restrict__ pixel_aux) {
-    __shared__ Staged sg[BATCH];
+               float* __restrict__ out_depth, float2* __restrict__ pixel_aux) {
+    __shared__ float4 s_st[4 * BATCH];
     __shared__ unsigned char s_blocks[BATCH];
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
@@ -695,53 +686,74 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     if (valid) pv = make_float3(pixels[3 * p], pixels[3 * p + 1], pixels[3 * p + 2]);
     const int s0 = tile_start[t];
     const int n = tile_start[t + 1] - s0;
-
-    int cnt = 0;
-    float sa = 0.f, sc = 0.f, sd = 0.f, sc_ns = 0.f, sd_ns = 0.f;
-    auto shade = [&](int j) {
-        const float4 q0 = sg[j].q0;
-        const float4 q3 = sg[j].q3;
-        const float3 d = make_float3(pv.x - q0.x, pv.y - q0.y, pv.z - q0.z);
-        if (!window_hit(d, geo.lat, geo.ax, q3.x, q3.y)) return;
-        ++cnt;
-        const float4 q1 = sg[j].q1;
-        const float4 q2 = sg[j].q2;
-        const float q = quad_form(d, q1, q2.x, q2.y);
-        if (q > chi2) return;
-        const float w = __expf(-0.5f * q);
-        const float ah = q0.w * w;
-        sc_ns += ah * q2.z;
-        sd_ns += ah * q2.w;
-        if (ah <= 1e-8f) return;
-        sa += ah;
-        sc += ah * q2.z;
-        sd += ah * q2.w;
-    };
-    // Without a slice cull every mask is full: plain sweep, same order and sums.
     const bool culled = header[H_MODE] != 0;
-    for (int b0 = 0; b0 < n; b0 += BATCH) {
-        const int nb = min(BATCH, n - b0);
-        __syncthreads();
-        for (int j = threadIdx.x; j < nb; j += blockDim.x) {
-            sg[j] = stage_gaussian(pack, sorted_gid[s0 + b0 + j], geo, chi2, beta);
-            s_blocks[j] = sorted_mask[s0 + b0 + j];
+    const bool windowed = !window_implied(beta);
+
+    // sums over the contributing pairs; kc, kd: the pairs the reference leaves out of the image
+    // (alpha-hat <= 1e-8) but keeps in the backward's numerator / depth sums
+    float sa = 0.f, sc = 0.f, sd = 0.f, kc = 0.f, kd = 0.f;
+    auto shade = [&](int j, auto box_tag) {
+        const float4 f0 = s_st[4 * j], f1 = s_st[4 * j + 1], f2 = s_st[4 * j + 2];
+        const float3 d = make_float3(pv.x - f0.x, pv.y - f0.y, pv.z - f0.z);
+        if constexpr (decltype(box_tag)::value) {
+            const float4 f3 = s_st[4 * j + 3];
+            if (!window_hit(d, geo.lat, geo.ax, f3.x, f3.y)) return;
         }
-        __syncthreads();
-        // Lanes of an invalid pixel run along (their sums are never stored).
-        if (!culled) {
-            for (int j = 0; j < nb; ++j) shade(j);
-            continue;
+        const float q = quad_form(d, f1, f2.x, f2.y);
+        if (q > chi2) return;
+        const float ah = f0.w * __expf(-0.5f * q);
+        if (ah <= 1e-8f) {
+            kc += ah * f2.z;
+            kd += ah * f2.w;
+            return;
         }
-        for (int jc = 0; jc < nb; jc += 32) {
-            const int jl = jc + lane;
-            unsigned bits = __ballot_sync(0xffffffffu, jl < nb && ((s_blocks[jl] >> warp) & 1u));
-            while (bits != 0u) {
-                const int j = jc + __ffs(bits) - 1;
-                bits &= bits - 1u;
-                shade(j);
+        sa += ah;
+        sc += ah * f2.z;
+        sd += ah * f2.w;
+    };
+    auto sweep = [&](auto box_tag) {
+        for (int b0 = 0; b0 < n; b0 += BATCH) {
+            const int nb = min(BATCH, n - b0);
+            __syncthreads();
+            for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+                const int g = sorted_gid[s0 + b0 + j];
+                const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+                const float dterm = f3_dot(f3_sub(make_float3(a.x, a.y, a.z), geo.o), geo.ele);
+                float4 q1;
+                float s12, s22;
+                precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
+                s_st[4 * j] = a;
+                s_st[4 * j + 1] = q1;
+                s_st[4 * j + 2] = make_float4(s12, s22, c.z, dterm);
+                if constexpr (decltype(box_tag)::value) {
+                    float r_lat, r_ax, r_ele;
+                    window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax,
+                                 r_ele);
+                    s_st[4 * j + 3] = make_float4(r_lat, r_ax, 0.f, 0.f);
+                }
+                s_blocks[j] = sorted_mask[s0 + b0 + j];
+            }
+            __syncthreads();
+            // Lanes of an invalid pixel run along (their sums are never stored).
+            if (!culled) {
+                for (int j = 0; j < nb; ++j) shade(j, box_tag);
+                continue;
+            }
+            for (int jc = 0; jc < nb; jc += 32) {
+                const int jl = jc + lane;
+                unsigned bits = __ballot_sync(0xffffffffu, jl < nb && ((s_blocks[jl] >> warp) & 1u));
+                while (bits != 0u) {
+                    const int j = jc + __ffs(bits) - 1;
+                    bits &= bits - 1u;
+                    shade(j, box_tag);
+                }
             }
         }
-    }
+    };
+    if (windowed)
+        sweep(std::true_type{});
+    else
+        sweep(std::false_type{});
     if (!valid) return;
     const float alpha_total = sa + bg_alpha;
     const float num = sc + bg_alpha * bg_intensity;
@@ -749,8 +761,7 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     out_alpha[p] = alpha_total;
     out_image[p] = fmaxf(0.0f, fminf(1.0f, img));
     out_depth[p] = sd / fmaxf(sa, 1e-8f);
-    if (out_counts && header[H_MODE] == 0) out_counts[p] = cnt;
-    pixel_aux[p] = make_float2(sc_ns, sd_ns);
+    pixel_aux[p] = make_float2(sc + kc, sd + kd);
 }
 
 // One block per tile; each thread owns one instance of the tile list at a time and sweeps the
@@ -763,6 +774,8 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
 // LOSS: dL/dimage comes from the fused per-frame loss (L1 + global SSIM of image against
 // target, coefficients per frame in loss_coef; see us3d_ug_loss) and dL/dalpha = dL/ddepth =
 // 0; otherwise from d_image, d_alpha, d_depth.
+// A pair contributes when q = quad_form <= chi2 (and the window is hit, when not implied): the
+// forward's selection, pair for pair.
 template <bool LOSS, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
@@ -825,6 +838,7 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
         }
     }
     const bool culled = header[H_MODE] != 0;  // otherwise every mask is full: no regrouping
+    const bool windowed = !window_implied(beta);
 
     for (int c0 = 0; c0 < n; c0 += BWD_CHUNK) {
         const int nc = min(BWD_CHUNK, n - c0);
@@ -860,47 +874,51 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
             const float3 m = make_float3(a.x, a.y, a.z);
             const float dterm = f3_dot(f3_sub(m, geo.o), geo.ele);
             const float o = a.w, ci = c.z;
-            const float cl11 = b.x * b.x + beta, cl12 = b.y, cl13 = b.z;  // precision factor L
-            const float cl22 = b.w * b.w + beta, cl23 = c.x, cl33 = c.y * c.y + beta;
+            float r_lat = 0.f, r_ax = 0.f, r_ele;
+            if (windowed)
+                window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax, r_ele);
             float acc_c = 0.f, acc_o = 0.f, acc_e = 0.f;
             float sdx = 0.f, sdy = 0.f, sdz = 0.f;
             float sxx = 0.f, sxy = 0.f, sxz = 0.f, syy = 0.f, syz = 0.f, szz = 0.f;
-            for (unsigned mb = blocks; mb != 0u; mb &= mb - 1u) {
-                const int blk = __ffs(mb) - 1;
-                const float4* pa_b = s_pa + blk * 65;
-                const float2* pb_b = s_pb + blk * 65;
+            auto sweep = [&](auto box_tag) {
+                for (unsigned mb = blocks; mb != 0u; mb &= mb - 1u) {
+                    const int blk = __ffs(mb) - 1;
+                    const float4* pa_b = s_pa + blk * 65;
+                    const float2* pb_b = s_pb + blk * 65;
 #pragma unroll
-                for (int jj = 0; jj < 32; ++jj) {
-                    const float4 pa = pa_b[jj];
-                    const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
-                    // q = |L^T d|^2. The lateral/axial window of the forward is the bounding
-                    // box of the chi-square ellipsoid, so q <= chi2 implies it up to float
-                    // rounding: the backward tests q only.
-                    const float u0 = cl11 * d.x + cl12 * d.y + cl13 * d.z;
-                    const float u1 = cl22 * d.y + cl23 * d.z;
-                    const float u2 = cl33 * d.z;
-                    const float q = u0 * u0 + u1 * u1 + u2 * u2;
-                    if (q > chi2) continue;
-                    const float2 pb = pb_b[jj];
-                    const float w = __expf(-0.5f * q);
-                    const float ah = o * w;
-                    const float dah = pa.w * ci + pb.x + pb.y * dterm;
-                    acc_c += pa.w * ah;
-                    acc_o += dah * w;
-                    acc_e += pb.y * ah;
-                    const float dq = -0.5f * dah * ah;
-                    const float ux = dq * d.x, uy = dq * d.y, uz = dq * d.z;
-                    sdx += ux;
-                    sdy += uy;
-                    sdz += uz;
-                    sxx += ux * d.x;
-                    sxy += ux * d.y;
-                    sxz += ux * d.z;
-                    syy += uy * d.y;
-                    syz += uy * d.z;
-                    szz += uz * d.z;
+                    for (int jj = 0; jj < 32; ++jj) {
+                        const float4 pa = pa_b[jj];
+                        const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
+                        if constexpr (decltype(box_tag)::value) {
+                            if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
+                        }
+                        const float q = quad_form(d, q1, s12, s22);
+                        if (q > chi2) continue;
+                        const float2 pb = pb_b[jj];
+                        const float w = __expf(-0.5f * q);
+                        const float ah = o * w;
+                        const float dah = pa.w * ci + pb.x + pb.y * dterm;
+                        acc_c += pa.w * ah;
+                        acc_o += dah * w;
+                        acc_e += pb.y * ah;
+                        const float dq = -0.5f * dah * ah;
+                        const float ux = dq * d.x, uy = dq * d.y, uz = dq * d.z;
+                        sdx += ux;
+                        sdy += uy;
+                        sdz += uz;
+                        sxx += ux * d.x;
+                        sxy += ux * d.y;
+                        sxz += ux * d.z;
+                        syy += uy * d.y;
+                        syz += uy * d.z;
+                        szz += uz * d.z;
+                    }
                 }
-            }
+            };
+            if (windowed)
+                sweep(std::true_type{});
+            else
+                sweep(std::false_type{});
             // d/dmean = -2 Lambda sum(dq d) + sum(ddw * ah) * ele (reference backward.cu:218-228).
             const float vx = q1.x * sdx + q1.y * sdy + q1.z * sdz;
             const float vy = q1.y * sdx + q1.w * sdy + s12 * sdz;
@@ -953,13 +971,16 @@ reduce_kernel(int64_t G, const int* __restrict__ inst_offset, const long long* _
     d_inten[g] = c.z;
 }
 
-// Per-pixel candidate indices in tile-list order (reference src/mapper/core.cu:237-287).
+// Per-pixel candidates of a full (reference) binning in tile-list order: the pixels' window
+// hits (reference src/mapper/core.cu:166-182). COUNT: their number per pixel into out_counts;
+// otherwise their Gaussian indices from offsets[p] on (src/mapper/core.cu:237-287).
+template <bool COUNT>
 __global__ void __launch_bounds__(TILE_PIX)
 pixel_csr_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                  const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
                  const long long* __restrict__ header, const float4* __restrict__ pack,
                  const float* __restrict__ pixels, float chi2, float beta, const int* __restrict__ offsets,
-                 int* __restrict__ out_indices) {
+                 int* __restrict__ out_indices, int* __restrict__ out_counts) {
     __shared__ float4 s_m[FWD_BATCH];   // mean, gaussian index (as float bits)
     __shared__ float2 s_r[FWD_BATCH];   // r_lat, r_ax
     const int64_t t = blockIdx.x;
@@ -976,7 +997,7 @@ pixel_csr_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ fram
     int wp = 0;
     if (valid) {
         pv = make_float3(pixels[3 * p], pixels[3 * p + 1], pixels[3 * p + 2]);
-        wp = offsets[p];
+        if (!COUNT) wp = offsets[p];
     }
     const int s0 = tile_start[t];
     const int n = tile_start[t + 1] - s0;
@@ -997,10 +1018,14 @@ pixel_csr_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ fram
                 const float4 m = s_m[j];
                 const float2 r = s_r[j];
                 const float3 d = make_float3(pv.x - m.x, pv.y - m.y, pv.z - m.z);
-                if (window_hit(d, geo.lat, geo.ax, r.x, r.y)) out_indices[wp++] = __float_as_int(m.w);
+                if (window_hit(d, geo.lat, geo.ax, r.x, r.y)) {
+                    if (!COUNT) out_indices[wp] = __float_as_int(m.w);
+                    ++wp;
+                }
             }
         }
     }
+    if (COUNT && valid) out_counts[p] = wp;
 }
 
 __global__ void export_kernel(int tile_off, int n_tiles_frame, const int* __restrict__ tile_start,
@@ -1187,7 +1212,7 @@ extern "C" int us3d_ug_forward(void* workspace, const us3d_slice_frame* frames, 
     auto launch = [&](auto kernel) {
         kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(
             n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_mask, w.header, w.pack,
-            pixels, chi2, beta, bg_alpha, bg_intensity, out_image, out_alpha, out_depth, out_counts, w.pixel_aux);
+            pixels, chi2, beta, bg_alpha, bg_intensity, out_image, out_alpha, out_depth, w.pixel_aux);
     };
     switch (g_fwd_batch.load()) {
         case 128: launch(forward_kernel<128>); break;
@@ -1195,8 +1220,14 @@ extern "C" int us3d_ug_forward(void* workspace, const us3d_slice_frame* frames, 
         default: launch(forward_kernel<512>); break;
     }
     US3D_CHECK_LAUNCH("ug forward");
+    if (out_counts) {  // the reference's per-pixel candidate counts (full binning only)
+        pixel_csr_kernel<true><<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(
+            n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.header, w.pack, pixels, chi2, beta,
+            nullptr, nullptr, out_counts);
+        US3D_CHECK_LAUNCH("ug counts");
+    }
     prof_end(prof, stream);
-    count_launches(1);
+    count_launches(1 + (out_counts != nullptr));
     return US3D_OK;
 }
 
@@ -1285,9 +1316,10 @@ extern "C" int us3d_ug_pixel_csr(void* workspace, const us3d_slice_frame* frames
     const Workspace w = carve(workspace, n_gauss, n_tiles, n_pixels, cap);
     if (n_tiles == 0) return US3D_OK;
     cudaStream_t stream = (cudaStream_t)stream_;
-    pixel_csr_kernel<<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(n_tiles, n_pixels, frames, w.tile_frame,
-                                                                  w.tile_start, w.sorted_gid, w.header, w.pack,
-                                                                  pixels, chi2, beta, offsets, out_indices);
+    pixel_csr_kernel<false><<<(unsigned)n_tiles, TILE_PIX, 0, stream>>>(n_tiles, n_pixels, frames, w.tile_frame,
+                                                                         w.tile_start, w.sorted_gid, w.header, w.pack,
+                                                                         pixels, chi2, beta, offsets, out_indices,
+                                                                         nullptr);
     US3D_CHECK_LAUNCH("ug pixel csr");
     count_launches(1);
     return US3D_OK;
