@@ -84,7 +84,8 @@ def _reference_run(REF, REFK, fx, device):
                 ref_d_intensity=c(da)[:, 1])
 
 
-def _scene_case(G, H, W, spacing, seed, frame=0, n_frames=4, sort=True, bg_a=1e-6, bg_i=0.0, chi2=7.815, **kw):
+def _scene_case(G, H, W, spacing, seed, frame=0, n_frames=4, sort=True, bg_a=1e-6, bg_i=0.0, chi2=7.815, beta=1e-4,
+                **kw):
     from us3d_b200 import scenes
 
     sc = scenes.make_scene(G, seed=seed, **kw)
@@ -95,7 +96,7 @@ def _scene_case(G, H, W, spacing, seed, frame=0, n_frames=4, sort=True, bg_a=1e-
                           np.array([spacing, spacing, 0.0, fr.lateral_col_offset], np.float32)]).astype(np.float32)
     return dict(means=sc.means.numpy(), precision_tril=sc.precision_tril.numpy(), opacities=sc.opacities.numpy(),
                 intensities=sc.intensities.numpy(), pixels=fr.pixels.numpy(), geo=geo, H=H, W=W,
-                chi2=np.float32(chi2), beta=np.float32(1e-4), sort_by_depth=int(sort), bg_alpha=np.float32(bg_a),
+                chi2=np.float32(chi2), beta=np.float32(beta), sort_by_depth=int(sort), bg_alpha=np.float32(bg_a),
                 bg_intensity=np.float32(bg_i), d_image=torch.randn(P, generator=g).numpy(),
                 d_alpha=(0.3 * torch.randn(P, generator=g)).numpy(), d_depth=(0.05 * torch.randn(P, generator=g)).numpy())
 
@@ -122,6 +123,18 @@ def test_live_reference_parity_dense_tiles(cuda_device):
     fx.update(_reference_run(REF, REFK, fx, cuda_device))
     n = fx["ref_range_end"] - fx["ref_range_start"]
     assert n.max() > 16384 and ((n > 4096) & (n <= 16384)).any() and ((n > 64) & (n <= 2048)).any()
+    out = run_b200(fx, cuda_device)
+    _assert_case(out, fx)
+
+
+@pytest.mark.parametrize("beta", [1e-12, 5e-11])
+def test_live_reference_parity_windowed(beta, cuda_device):
+    """A diagonal offset in (0, 1e-10) (the reference's clamp inside the window radii can then
+    cut the chi-square ellipsoid): the kernels that apply the lateral/axial window per pair, against
+    the reference's own binning, candidate lists, forward and backward."""
+    REF, REFK = _reference_modules()
+    fx = _scene_case(20000, 160, 128, 0.25, 11, frame=2, beta=beta)
+    fx.update(_reference_run(REF, REFK, fx, cuda_device))
     out = run_b200(fx, cuda_device)
     _assert_case(out, fx)
 
@@ -339,16 +352,18 @@ def test_culled_batched_deterministic(cuda_device):
             assert np.array_equal(x, y)
 
 
-@pytest.mark.parametrize("jitter,scale", [(0.0, 1.0), (0.0, 0.3), (2e-3, 1.0), (0.5, 1.0)])
-def test_slice_cull_identical_results(jitter, scale, cuda_device):
+@pytest.mark.parametrize("jitter,scale,beta", [(0.0, 1.0, 1e-4), (0.0, 0.3, 1e-4), (2e-3, 1.0, 1e-4), (0.5, 1.0, 1e-4),
+                                               (0.0, 1.0, 1e-12)])
+def test_slice_cull_identical_results(jitter, scale, beta, cuda_device):
     """A slice-culled binning keeps fewer instances but gives bit-identical images, alpha,
-    depth and gradients (pixels on the frame grid, slightly off it, and far off it)."""
+    depth and gradients (pixels on the frame grid, slightly off it, and far off it; beta below
+    1e-10 runs the kernels that apply the window per pair)."""
     from us3d_b200 import ultragauss as UG
 
     args, ft, pix, gg = _cull_case(cuda_device, jitter=jitter, scale_mm=scale)
     out = {}
     for cull in (False, True):
-        b = UG.bin_gaussians(*args, ft, 7.815, 1e-4, True, slice_cull_pixels=pix if cull else None)
+        b = UG.bin_gaussians(*args, ft, 7.815, beta, True, slice_cull_pixels=pix if cull else None)
         img, alp, dep, cnt = UG.forward(b, pix, 1e-6, 0.0)
         assert (cnt is None) == cull
         d = UG.backward(b, pix, gg[0].contiguous(), gg[1].contiguous(), gg[2].contiguous(), alp, 1e-6, 0.0)

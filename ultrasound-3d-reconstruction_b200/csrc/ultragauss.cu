@@ -25,7 +25,6 @@
 #include <algorithm>
 
 #include <atomic>
-#include <type_traits>
 
 #include "us3d_common.cuh"
 #include "scan.cuh"
@@ -642,7 +641,7 @@ __device__ __forceinline__ float quad_form(const float3 d, const float4 q1, cons
 // reference is the bounding box of the chi-square ellipsoid (the clamps inside window_radii only
 // widen it), so q <= chi2 implies the window test up to float rounding and the test can be left
 // out; below that the clamp can cut the ellipsoid and the window is applied.
-__device__ __forceinline__ bool window_implied(float beta) { return beta >= 1e-10f; }
+__host__ __device__ __forceinline__ bool window_implied(float beta) { return beta >= 1e-10f; }
 
 __device__ __forceinline__ int find_tile_coords(const Geo& geo, int64_t t, int& tx, int& ty) {
     const int lt = (int)(t - geo.tile_off);
@@ -658,11 +657,12 @@ __device__ __forceinline__ int block_row(int k) { return (k >> 6) * BLK_H + ((k 
 // One block per tile, one thread per pixel; warp w owns warp block w of the tile and visits
 // only the staged Gaussians whose block mask has bit w (the others reach none of its pixels;
 // without a slice cull every mask is full and all staged Gaussians are visited in list order).
-// A staged Gaussian is four float4: mean + opacity, the precision Lambda, intensity + depth term,
-// and the window radii, which are computed and tested only when the window is not implied by the
-// chi-square test. Both binnings therefore run the same arithmetic per pair (bit-identical
-// results); the reference's candidate counts come from pixel_csr_kernel<true>.
-template <int BATCH>
+// A staged Gaussian is three float4: mean + opacity, the precision Lambda, intensity + depth term;
+// a fourth holds the window radii, which are computed and tested only when the window is not implied by the
+// chi-square test (WINDOWED, chosen by the host from beta). Both binnings therefore run the same
+// arithmetic per pair (bit-identical results); the reference's candidate counts come from
+// pixel_csr_kernel<true>.
+template <int BATCH, bool WINDOWED>
 __global__ void __launch_bounds__(TILE_PIX, US3D_UG_FWD_MIN_CTAS)
 forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
@@ -670,7 +670,8 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
                const float4* __restrict__ pack, const float* __restrict__ pixels, float chi2, float beta,
                float bg_alpha, float bg_intensity, float* __restrict__ out_image, float* __restrict__ out_alpha,
                float* __restrict__ out_depth, float2* __restrict__ pixel_aux) {
-    __shared__ float4 s_st[4 * BATCH];
+    constexpr int STRIDE = WINDOWED ? 4 : 3;
+    __shared__ float4 s_st[STRIDE * BATCH];
     __shared__ unsigned char s_blocks[BATCH];
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
@@ -687,16 +688,15 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     const int s0 = tile_start[t];
     const int n = tile_start[t + 1] - s0;
     const bool culled = header[H_MODE] != 0;
-    const bool windowed = !window_implied(beta);
 
     // sums over the contributing pairs; kc, kd: the pairs the reference leaves out of the image
     // (alpha-hat <= 1e-8) but keeps in the backward's numerator / depth sums
     float sa = 0.f, sc = 0.f, sd = 0.f, kc = 0.f, kd = 0.f;
-    auto shade = [&](int j, auto box_tag) {
-        const float4 f0 = s_st[4 * j], f1 = s_st[4 * j + 1], f2 = s_st[4 * j + 2];
+    auto shade = [&](int j) {
+        const float4 f0 = s_st[STRIDE * j], f1 = s_st[STRIDE * j + 1], f2 = s_st[STRIDE * j + 2];
         const float3 d = make_float3(pv.x - f0.x, pv.y - f0.y, pv.z - f0.z);
-        if constexpr (decltype(box_tag)::value) {
-            const float4 f3 = s_st[4 * j + 3];
+        if constexpr (WINDOWED) {
+            const float4 f3 = s_st[STRIDE * j + 3];
             if (!window_hit(d, geo.lat, geo.ax, f3.x, f3.y)) return;
         }
         const float q = quad_form(d, f1, f2.x, f2.y);
@@ -711,49 +711,43 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
         sc += ah * f2.z;
         sd += ah * f2.w;
     };
-    auto sweep = [&](auto box_tag) {
-        for (int b0 = 0; b0 < n; b0 += BATCH) {
-            const int nb = min(BATCH, n - b0);
-            __syncthreads();
-            for (int j = threadIdx.x; j < nb; j += blockDim.x) {
-                const int g = sorted_gid[s0 + b0 + j];
-                const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
-                const float dterm = f3_dot(f3_sub(make_float3(a.x, a.y, a.z), geo.o), geo.ele);
-                float4 q1;
-                float s12, s22;
-                precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
-                s_st[4 * j] = a;
-                s_st[4 * j + 1] = q1;
-                s_st[4 * j + 2] = make_float4(s12, s22, c.z, dterm);
-                if constexpr (decltype(box_tag)::value) {
-                    float r_lat, r_ax, r_ele;
-                    window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax,
-                                 r_ele);
-                    s_st[4 * j + 3] = make_float4(r_lat, r_ax, 0.f, 0.f);
-                }
-                s_blocks[j] = sorted_mask[s0 + b0 + j];
+    for (int b0 = 0; b0 < n; b0 += BATCH) {
+        const int nb = min(BATCH, n - b0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+            const int g = sorted_gid[s0 + b0 + j];
+            const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+            const float dterm = f3_dot(f3_sub(make_float3(a.x, a.y, a.z), geo.o), geo.ele);
+            float4 q1;
+            float s12, s22;
+            precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
+            s_st[STRIDE * j] = a;
+            s_st[STRIDE * j + 1] = q1;
+            s_st[STRIDE * j + 2] = make_float4(s12, s22, c.z, dterm);
+            if constexpr (WINDOWED) {
+                float r_lat, r_ax, r_ele;
+                window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax,
+                             r_ele);
+                s_st[STRIDE * j + 3] = make_float4(r_lat, r_ax, 0.f, 0.f);
             }
-            __syncthreads();
-            // Lanes of an invalid pixel run along (their sums are never stored).
-            if (!culled) {
-                for (int j = 0; j < nb; ++j) shade(j, box_tag);
-                continue;
-            }
-            for (int jc = 0; jc < nb; jc += 32) {
-                const int jl = jc + lane;
-                unsigned bits = __ballot_sync(0xffffffffu, jl < nb && ((s_blocks[jl] >> warp) & 1u));
-                while (bits != 0u) {
-                    const int j = jc + __ffs(bits) - 1;
-                    bits &= bits - 1u;
-                    shade(j, box_tag);
-                }
+            s_blocks[j] = sorted_mask[s0 + b0 + j];
+        }
+        __syncthreads();
+        // Lanes of an invalid pixel run along (their sums are never stored).
+        if (!culled) {
+            for (int j = 0; j < nb; ++j) shade(j);
+            continue;
+        }
+        for (int jc = 0; jc < nb; jc += 32) {
+            const int jl = jc + lane;
+            unsigned bits = __ballot_sync(0xffffffffu, jl < nb && ((s_blocks[jl] >> warp) & 1u));
+            while (bits != 0u) {
+                const int j = jc + __ffs(bits) - 1;
+                bits &= bits - 1u;
+                shade(j);
             }
         }
-    };
-    if (windowed)
-        sweep(std::true_type{});
-    else
-        sweep(std::false_type{});
+    }
     if (!valid) return;
     const float alpha_total = sa + bg_alpha;
     const float num = sc + bg_alpha * bg_intensity;
@@ -774,9 +768,9 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
 // LOSS: dL/dimage comes from the fused per-frame loss (L1 + global SSIM of image against
 // target, coefficients per frame in loss_coef; see us3d_ug_loss) and dL/dalpha = dL/ddepth =
 // 0; otherwise from d_image, d_alpha, d_depth.
-// A pair contributes when q = quad_form <= chi2 (and the window is hit, when not implied): the
-// forward's selection, pair for pair.
-template <bool LOSS, int THREADS>
+// A pair contributes when q = quad_form <= chi2 (and, WINDOWED, the window is hit): the forward's
+// selection, pair for pair.
+template <bool LOSS, int THREADS, bool WINDOWED>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                 const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
@@ -838,7 +832,6 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
         }
     }
     const bool culled = header[H_MODE] != 0;  // otherwise every mask is full: no regrouping
-    const bool windowed = !window_implied(beta);
 
     for (int c0 = 0; c0 < n; c0 += BWD_CHUNK) {
         const int nc = min(BWD_CHUNK, n - c0);
@@ -875,50 +868,44 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
             const float dterm = f3_dot(f3_sub(m, geo.o), geo.ele);
             const float o = a.w, ci = c.z;
             float r_lat = 0.f, r_ax = 0.f, r_ele;
-            if (windowed)
+            if (WINDOWED)
                 window_radii(b.x, b.y, b.z, b.w, c.x, c.y, chi2, beta, geo.lat, geo.ax, geo.ele, r_lat, r_ax, r_ele);
             float acc_c = 0.f, acc_o = 0.f, acc_e = 0.f;
             float sdx = 0.f, sdy = 0.f, sdz = 0.f;
             float sxx = 0.f, sxy = 0.f, sxz = 0.f, syy = 0.f, syz = 0.f, szz = 0.f;
-            auto sweep = [&](auto box_tag) {
-                for (unsigned mb = blocks; mb != 0u; mb &= mb - 1u) {
-                    const int blk = __ffs(mb) - 1;
-                    const float4* pa_b = s_pa + blk * 65;
-                    const float2* pb_b = s_pb + blk * 65;
+            for (unsigned mb = blocks; mb != 0u; mb &= mb - 1u) {
+                const int blk = __ffs(mb) - 1;
+                const float4* pa_b = s_pa + blk * 65;
+                const float2* pb_b = s_pb + blk * 65;
 #pragma unroll
-                    for (int jj = 0; jj < 32; ++jj) {
-                        const float4 pa = pa_b[jj];
-                        const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
-                        if constexpr (decltype(box_tag)::value) {
-                            if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
-                        }
-                        const float q = quad_form(d, q1, s12, s22);
-                        if (q > chi2) continue;
-                        const float2 pb = pb_b[jj];
-                        const float w = __expf(-0.5f * q);
-                        const float ah = o * w;
-                        const float dah = pa.w * ci + pb.x + pb.y * dterm;
-                        acc_c += pa.w * ah;
-                        acc_o += dah * w;
-                        acc_e += pb.y * ah;
-                        const float dq = -0.5f * dah * ah;
-                        const float ux = dq * d.x, uy = dq * d.y, uz = dq * d.z;
-                        sdx += ux;
-                        sdy += uy;
-                        sdz += uz;
-                        sxx += ux * d.x;
-                        sxy += ux * d.y;
-                        sxz += ux * d.z;
-                        syy += uy * d.y;
-                        syz += uy * d.z;
-                        szz += uz * d.z;
+                for (int jj = 0; jj < 32; ++jj) {
+                    const float4 pa = pa_b[jj];
+                    const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
+                    if constexpr (WINDOWED) {
+                        if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
                     }
+                    const float q = quad_form(d, q1, s12, s22);
+                    if (q > chi2) continue;
+                    const float2 pb = pb_b[jj];
+                    const float w = __expf(-0.5f * q);
+                    const float ah = o * w;
+                    const float dah = pa.w * ci + pb.x + pb.y * dterm;
+                    acc_c += pa.w * ah;
+                    acc_o += dah * w;
+                    acc_e += pb.y * ah;
+                    const float dq = -0.5f * dah * ah;
+                    const float ux = dq * d.x, uy = dq * d.y, uz = dq * d.z;
+                    sdx += ux;
+                    sdy += uy;
+                    sdz += uz;
+                    sxx += ux * d.x;
+                    sxy += ux * d.y;
+                    sxz += ux * d.z;
+                    syy += uy * d.y;
+                    syz += uy * d.z;
+                    szz += uz * d.z;
                 }
-            };
-            if (windowed)
-                sweep(std::true_type{});
-            else
-                sweep(std::false_type{});
+            }
             // d/dmean = -2 Lambda sum(dq d) + sum(ddw * ah) * ele (reference backward.cu:218-228).
             const float vx = q1.x * sdx + q1.y * sdy + q1.z * sdz;
             const float vy = q1.y * sdx + q1.w * sdy + s12 * sdz;
@@ -1214,10 +1201,14 @@ extern "C" int us3d_ug_forward(void* workspace, const us3d_slice_frame* frames, 
             n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_mask, w.header, w.pack,
             pixels, chi2, beta, bg_alpha, bg_intensity, out_image, out_alpha, out_depth, w.pixel_aux);
     };
-    switch (g_fwd_batch.load()) {
-        case 128: launch(forward_kernel<128>); break;
-        case 256: launch(forward_kernel<256>); break;
-        default: launch(forward_kernel<512>); break;
+    if (!window_implied(beta)) {
+        launch(forward_kernel<256, true>);
+    } else {
+        switch (g_fwd_batch.load()) {
+            case 128: launch(forward_kernel<128, false>); break;
+            case 256: launch(forward_kernel<256, false>); break;
+            default: launch(forward_kernel<512, false>); break;
+        }
     }
     US3D_CHECK_LAUNCH("ug forward");
     if (out_counts) {  // the reference's per-pixel candidate counts (full binning only)
@@ -1263,10 +1254,14 @@ static int ug_backward_impl(void* workspace, const us3d_slice_frame* frames, int
                 w.header, w.pack, pixels, d_image, d_alpha, d_depth, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha,
                 bg_intensity, loss_image, loss_target, loss_coef, partial);
         };
-        if (fused)
-            threads == 128 ? launch(backward_kernel<true, 128>, 128) : launch(backward_kernel<true, 256>, 256);
+        if (!window_implied(beta))
+            fused ? launch(backward_kernel<true, 256, true>, 256) : launch(backward_kernel<false, 256, true>, 256);
+        else if (fused)
+            threads == 128 ? launch(backward_kernel<true, 128, false>, 128)
+                           : launch(backward_kernel<true, 256, false>, 256);
         else
-            threads == 128 ? launch(backward_kernel<false, 128>, 128) : launch(backward_kernel<false, 256>, 256);
+            threads == 128 ? launch(backward_kernel<false, 128, false>, 128)
+                           : launch(backward_kernel<false, 256, false>, 256);
         US3D_CHECK_LAUNCH("ug backward");
     }
     if (n_gauss > 0) {
