@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-train", action="store_true", help="skip the training-step measurement")
+    ap.add_argument("--launch-shape", default=None,
+                    help="forward batch / backward threads, e.g. 512/256, instead of autotuning")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -226,10 +228,15 @@ def run_b200(a):
         return max_over_ranks(st.elapsed_time(en), device=dev)
 
     # -- launch-shape autotuning on the first batch (untimed; changes no result) --
-    from us3d_b200.batch import autotune_launch
+    from us3d_b200.batch import autotune_launch, set_launch_config
 
-    tuned = autotune_launch(batches[0][0], params, batches[0][1])
-    launch_shape = min(tuned, key=tuned.get)
+    if a.launch_shape:
+        launch_shape = tuple(int(x) for x in a.launch_shape.split("/"))
+        set_launch_config(*launch_shape)
+        tuned = {}
+    else:
+        tuned = autotune_launch(batches[0][0], params, batches[0][1])
+        launch_shape = min(tuned, key=tuned.get)
 
     # -- warm-up + stage selection for the roofline (untimed) --
     stage_ms = {}

@@ -349,6 +349,9 @@ __device__ __forceinline__ void slice_setup(const float4 a, const float4 b, cons
 // over the reference rectangle `r` (tiles). Returns false when no pixel can pass.
 struct SliceEllipse {
     double xc, yc, h00, h01, h11, det, rho;
+    // row-range constants: half-height, x-shear h01/h00, det/h00, 1/h00, y offset of the
+    // rightmost point
+    double ymax, s1, kk, inv_h00, dys;
     int ok;  // 0: degenerate quadratic, keep every tile of the rectangle
 };
 
@@ -371,21 +374,29 @@ __device__ __forceinline__ bool slice_ellipse(const SliceQuad& S, const int4 r, 
     const double dm = sqrt(dmax2) + dv;
     const double tau = 2.0 * sqrt(((double)chi2 + 1.0) * S.lam) * dv + S.lam * dv * dv + 1.2e-5 * S.lam * dm * dm + 1e-6;
     E.rho = (double)chi2 + tau - qc;
-    return E.rho >= 0.0;
+    if (E.rho < 0.0) return false;
+    E.inv_h00 = 1.0 / E.h00;
+    E.s1 = E.h01 * E.inv_h00;
+    E.kk = E.det * E.inv_h00;
+    E.ymax = sqrt(E.rho * E.h00 / E.det);
+    E.dys = -E.h01 * sqrt(E.rho / (E.h11 * E.det));
+    return true;
 }
 
 // Pixel-centre x-range [xl, xr] of the ellipse inside the tile row y in [y0, y1] (exact:
 // the ellipse's x-extent over a horizontal band); false if the band misses the ellipse.
 __device__ __forceinline__ bool ellipse_row_range(const SliceEllipse& E, double y0, double y1, double& xl,
                                                   double& xr) {
-    const double ymax = sqrt(E.rho * E.h00 / E.det);
-    const double a = fmax(y0 - E.yc, -ymax), b = fmin(y1 - E.yc, ymax);
+    const double a = fmax(y0 - E.yc, -E.ymax), b = fmin(y1 - E.yc, E.ymax);
     if (a > b) return false;
-    const double s1 = E.h01 / E.h00, kk = E.det / E.h00;
-    const double dys = -E.h01 * sqrt(E.rho / (E.h11 * E.det));  // dy of the rightmost point
-    const double dr = fmin(fmax(dys, a), b), dl = fmin(fmax(-dys, a), b);
-    xr = E.xc - s1 * dr + sqrt(fmax(0.0, (E.rho - kk * dr * dr) / E.h00));
-    xl = E.xc - s1 * dl - sqrt(fmax(0.0, (E.rho - kk * dl * dl) / E.h00));
+    const double dr = fmin(fmax(E.dys, a), b), dl = fmin(fmax(-E.dys, a), b);
+    // The half-widths are rounded to float before their square root: a relative error of a
+    // few 1e-7 of the half-width, well inside the slack below (at least 2e-6 of it, since
+    // |xl| + |xr| >= xr - xl).
+    const float hr = sqrtf((float)fmax(0.0, (E.rho - E.kk * dr * dr) * E.inv_h00));
+    const float hl = sqrtf((float)fmax(0.0, (E.rho - E.kk * dl * dl) * E.inv_h00));
+    xr = E.xc - E.s1 * dr + (double)hr;
+    xl = E.xc - E.s1 * dl - (double)hl;
     const double slack = 1e-6 * (fabs(xl) + fabs(xr) + 1.0);
     xl -= slack;
     xr += slack;
@@ -471,14 +482,15 @@ __global__ void task_check_kernel(long long* __restrict__ header, int64_t tc) {
     }
 }
 
-// Tiles of task k in the order both passes enumerate them; calls fn(tile_index, i, blocks)
-// for each, i counting the task's tiles. With WANT_BLOCKS, `blocks` marks the tile's warp
-// blocks that the in-slice ellipse reaches: each 4-row band's exact pixel-centre x-range,
-// tested against the block's columns (the same conservative bound as the tile cull, so a
-// pixel that passes the chi-square test always lies in a marked block); 0xff without a cull.
-template <bool WANT_BLOCKS, typename Fn>
+// Tiles of task k in the order both passes enumerate them, one tile row at a time:
+// row(row_base, xa, xb, blocks) for the row's tiles x in [xa, xb) (tile index row_base + x),
+// blocks(x) giving the warp blocks of tile x that the in-slice ellipse reaches (each 4-row
+// band's exact pixel-centre x-range tested against the block's columns: the same conservative
+// bound as the tile cull, so a pixel that passes the chi-square test always lies in a marked
+// block); 0xff without WANT_BLOCKS or a cull. Returns the number of tiles.
+template <bool WANT_BLOCKS, typename Row>
 __device__ __forceinline__ int task_tiles(const int4 r, const Geo& geo, const float4 a, const float4 b,
-                                          const float4 c, float chi2, float beta, const unsigned* frame_dev, Fn fn) {
+                                          const float4 c, float chi2, float beta, const unsigned* frame_dev, Row row) {
     SliceEllipse E;
     E.ok = 0;
     if (frame_dev) {
@@ -511,9 +523,11 @@ __device__ __forceinline__ int task_tiles(const int4 r, const Geo& geo, const fl
                 }
             }
         }
-        for (int x = xa; x < xb; ++x) {
+        if (xa >= xb) continue;
+        const bool ell = E.ok != 0;
+        row(geo.tile_off + y * geo.tx, xa, xb, n, [&](int x) -> unsigned {
             unsigned blocks = 0xffu;
-            if (WANT_BLOCKS && E.ok) {
+            if (WANT_BLOCKS && ell) {
                 blocks = 0u;
 #pragma unroll
                 for (int sb = 0; sb < TILE / BLK_H; ++sb)
@@ -523,9 +537,9 @@ __device__ __forceinline__ int task_tiles(const int4 r, const Geo& geo, const fl
                         if (bl[sb] <= c1 && br[sb] >= c0) blocks |= 1u << (sb * (TILE / BLK_W) + bx);
                     }
             }
-            fn(geo.tile_off + y * geo.tx + x, n, blocks);
-            ++n;
-        }
+            return blocks;
+        });
+        n += xb - xa;
     }
     return n;
 }
@@ -542,7 +556,9 @@ task_count_kernel(const long long* __restrict__ header, const us3d_slice_frame* 
         const float4 a = pack[3 * (int64_t)gf.x], b = pack[3 * (int64_t)gf.x + 1], c = pack[3 * (int64_t)gf.x + 2];
         const Geo geo = load_geo(frames + gf.y);
         task_ntiles[k] = task_tiles<false>(task_rect[k], geo, a, b, c, chi2, beta, frame_dev,
-                                           [&](int t, int, unsigned) { atomicAdd(&tile_count[t], 1); });
+                                           [&](int base, int xa, int xb, int, auto) {
+                                               for (int x = xa; x < xb; ++x) atomicAdd(&tile_count[base + x], 1);
+                                           });
     }
 }
 
@@ -570,13 +586,27 @@ task_scatter_kernel(const long long* __restrict__ header, const us3d_slice_frame
         const unsigned long long key =
             ((unsigned long long)depth_key(task_v[k], sort_by_depth) << 32) | (unsigned long long)(uint32_t)gf.x;
         const int i0 = task_inst[k];
-        task_tiles<true>(task_rect[k], geo, a, b, c, chi2, beta, frame_dev, [&](int t, int i, unsigned blocks) {
-            const int slot = tile_start[t] + atomicAdd(&tile_cursor[t], 1);
-            if (slot >= tile_start[t + 1]) return;  // never outside the bucket (verify_kernel flags it)
-            keys[slot] = key;
-            slot_inst[slot] = i0 + i;
-            slot_mask[slot] = (unsigned char)blocks;
-        });
+        // Slots are reserved four tiles at a time, so that the atomics' round trips overlap.
+        task_tiles<true>(task_rect[k], geo, a, b, c, chi2, beta, frame_dev,
+                         [&](int base, int xa, int xb, int i, auto blocks_of) {
+                             for (int x0 = xa; x0 < xb; x0 += 4) {
+                                 int within[4];
+#pragma unroll
+                                 for (int u = 0; u < 4; ++u)
+                                     if (x0 + u < xb) within[u] = atomicAdd(&tile_cursor[base + x0 + u], 1);
+#pragma unroll
+                                 for (int u = 0; u < 4; ++u) {
+                                     if (x0 + u >= xb) break;
+                                     const int t = base + x0 + u;
+                                     const int slot = tile_start[t] + within[u];
+                                     // never outside the bucket (verify_kernel flags it)
+                                     if (slot >= tile_start[t + 1]) continue;
+                                     keys[slot] = key;
+                                     slot_inst[slot] = i0 + i + (x0 - xa) + u;
+                                     slot_mask[slot] = (unsigned char)blocks_of(x0 + u);
+                                 }
+                             }
+                         });
     }
 }
 
