@@ -256,10 +256,13 @@ static __device__ __forceinline__ void seg_store(unsigned long long* sk, int* sv
 // (16-byte aligned key array, 8-byte aligned payload array), the same mirror network as
 // bitonic_sort: passes that stay inside 64-element segments run in registers with warp
 // shuffles, the others as shared-memory compare-exchanges between block barriers. The
-// caller pads the keys past the bucket with SORT_PAD_KEY and synchronises first.
-static __device__ void block_sort_smem(unsigned long long* sk, int* sv, int npow) {
+// caller pads the keys past the first n with SORT_PAD_KEY and synchronises first. Every
+// compare-exchange puts the smaller key at the lower index, so the padding never moves and an
+// exchange whose upper index is >= n does nothing: those exchanges, and the 64-element
+// segments lying wholly in the padding, are skipped.
+static __device__ void block_sort_smem(unsigned long long* sk, int* sv, int npow, int n) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int nseg = npow >> 6, half_n = npow >> 1;
+    const int nseg = (n + 63) >> 6, half_n = npow >> 1;
     for (int s = warp; s < nseg; s += nwarp) {
         SortKV x0, x1;
         seg_load(sk, sv, s, lane, x0, x1);
@@ -276,14 +279,15 @@ static __device__ void block_sort_smem(unsigned long long* sk, int* sv, int npow
         const int size = 1 << ls, lh = ls - 1, hs = size >> 1;
         for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
             const int base = (i >> lh) << ls, off = i & (hs - 1);
-            cswap(sk, sv, base + off, base + size - 1 - off);
+            const int b = base + size - 1 - off;
+            if (b < n) cswap(sk, sv, base + off, b);
         }
         __syncthreads();
         for (int l2 = lh - 1; l2 >= 6; --l2) {
             const int h = 1 << l2;
             for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
                 const int a = ((i >> l2) << (l2 + 1)) + (i & (h - 1));
-                cswap(sk, sv, a, a + h);
+                if (a + h < n) cswap(sk, sv, a, a + h);
             }
             __syncthreads();
         }
@@ -313,7 +317,7 @@ static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_ke
         s_idx[i] = i;
     }
     __syncthreads();
-    block_sort_smem(s_keys, s_idx, npow);
+    block_sort_smem(s_keys, s_idx, npow, n);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const unsigned long long k = s_keys[i];
         sorted_gid[s0 + i] = (int)(uint32_t)(k & 0xffffffffull);
