@@ -966,14 +966,24 @@ reduce_kernel(int64_t G, const int* __restrict__ inst_offset, const long long* _
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, c = a;
+    auto add = [&](const float4 x, const float4 y, const float4 z) {
+        a.x += x.x; a.y += x.y; a.z += x.z; a.w += x.w;
+        b.x += y.x; b.y += y.y; b.z += y.z; b.w += y.w;
+        c.x += z.x; c.y += z.y; c.z += z.z;
+    };
     if (header[H_FLAGS] == 0) {
         const int i0 = inst_offset[g], i1 = inst_offset[g + 1];
-        for (int i = i0; i < i1; ++i) {
-            const float4 x = partial[3 * (int64_t)i], y = partial[3 * (int64_t)i + 1], z = partial[3 * (int64_t)i + 2];
-            a.x += x.x; a.y += x.y; a.z += x.z; a.w += x.w;
-            b.x += y.x; b.y += y.y; b.z += y.z; b.w += y.w;
-            c.x += z.x; c.y += z.y; c.z += z.z;
+        const float4* src = partial + 3 * (int64_t)i0;
+        int i = i0;
+        // four instances' loads in flight at a time; the sums keep instance order
+        for (; i + 4 <= i1; i += 4, src += 12) {
+            float4 v[12];
+#pragma unroll
+            for (int u = 0; u < 12; ++u) v[u] = src[u];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) add(v[3 * u], v[3 * u + 1], v[3 * u + 2]);
         }
+        for (; i < i1; ++i, src += 3) add(src[0], src[1], src[2]);
     }
     d_means[3 * g + 0] = a.x;
     d_means[3 * g + 1] = a.y;
