@@ -99,10 +99,17 @@ class Clocks:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+        # the timed region starts once the sampler is running (first sample written)
+        t0 = time.time()
+        while self.proc is not None and self.proc.poll() is None and time.time() - t0 < 5.0:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.01)
+        self.skip = 1 if self.proc is not None and os.path.getsize(self.path) > 0 else 0
         return self
 
     def __exit__(self, *exc):
@@ -118,7 +125,8 @@ class Clocks:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        # the first sample precedes the timed region
+        for line in open(self.path).readlines()[getattr(self, "skip", 0):]:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -431,6 +439,7 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
     def step(i):
         sl = slots[i % 2]
         sl["landed"].synchronize()  # step i-2's loss and gradients are on the host
+        sl["outs"] = None  # ... so its device results can be recycled
         if sl["step"] != i:
             prefetch(i)
         compute.wait_event(sl["ready"])
@@ -448,9 +457,8 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
             sl["loss_host"].copy_(outs[0], non_blocking=True)
             for gh, g in zip(sl["grad_host"], outs[1:]):
                 gh.copy_(g, non_blocking=True)
-            for t in outs:
-                t.record_stream(d2h_stream)
             sl["landed"].record(d2h_stream)
+        sl["outs"] = outs  # kept until the copies have landed (no cross-stream frees)
         sl["free"].record(compute)
 
     def timed_e2e(steps, warm):
