@@ -308,8 +308,8 @@ static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_ke
                                                         unsigned long long* __restrict__ keys,
                                                         const int* __restrict__ slot_inst,
                                                         int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
-                                                        const unsigned char* __restrict__ slot_mask,
-                                                        unsigned char* __restrict__ sorted_mask) {
+                                                        const uint16_t* __restrict__ slot_mask,
+                                                        uint16_t* __restrict__ sorted_mask) {
     int npow = 64;
     while (npow < n) npow <<= 1;
     for (int i = threadIdx.x; i < npow; i += blockDim.x) {
@@ -331,13 +331,13 @@ static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_ke
 // order the reference's stable radix sort of (tile << 32 | depth key) over instances
 // enumerated Gaussian by Gaussian produces (src/mapper/wrapper_mapper.cu:134-146). Keys
 // within a bucket are distinct (a Gaussian enters a tile's bucket at most once), so any
-// correct sorting network gives that order. The optional per-slot byte (slot_mask) follows
+// correct sorting network gives that order. The optional 16-bit per-slot mask (slot_mask) follows
 // its instance into sorted_mask.
 static __global__ void __launch_bounds__(SORT_THREADS, SORT_MIN_BLOCKS)
 tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
                  unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
                  int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
-                 const unsigned char* __restrict__ slot_mask, unsigned char* __restrict__ sorted_mask) {
+                 const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask) {
     __shared__ __align__(16) unsigned long long s_keys[SORT_SMEM_CAP];
     __shared__ __align__(16) int s_idx[SORT_SMEM_CAP];
     const int64_t t = blockIdx.x;
@@ -371,7 +371,7 @@ static __global__ void __launch_bounds__(SORT_THREADS)
 tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
                      unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
                      int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
-                     const unsigned char* __restrict__ slot_mask, unsigned char* __restrict__ sorted_mask) {
+                     const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask) {
     extern __shared__ __align__(16) unsigned long long s_big_keys[];
     int* s_big_idx = reinterpret_cast<int*>(s_big_keys + SORT_BIG_CAP);
     __shared__ int s_list[SORT_THREADS];
@@ -410,8 +410,8 @@ static inline size_t tile_sort_big_smem_bytes() { return SORT_BIG_CAP * (sizeof(
 static inline cudaError_t launch_tile_sort(int64_t T, const int* tile_start, const long long* header,
                                            unsigned long long* keys, const int* slot_inst, int* sorted_gid,
                                            int* sorted_inst, bool* attr_done, cudaStream_t stream,
-                                           const unsigned char* slot_mask = nullptr,
-                                           unsigned char* sorted_mask = nullptr) {
+                                           const uint16_t* slot_mask = nullptr,
+                                           uint16_t* sorted_mask = nullptr) {
     if (T <= 0) return cudaSuccess;
     tile_sort_kernel<<<(unsigned)T, SORT_THREADS, 0, stream>>>(T, tile_start, header, keys, slot_inst, sorted_gid,
                                                                 sorted_inst, slot_mask, sorted_mask);

@@ -46,10 +46,17 @@ constexpr int TILE_PIX = TILE * TILE;
 // threads resident CTAs per SM).
 constexpr int FWD_BATCH = 512;
 constexpr int BWD_THREADS = 256;
-// A tile's pixels are shaded by 8 warps, each owning a block of 8 columns x 4 rows; bit
-// (band * 2 + half) of an instance's block mask is set when the Gaussian can reach block
-// (4-row band `band`, 8-column half `half`) of that tile.
+// A tile's pixels are shaded by 8 warps, each owning a block of 8 columns x 4 rows (warp
+// w = 2 * band + half). An instance's mask marks 4x4-pixel sub-blocks: bit (band * 4 + quarter)
+// is set when the Gaussian can reach sub-block (4-row band, 4-column quarter) of the tile, so
+// warp block w is sub-blocks 2w and 2w + 1. The forward visits an instance when either of its
+// warp's sub-blocks is marked; the backward sweeps the marked sub-blocks only.
 constexpr int BLK_W = 8, BLK_H = 4;
+constexpr int SUB = 4;                                    // sub-block edge (pixels)
+constexpr int NSUB = (TILE / SUB) * (TILE / SUB);         // 16 sub-blocks per tile
+constexpr int SUB_PIX = SUB * SUB;                        // 16 pixels per sub-block
+typedef uint16_t blockmask_t;
+constexpr unsigned FULL_MASK = 0xffffu;
 constexpr int BWD_CHUNK = 1024;      // instances regrouped per backward pass
 
 // Header words at the start of the workspace.
@@ -78,8 +85,8 @@ struct Workspace {
     int* slot_inst;          // cap: instance index of each bucket slot (unsorted)
     int* sorted_gid;         // cap
     int* sorted_inst;        // cap
-    unsigned char* slot_mask;    // cap: warp-block mask of each bucket slot (unsorted)
-    unsigned char* sorted_mask;  // cap
+    blockmask_t* slot_mask;    // cap: sub-block mask of each bucket slot (unsorted)
+    blockmask_t* sorted_mask;  // cap
     float2* pixel_aux;       // P: no-skip sums (sum a*c, sum a*depth) for the backward
     size_t bytes;
 };
@@ -116,8 +123,8 @@ static Workspace carve(void* base, int64_t G, int64_t T, int64_t P, int64_t cap)
     w.slot_inst = c.take<int>((size_t)cap);
     w.sorted_gid = c.take<int>((size_t)cap);
     w.sorted_inst = c.take<int>((size_t)cap);
-    w.slot_mask = c.take<unsigned char>((size_t)cap);
-    w.sorted_mask = c.take<unsigned char>((size_t)cap);
+    w.slot_mask = c.take<blockmask_t>((size_t)cap);
+    w.sorted_mask = c.take<blockmask_t>((size_t)cap);
     w.pixel_aux = c.take<float2>((size_t)P);
     w.bytes = align_up(c.off, 256);
     return w;
@@ -501,7 +508,7 @@ __device__ __forceinline__ int task_tiles(const int4 r, const Geo& geo, const fl
     int n = 0;
     for (int y = r.y; y < r.w; ++y) {
         int xa = r.x, xb = r.z;
-        double bl[TILE / BLK_H], br[TILE / BLK_H];
+        double bl[TILE / SUB], br[TILE / SUB];
         if (E.ok) {
             double xl, xr;
             if (!ellipse_row_range(E, y * TILE, min(y * TILE + TILE - 1, geo.H - 1), xl, xr)) continue;
@@ -510,10 +517,10 @@ __device__ __forceinline__ int task_tiles(const int4 r, const Geo& geo, const fl
             xb = min(xb, (int)floor(fmin(xr, 1e9) / TILE) + 1);
             if (WANT_BLOCKS && xa < xb) {
 #pragma unroll
-                for (int sb = 0; sb < TILE / BLK_H; ++sb) {
-                    const int ya = y * TILE + sb * BLK_H;
+                for (int sb = 0; sb < TILE / SUB; ++sb) {
+                    const int ya = y * TILE + sb * SUB;
                     double u = 1e300, v = -1e300;  // empty band
-                    if (ya <= geo.H - 1 && ellipse_row_range(E, ya, min(ya + BLK_H - 1, geo.H - 1), u, v) &&
+                    if (ya <= geo.H - 1 && ellipse_row_range(E, ya, min(ya + SUB - 1, geo.H - 1), u, v) &&
                         !(u <= v)) {
                         u = -1e300;  // NaN: keep the whole band
                         v = 1e300;
@@ -526,15 +533,15 @@ __device__ __forceinline__ int task_tiles(const int4 r, const Geo& geo, const fl
         if (xa >= xb) continue;
         const bool ell = E.ok != 0;
         row(geo.tile_off + y * geo.tx, xa, xb, n, [&](int x) -> unsigned {
-            unsigned blocks = 0xffu;
+            unsigned blocks = FULL_MASK;
             if (WANT_BLOCKS && ell) {
                 blocks = 0u;
 #pragma unroll
-                for (int sb = 0; sb < TILE / BLK_H; ++sb)
+                for (int sb = 0; sb < TILE / SUB; ++sb)
 #pragma unroll
-                    for (int bx = 0; bx < TILE / BLK_W; ++bx) {
-                        const double c0 = (double)(x * TILE + bx * BLK_W), c1 = c0 + (BLK_W - 1);
-                        if (bl[sb] <= c1 && br[sb] >= c0) blocks |= 1u << (sb * (TILE / BLK_W) + bx);
+                    for (int qx = 0; qx < TILE / SUB; ++qx) {
+                        const double c0 = (double)(x * TILE + qx * SUB), c1 = c0 + (SUB - 1);
+                        if (bl[sb] <= c1 && br[sb] >= c0) blocks |= 1u << (sb * (TILE / SUB) + qx);
                     }
             }
             return blocks;
@@ -576,7 +583,7 @@ task_scatter_kernel(const long long* __restrict__ header, const us3d_slice_frame
                     const int2* __restrict__ task_gf, const float* __restrict__ task_v,
                     const int* __restrict__ task_inst, const int* __restrict__ tile_start, int* __restrict__ tile_cursor,
                     unsigned long long* __restrict__ keys, int* __restrict__ slot_inst,
-                    unsigned char* __restrict__ slot_mask) {
+                    blockmask_t* __restrict__ slot_mask) {
     if (header[H_FLAGS] != 0) return;
     const long long nt = header[H_NTASK];
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += (long long)gridDim.x * blockDim.x) {
@@ -603,7 +610,7 @@ task_scatter_kernel(const long long* __restrict__ header, const us3d_slice_frame
                                      if (slot >= tile_start[t + 1]) continue;
                                      keys[slot] = key;
                                      slot_inst[slot] = i0 + i + (x0 - xa) + u;
-                                     slot_mask[slot] = (unsigned char)blocks_of(x0 + u);
+                                     slot_mask[slot] = (blockmask_t)blocks_of(x0 + u);
                                  }
                              }
                          });
@@ -696,13 +703,13 @@ template <int BATCH, bool WINDOWED>
 __global__ void __launch_bounds__(TILE_PIX, US3D_UG_FWD_MIN_CTAS)
 forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
-               const unsigned char* __restrict__ sorted_mask, const long long* __restrict__ header,
+               const blockmask_t* __restrict__ sorted_mask, const long long* __restrict__ header,
                const float4* __restrict__ pack, const float* __restrict__ pixels, float chi2, float beta,
                float bg_alpha, float bg_intensity, float* __restrict__ out_image, float* __restrict__ out_alpha,
                float* __restrict__ out_depth, float2* __restrict__ pixel_aux) {
     constexpr int STRIDE = WINDOWED ? 4 : 3;
     __shared__ float4 s_st[STRIDE * BATCH];
-    __shared__ unsigned char s_blocks[BATCH];
+    __shared__ blockmask_t s_blocks[BATCH];
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
     const Geo geo = load_geo(frames + tile_frame[t]);
@@ -770,7 +777,7 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
         }
         for (int jc = 0; jc < nb; jc += 32) {
             const int jl = jc + lane;
-            unsigned bits = __ballot_sync(0xffffffffu, jl < nb && ((s_blocks[jl] >> warp) & 1u));
+            unsigned bits = __ballot_sync(0xffffffffu, jl < nb && ((s_blocks[jl] >> (2 * warp)) & 3u));
             while (bits != 0u) {
                 const int j = jc + __ffs(bits) - 1;
                 bits &= bits - 1u;
@@ -789,12 +796,12 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
 }
 
 // One block per tile; each thread owns one instance of the tile list at a time and sweeps the
-// pixels of the warp blocks its mask marks (pixels and their upstream coefficients sit in
-// shared memory in warp-block-major order). Instances are regrouped by the number of marked
-// blocks so that the lanes of a warp do similar amounts of work; every instance's sums run
-// over its blocks in ascending order, pixel order within block b rotated by b (conflict-free
-// shared-memory reads across lanes in different blocks), so its partial does not depend on
-// the grouping, and blocks without a contributing pixel add nothing.
+// pixels of the 4x4 sub-blocks its mask marks (pixels and their upstream coefficients sit in
+// shared memory in sub-block-major order). Instances are regrouped by the number of marked
+// sub-blocks so that the lanes of a warp do similar amounts of work; every instance's sums run
+// over its sub-blocks in ascending order, pixel order within sub-block c rotated by c (lanes in
+// different sub-blocks mostly read different banks), so its partial does not depend on the
+// grouping, and sub-blocks without a contributing pixel add nothing.
 // LOSS: dL/dimage comes from the fused per-frame loss (L1 + global SSIM of image against
 // target, coefficients per frame in loss_coef; see us3d_ug_loss) and dL/dalpha = dL/ddepth =
 // 0; otherwise from d_image, d_alpha, d_depth.
@@ -804,19 +811,19 @@ template <bool LOSS, int THREADS, bool WINDOWED>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, const int* __restrict__ tile_frame,
                 const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
-                const int* __restrict__ sorted_inst, const unsigned char* __restrict__ sorted_mask,
+                const int* __restrict__ sorted_inst, const blockmask_t* __restrict__ sorted_mask,
                 const long long* __restrict__ header, const float4* __restrict__ pack,
                 const float* __restrict__ pixels, const float* __restrict__ d_image, const float* __restrict__ d_alpha,
                 const float* __restrict__ d_depth, const float* __restrict__ saved_alpha,
                 const float2* __restrict__ pixel_aux, float chi2, float beta, float bg_alpha,
                 float bg_intensity, const float* __restrict__ loss_image, const float* __restrict__ loss_target,
                 const float4* __restrict__ loss_coef, float4* __restrict__ partial) {
-    // Per warp block b, entries [64 b, 64 b + 64) hold its 32 pixels twice, so that the sweep
-    // rotated by b reads 32 consecutive entries from 65 b.
+    // Per sub-block c, entries [32 c, 32 c + 32) hold its 16 pixels twice, so that the sweep
+    // rotated by c reads 16 consecutive entries from 33 c.
     __shared__ float4 s_pa[2 * TILE_PIX];  // pixel position, dL/dnum
     __shared__ float2 s_pb[2 * TILE_PIX];  // dL/dalpha_total + dL/dsum_alpha (depth), dL/ddepth_weighted
     __shared__ short s_perm[BWD_CHUNK];
-    __shared__ int s_class[9];
+    __shared__ int s_class[NSUB + 1];
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0) return;
     const int s0 = tile_start[t];
@@ -826,8 +833,9 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
     int tx, ty;
     find_tile_coords(geo, t, tx, ty);
     for (int slot = threadIdx.x; slot < TILE_PIX; slot += THREADS) {
-        const int r = block_row(slot), c = block_col(slot);
-        const int e0 = (slot >> 5) * 64 + (slot & 31), e1 = e0 + 32;
+        const int sc = slot / SUB_PIX, within = slot % SUB_PIX;  // sub-block, pixel in it
+        const int r = (sc / (TILE / SUB)) * SUB + within / SUB, c = (sc % (TILE / SUB)) * SUB + within % SUB;
+        const int e0 = sc * (2 * SUB_PIX) + within, e1 = e0 + SUB_PIX;
         const int64_t p = (int64_t)geo.pix_off + (int64_t)(ty * TILE + r) * geo.W + (tx * TILE + c);
         if (ty * TILE + r < geo.H && tx * TILE + c < geo.W && p < P) {
             // Per-pixel adjoint coefficients (reference src/shader/backward.cu:175-197).
@@ -865,15 +873,15 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
 
     for (int c0 = 0; c0 < n; c0 += BWD_CHUNK) {
         const int nc = min(BWD_CHUNK, n - c0);
-        if (threadIdx.x < 9) s_class[threadIdx.x] = 0;
+        if (threadIdx.x <= NSUB) s_class[threadIdx.x] = 0;
         __syncthreads();
         if (culled) {
             for (int k = threadIdx.x; k < nc; k += blockDim.x)
-                atomicAdd(&s_class[8 - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1);
+                atomicAdd(&s_class[NSUB - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1);
             __syncthreads();
             if (threadIdx.x == 0) {
                 int acc = 0;
-                for (int i = 0; i < 9; ++i) {
+                for (int i = 0; i <= NSUB; ++i) {
                     const int v = s_class[i];
                     s_class[i] = acc;
                     acc += v;
@@ -881,7 +889,7 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
             }
             __syncthreads();
             for (int k = threadIdx.x; k < nc; k += blockDim.x)
-                s_perm[atomicAdd(&s_class[8 - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1)] = (short)k;
+                s_perm[atomicAdd(&s_class[NSUB - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1)] = (short)k;
             __syncthreads();
         }
 
@@ -905,10 +913,10 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
             float sxx = 0.f, sxy = 0.f, sxz = 0.f, syy = 0.f, syz = 0.f, szz = 0.f;
             for (unsigned mb = blocks; mb != 0u; mb &= mb - 1u) {
                 const int blk = __ffs(mb) - 1;
-                const float4* pa_b = s_pa + blk * 65;
-                const float2* pb_b = s_pb + blk * 65;
+                const float4* pa_b = s_pa + blk * (2 * SUB_PIX + 1);
+                const float2* pb_b = s_pb + blk * (2 * SUB_PIX + 1);
 #pragma unroll
-                for (int jj = 0; jj < 32; ++jj) {
+                for (int jj = 0; jj < SUB_PIX; ++jj) {
                     const float4 pa = pa_b[jj];
                     const float3 d = make_float3(pa.x - m.x, pa.y - m.y, pa.z - m.z);
                     if constexpr (WINDOWED) {
