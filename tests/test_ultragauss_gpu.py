@@ -395,6 +395,58 @@ def test_slice_cull_dropin_renderer(cuda_device):
         assert torch.equal(a, c)
 
 
+def test_autograd_steps_free_memory_without_gc(cuda_device):
+    """Forward + backward through both autograd entry points (the drop-in renderer and the
+    batched renderer), with the cyclic garbage collector off: once a step's tensors are dropped,
+    the memory in use returns to its level before the step (nothing the step allocated is kept
+    alive by a reference cycle through the autograd graph)."""
+    import gc
+
+    from ultragauss_renderer import SliceGeometry, UltraGaussRenderConfig, UltraGaussRenderer
+    from us3d_b200 import scenes
+    from us3d_b200 import ultragauss as UG
+    from us3d_b200.batch import UltraGaussBatchRenderer
+
+    dev = cuda_device
+    sc = scenes.make_scene(40000, seed=9).to(dev)
+    sweep = scenes.linear_sweep(3, 160, 160, 0.25, seed=9)
+    fr = sweep[1].to(dev)
+    cfg = UltraGaussRenderConfig(H=160, W=160, lateral_spacing_mm_per_pix=0.25, axial_spacing_mm_per_pix=0.25,
+                                 axial_near_mm=fr.axial_near, lateral_col_offset=fr.lateral_col_offset)
+    geo = SliceGeometry(fr.origin, fr.axis_lat, fr.axis_ax, fr.axis_ele)
+    specs = [UG.SliceSpec(f.height, f.width, f.lateral_spacing, f.axial_spacing, f.axial_near, f.lateral_col_offset,
+                          f.origin, f.axis_lat, f.axis_ax, f.axis_ele) for f in sweep]
+    batch_pix = torch.cat([f.pixels for f in sweep]).to(dev)
+    batched = UltraGaussBatchRenderer(specs, dev)
+
+    def dropin_step():
+        ps = [x.clone().requires_grad_(True) for x in (sc.means, sc.precision_tril, sc.opacities, sc.intensities)]
+        img, alpha, depth, _ = UltraGaussRenderer(cfg)(*ps, fr.pixels, geo, return_intermediates=False)
+        (img.sum() + alpha.sum() + depth.sum()).backward()
+
+    def batched_step():
+        ps = [x.clone().requires_grad_(True) for x in (sc.means, sc.precision_tril, sc.opacities, sc.intensities)]
+        img, alpha, depth = batched(*ps, batch_pix)
+        (img.sum() + alpha.sum() + depth.sum()).backward()
+        batched.last = {}
+
+    gc.collect()
+    was_enabled = gc.isenabled()
+    gc.disable()
+    try:
+        for step in (dropin_step, batched_step):
+            step()  # first call: kernel attributes, cached backward scratch
+            torch.cuda.synchronize()
+            before = torch.cuda.memory_allocated(dev)
+            for _ in range(3):
+                step()
+            torch.cuda.synchronize()
+            assert torch.cuda.memory_allocated(dev) == before, step.__name__
+    finally:
+        if was_enabled:
+            gc.enable()
+
+
 def test_graphed_training_step_matches_eager(cuda_device):
     """A CUDA-graph replay of bin + forward + loss gradient + backward equals the same step
     run eagerly, also after the parameters are updated in place between replays."""

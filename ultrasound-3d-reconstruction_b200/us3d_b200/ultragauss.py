@@ -9,7 +9,7 @@ different sizes (the batched form); the plain drop-in renderer bins one frame pe
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import List, Optional, Sequence
 
 import torch
@@ -109,7 +109,6 @@ class UGBinning:
     slice_cull: bool = False
     pixels: Optional[torch.Tensor] = None
     counts: Optional[torch.Tensor] = None
-    alpha: Optional[torch.Tensor] = field(default=None, repr=False)
 
 
 def _check_params(means, tril, opac, inten):
@@ -189,10 +188,37 @@ def forward(b: UGBinning, pixels: torch.Tensor, bg_alpha: float, bg_intensity: f
         _ptr(alpha), _ptr(depth), _ptr(counts), _stream(),
     )
     _lib.check(st, "us3d_ug_forward")
+    # No reference to the outputs here: an autograd function keeping the binning on its ctx
+    # would otherwise form a cycle (output -> node -> binning -> output) that only the cyclic
+    # garbage collector frees, keeping each step's workspace alive for an unknown time.
     b.pixels = pixels
     b.counts = counts
-    b.alpha = alpha
     return image, alpha, depth, counts
+
+
+# Backward scratch (the per-instance partials) kept per (device, stream): the partials are
+# consumed by the same call's reduction, and a later call on the same stream runs after it, so
+# every call on a stream can reuse one buffer instead of allocating ~48 bytes per instance.
+_SCRATCH = {}
+
+
+def _backward_scratch(dev: torch.device, nbytes: int) -> torch.Tensor:
+    if torch.cuda.is_current_stream_capturing():
+        # a graph keeps its own (private pool) buffer: the cached one may be freed later
+        return torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
+    key = (dev.index if dev.index is not None else torch.cuda.current_device(),
+           torch.cuda.current_stream(dev).cuda_stream)
+    buf = _SCRATCH.get(key)
+    if buf is None or buf.numel() < nbytes:
+        _SCRATCH.pop(key, None)
+        buf = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
+        _SCRATCH[key] = buf
+    return buf
+
+
+def release_scratch() -> None:
+    """Frees the backward scratch buffers kept per stream (they are re-created on demand)."""
+    _SCRATCH.clear()
 
 
 def backward(b: UGBinning, pixels: torch.Tensor, d_image: torch.Tensor, d_alpha: torch.Tensor,
@@ -203,7 +229,7 @@ def backward(b: UGBinning, pixels: torch.Tensor, d_image: torch.Tensor, d_alpha:
     dev = pixels.device
     sbytes = int(_lib.call("us3d_ug_backward_scratch_bytes", b.capacity))
     if scratch is None or scratch.numel() < sbytes:
-        scratch = torch.empty(max(sbytes, 16), dtype=torch.uint8, device=dev)
+        scratch = _backward_scratch(dev, sbytes)
     if out is None:
         out = (
             torch.empty((G, 3), dtype=torch.float32, device=dev),
@@ -251,7 +277,7 @@ def backward_loss(b: UGBinning, pixels: torch.Tensor, image: torch.Tensor, targe
     dev = pixels.device
     sbytes = int(_lib.call("us3d_ug_backward_scratch_bytes", b.capacity))
     if scratch is None or scratch.numel() < sbytes:
-        scratch = torch.empty(max(sbytes, 16), dtype=torch.uint8, device=dev)
+        scratch = _backward_scratch(dev, sbytes)
     if out is None:
         out = (
             torch.empty((G, 3), dtype=torch.float32, device=dev),
