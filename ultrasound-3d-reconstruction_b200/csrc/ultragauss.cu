@@ -710,6 +710,7 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     constexpr int STRIDE = WINDOWED ? 4 : 3;
     __shared__ float4 s_st[STRIDE * BATCH];
     __shared__ blockmask_t s_blocks[BATCH];
+    __shared__ short s_list[TILE_PIX / 32][BATCH];  // per warp: staged Gaussians reaching its block
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
     const Geo geo = load_geo(frames + tile_frame[t]);
@@ -736,17 +737,21 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
             const float4 f3 = s_st[STRIDE * j + 3];
             if (!window_hit(d, geo.lat, geo.ax, f3.x, f3.y)) return;
         }
+        // The exponential is evaluated for every pair and the sums are predicated: the lanes of
+        // a warp (one 8x4 block) run the pair together anyway.
         const float q = quad_form(d, f1, f2.x, f2.y);
-        if (q > chi2) return;
         const float ah = f0.w * __expf(-0.5f * q);
-        if (ah <= 1e-8f) {
+        const bool pass = q <= chi2;
+        const bool keep = pass && ah > 1e-8f;
+        if (keep) {
+            sa += ah;
+            sc += ah * f2.z;
+            sd += ah * f2.w;
+        }
+        if (pass && !keep) {
             kc += ah * f2.z;
             kd += ah * f2.w;
-            return;
         }
-        sa += ah;
-        sc += ah * f2.z;
-        sd += ah * f2.w;
     };
     for (int b0 = 0; b0 < n; b0 += BATCH) {
         const int nb = min(BATCH, n - b0);
@@ -775,15 +780,18 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
             for (int j = 0; j < nb; ++j) shade(j);
             continue;
         }
+        // Each warp lists, in staging order, the Gaussians whose mask marks one of its two
+        // sub-blocks, then shades them.
+        int n_w = 0;
         for (int jc = 0; jc < nb; jc += 32) {
             const int jl = jc + lane;
-            unsigned bits = __ballot_sync(0xffffffffu, jl < nb && ((s_blocks[jl] >> (2 * warp)) & 3u));
-            while (bits != 0u) {
-                const int j = jc + __ffs(bits) - 1;
-                bits &= bits - 1u;
-                shade(j);
-            }
+            const bool mine = jl < nb && ((s_blocks[jl] >> (2 * warp)) & 3u);
+            const unsigned bits = __ballot_sync(0xffffffffu, mine);
+            if (mine) s_list[warp][n_w + __popc(bits & ((1u << lane) - 1u))] = (short)jl;
+            n_w += __popc(bits);
         }
+        __syncwarp();
+        for (int k = 0; k < n_w; ++k) shade(s_list[warp][k]);
     }
     if (!valid) return;
     const float alpha_total = sa + bg_alpha;

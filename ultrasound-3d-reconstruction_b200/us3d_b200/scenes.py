@@ -66,14 +66,30 @@ def quat_to_rot(q: torch.Tensor) -> torch.Tensor:
 
 def precision_tril_from_scales_quats(scales: torch.Tensor, quats: torch.Tensor, beta: float = 1e-4) -> torch.Tensor:
     """Raw lower-Cholesky factor of Lambda = R diag(1/s^2) R^T with diagonal raw^2 + beta
-    (the parameterisation UltraGauss learns); computed in float64."""
+    (the parameterisation UltraGauss learns); computed in float64 with elementwise operations
+    only, written out for 3x3 matrices: batched BLAS / LAPACK kernels may round differently
+    from run to run (buffer alignment, threads), which would make the scenes, and results that
+    sit on a threshold, differ between processes."""
     s = scales.double().clamp_min(beta)
     R = quat_to_rot(quats.double())
-    lam = R @ torch.diag_embed(1.0 / (s * s)) @ R.transpose(-1, -2)
-    L = torch.linalg.cholesky(lam)
-    diag = torch.diagonal(L, dim1=-2, dim2=-1)
-    raw = (diag - beta).clamp_min(1e-8).sqrt()
-    return torch.stack([raw[:, 0], L[:, 1, 0], L[:, 2, 0], raw[:, 1], L[:, 2, 1], raw[:, 2]], dim=1).float()
+    inv = 1.0 / (s * s)
+
+    def lam(i, j):  # Lambda_ij = sum_k R_ik R_jk / s_k^2
+        return (R[:, i, 0] * R[:, j, 0] * inv[:, 0] + R[:, i, 1] * R[:, j, 1] * inv[:, 1]
+                + R[:, i, 2] * R[:, j, 2] * inv[:, 2])
+
+    a00, a10, a20, a11, a21, a22 = lam(0, 0), lam(1, 0), lam(2, 0), lam(1, 1), lam(2, 1), lam(2, 2)
+    l00 = a00.sqrt()
+    l10 = a10 / l00
+    l20 = a20 / l00
+    l11 = (a11 - l10 * l10).sqrt()
+    l21 = (a21 - l20 * l10) / l11
+    l22 = (a22 - l20 * l20 - l21 * l21).sqrt()
+
+    def raw(d):
+        return (d - beta).clamp_min(1e-8).sqrt()
+
+    return torch.stack([raw(l00), l10, l20, raw(l11), l21, raw(l22)], dim=1).float()
 
 
 def make_scene(n: int, seed: int = 0, cube_mm: float = 64.0, log_scale_mean: float = 0.0,
