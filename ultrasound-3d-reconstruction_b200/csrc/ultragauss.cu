@@ -930,10 +930,11 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
                     if constexpr (WINDOWED) {
                         if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
                     }
+                    // A pair failing the chi-square test gets w = 0, so that every term it adds is
+                    // an exact zero: no branch in the unrolled sweep.
                     const float q = quad_form(d, q1, s12, s22);
-                    if (q > chi2) continue;
                     const float2 pb = pb_b[jj];
-                    const float w = __expf(-0.5f * q);
+                    const float w = q <= chi2 ? __expf(-0.5f * q) : 0.0f;
                     const float ah = o * w;
                     const float dah = pa.w * ci + pb.x + pb.y * dterm;
                     acc_c += pa.w * ah;

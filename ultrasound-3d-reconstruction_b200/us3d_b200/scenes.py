@@ -95,14 +95,19 @@ def precision_tril_from_scales_quats(scales: torch.Tensor, quats: torch.Tensor, 
 def make_scene(n: int, seed: int = 0, cube_mm: float = 64.0, log_scale_mean: float = 0.0,
                log_scale_std: float = 0.3, opacity_mu: float = 0.0, opacity_std: float = 1.0,
                beta: float = 1e-4) -> GaussianScene:
+    # The transcendental functions and the quaternion norm run in float64 on elementwise
+    # operations and are rounded to float32 once: CPU kernels evaluate exp / sigmoid / norms with
+    # vector and scalar code paths whose last bits differ, and which elements take which path can
+    # change from process to process.
     g = torch.Generator().manual_seed(seed)
     means = torch.rand((n, 3), generator=g) * cube_mm
-    scales = torch.exp(log_scale_mean + log_scale_std * torch.randn((n, 3), generator=g))
-    quats = torch.nn.functional.normalize(torch.randn((n, 4), generator=g), dim=-1)
+    scales64 = torch.exp(log_scale_mean + log_scale_std * torch.randn((n, 3), generator=g).double())
+    q = torch.randn((n, 4), generator=g).double()
+    q = q / (q[:, 0] * q[:, 0] + q[:, 1] * q[:, 1] + q[:, 2] * q[:, 2] + q[:, 3] * q[:, 3]).sqrt().clamp_min(1e-12)[:, None]
     intensities = torch.rand((n,), generator=g)
-    opacities = torch.sigmoid(opacity_mu + opacity_std * torch.randn((n,), generator=g))
-    tril = precision_tril_from_scales_quats(scales, quats, beta)
-    return GaussianScene(means, scales, quats, opacities, intensities, tril)
+    opacities = torch.sigmoid(opacity_mu + opacity_std * torch.randn((n,), generator=g).double()).float()
+    tril = precision_tril_from_scales_quats(scales64, q, beta)
+    return GaussianScene(means, scales64.float(), q.float(), opacities, intensities, tril)
 
 
 def slice_pixels(origin, lat, ax, H, W, lateral_spacing, axial_spacing, axial_near, col_offset) -> torch.Tensor:
