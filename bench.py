@@ -38,9 +38,11 @@ BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (param
 
 # DRAM bytes (read + write) per frame of each stage's dominant kernel, from one ncu capture
 # of a 4-frame launch of the same scene, scaled linearly to the frames of a launch.
+# dram__bytes_read.sum + dram__bytes_write.sum of one 4-frame launch of the headline scene
+# (ncu --set full), per frame; the backward stage is backward_kernel + reduce_kernel.
 NCU_TRAFFIC_PER_FRAME = {
-    "ug_backward": (98.878464e6 + 115.803392e6) / 4,  # backward_kernel, profiles/ultragauss_backward_kernel_4frames.md
-    "ug_forward": (49.083136e6 + 3.089408e6) / 4,     # forward_kernel, profiles/ultragauss_forward_kernel_4frames.md
+    "ug_backward": (101.160192e6 + 115.272448e6 + 156.033024e6 + 28.610560e6) / 4,
+    "ug_forward": (52.276224e6 + 5.576192e6) / 4,
 }
 
 
@@ -318,6 +320,13 @@ def run_b200(a):
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
                 "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
                 "algorithmic_bytes_per_launch": int(alg)}
+    # The whole step against the same peak, with the per-frame algorithmic bytes of the forward
+    # (params once, instance key + value written and read, outputs) plus the backward (params
+    # and gradients, instance list, saved outputs and upstream gradients).
+    b_frame = (G * BP + I * 16 + P * BO) + (G * (BP + BG) + I * 4 + P * (BO + BD))
+    step_gbs = b_frame * frames_total / (ms_batched / 1e3) / 1e9
+    roofline["step"] = {"bytes_per_frame": int(b_frame), "achieved": round(step_gbs, 2),
+                        "frac": round(step_gbs / peak, 4)}
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
