@@ -674,6 +674,8 @@ __device__ __forceinline__ float quad_form(const float3 d, const float4 q1, cons
            (q1.z * d.x + s12 * d.y + s22 * d.z) * d.z;
 }
 
+constexpr float kNegHalfLog2e = -0.72134752044448170f;  // -log2(e) / 2
+
 // When the diagonal of L is at least 1e-10 (beta >= 1e-10), the lateral/axial window of the
 // reference is the bounding box of the chi-square ellipsoid (the clamps inside window_radii only
 // widen it), so q <= chi2 implies the window test up to float rounding and the test can be left
@@ -931,16 +933,17 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
                         if (!window_hit(d, geo.lat, geo.ax, r_lat, r_ax)) continue;
                     }
                     // A pair failing the chi-square test gets w = 0, so that every term it adds is
-                    // an exact zero: no branch in the unrolled sweep.
+                    // an exact zero: no branch in the unrolled sweep. exp(-q/2) = 2^(q c) with
+                    // c = -log2(e)/2.
                     const float q = quad_form(d, q1, s12, s22);
                     const float2 pb = pb_b[jj];
-                    const float w = q <= chi2 ? __expf(-0.5f * q) : 0.0f;
+                    const float w = q <= chi2 ? exp2f(q * kNegHalfLog2e) : 0.0f;
                     const float ah = o * w;
                     const float dah = pa.w * ci + pb.x + pb.y * dterm;
                     acc_c += pa.w * ah;
                     acc_o += dah * w;
                     acc_e += pb.y * ah;
-                    const float dq = -0.5f * dah * ah;
+                    const float dq = dah * ah;  // dL/dq without its factor -1/2 (applied below)
                     const float ux = dq * d.x, uy = dq * d.y, uz = dq * d.z;
                     sdx += ux;
                     sdy += uy;
@@ -953,6 +956,10 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
                     szz += uz * d.z;
                 }
             }
+            // The factor -1/2 of dL/dq, applied once: scaling by a power of two commutes with
+            // the roundings of the sums.
+            sdx *= -0.5f; sdy *= -0.5f; sdz *= -0.5f;
+            sxx *= -0.5f; sxy *= -0.5f; sxz *= -0.5f; syy *= -0.5f; syz *= -0.5f; szz *= -0.5f;
             // d/dmean = -2 Lambda sum(dq d) + sum(ddw * ah) * ele (reference backward.cu:218-228).
             const float vx = q1.x * sdx + q1.y * sdy + q1.z * sdz;
             const float vy = q1.y * sdx + q1.w * sdy + s12 * sdz;
