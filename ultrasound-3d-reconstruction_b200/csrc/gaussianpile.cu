@@ -22,6 +22,8 @@
 // rectangles, window test, weights) uses the reference's operations in the reference's
 // order, so that with the same --use_fast_math flags rectangles, sorted ids and tile ranges
 // are bit-exact and images match to rounding of the summation.
+#include <algorithm>
+
 #include "us3d_common.cuh"
 #include "scan.cuh"
 #include "binning.cuh"
@@ -53,6 +55,8 @@ struct Workspace {
     int* tile_cursor;   // T
     long long* bs_t;
     float4* cand;       // G x 3: (base_weight, intensity, mu2_lat, mu2_ax) (inv00, inv01, inv11, r_lat) (r_ax, valid)
+    float4* bfp;        // G x 4: the forward's footprint for the backward: (mu2_lat, mu2_ax, r_lat, r_ax)
+                        // (inv00, inv01, inv11, det2) (s2_00, s2_01, s2_11, sc22) (sigma_ele, mu_ele, mu_ax, valid)
     unsigned long long* keys;
     int* slot_inst;
     int* sorted_gid;
@@ -74,6 +78,7 @@ static Workspace carve(void* base, int64_t G, int64_t T, int64_t cap) {
     w.tile_cursor = c.take<int>((size_t)T);
     w.bs_t = c.take<long long>((size_t)scan_num_blocks(T) + 1);
     w.cand = c.take<float4>((size_t)G * 3);
+    w.bfp = c.take<float4>((size_t)G * 4);
     w.keys = c.take<unsigned long long>((size_t)cap);
     w.slot_inst = c.take<int>((size_t)cap);
     w.sorted_gid = c.take<int>((size_t)cap);
@@ -275,7 +280,8 @@ preprocess_kernel(int64_t G, int H, int W, int tile, int tiles_x, int tiles_y, f
                   const float* __restrict__ scales, const float* __restrict__ quats, const float* __restrict__ opac,
                   const float* __restrict__ inten, const float* __restrict__ pose, const float* __restrict__ grid,
                   const float* __restrict__ params, int4* __restrict__ rects, uint32_t* __restrict__ dkey,
-                  int* __restrict__ touched, int* __restrict__ tile_count, float4* __restrict__ cand) {
+                  int* __restrict__ touched, int* __restrict__ tile_count, float4* __restrict__ cand,
+                  float4* __restrict__ bfp) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
     const Axes A = axes_from_pose(pose);
@@ -327,6 +333,10 @@ preprocess_kernel(int64_t G, int H, int W, int tile, int tiles_x, int tiles_y, f
     cand[3 * g + 0] = make_float4(bw, inten[g], Ff.mu2_lat, Ff.mu2_ax);
     cand[3 * g + 1] = make_float4(Ff.inv00, Ff.inv01, Ff.inv11, Ff.r_lat);
     cand[3 * g + 2] = make_float4(Ff.r_ax, valid ? 1.f : 0.f, 0.f, 0.f);
+    bfp[4 * g + 0] = make_float4(Ff.mu2_lat, Ff.mu2_ax, Ff.r_lat, Ff.r_ax);
+    bfp[4 * g + 1] = make_float4(Ff.inv00, Ff.inv01, Ff.inv11, Ff.det2);
+    bfp[4 * g + 2] = make_float4(Ff.s2_00, Ff.s2_01, Ff.s2_11, Ff.sc22);
+    bfp[4 * g + 3] = make_float4(Ff.sigma_ele, Ff.mu_ele, Ff.mu_ax, okf ? 1.f : 0.f);
 }
 
 __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
@@ -343,22 +353,32 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
 // Forward
 // ------------------------------------------------------------------------------------
 
-// One block of tile x tile threads per tile; candidates of the tile list are staged in
-// shared memory and every pixel sums intensity * weight over them in list order
-// (reference src/shader/forward.cu:88-210).
+// One block per tile with PARTS threads per pixel (tile x tile pixels rounded up to whole
+// warps, times PARTS); candidates of the tile list are staged in shared memory. The sum over a
+// pixel's candidates is split by Gaussian index into four classes (g mod 4), each summed in
+// list order, and the class sums are added as ((c0 + c1) + c2) + c3; thread part p of a pixel
+// owns the classes congruent to p mod PARTS. The grouping depends on neither PARTS nor the
+// tile size, so the image does not either (the reference sums the whole list in order,
+// src/shader/forward.cu:88-210: the results agree up to rounding).
+template <int PARTS>
 __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float* __restrict__ grid,
                                const float* __restrict__ params, const int* __restrict__ tile_start,
                                const int* __restrict__ sorted_gid, const long long* __restrict__ header,
                                const float4* __restrict__ cand, float* __restrict__ image) {
+    constexpr int PER = 4 / PARTS;  // classes per thread
     __shared__ float4 sc0[FWD_BATCH], sc1[FWD_BATCH];
     __shared__ float2 sc2[FWD_BATCH];
+    __shared__ unsigned char s_cls[FWD_BATCH];
+    __shared__ float s_class_sum[4 * 1024 / PARTS];
     if (header[H_FLAGS] != 0) return;
     const int t = blockIdx.x;
     const int tx = t % tiles_x, ty = t / tiles_x;
-    const int lx = threadIdx.x % tile, ly = threadIdx.x / tile;
+    const int npix = (tile * tile + 31) / 32 * 32;  // pixel slots per part (whole warps)
+    const int slot = threadIdx.x % npix, part = threadIdx.x / npix;
+    const int lx = slot % tile, ly = slot / tile;
     const int x = tx * tile + lx, y = ty * tile + ly;
-    // blocks are whole warps (tile x tile rounded up to 32 threads): the extra threads own no pixel
-    const bool valid = (int)threadIdx.x < tile * tile && (x < W) && (y < H);
+    // the extra slots of the last warp own no pixel
+    const bool valid = slot < tile * tile && (x < W) && (y < H);
     const float weight_min = params[UF_WEIGHT_MIN];
     float xi_lat = 0.f, xi_ax = 0.f;
     if (valid) {
@@ -366,7 +386,9 @@ __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float*
         xi_ax = static_cast<float>(y) * grid[SG_DELTA_AX_MM] + grid[SG_NEAR_MM];
     }
     const int s0 = tile_start[t], n = tile_start[t + 1] - s0;
-    float accum = 0.f;
+    float acc[PER];
+#pragma unroll
+    for (int c = 0; c < PER; ++c) acc[c] = 0.f;
     const int nthreads = blockDim.x;
     // The warp's pixel extent in mm: a candidate whose box misses it (with a margin for the
     // rounding of the per-pixel test) is skipped by the whole warp.
@@ -389,14 +411,16 @@ __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float*
             sc1[j] = cand[3 * g + 1];
             const float4 c2 = cand[3 * g + 2];
             sc2[j] = make_float2(c2.x, c2.y);
+            s_cls[j] = (unsigned char)(g & 3);
         }
         __syncthreads();
         for (int jc = 0; jc < nb; jc += 32) {
             bool near = false;
-            if (jc + lane < nb) {
-                const float2 c2 = sc2[jc + lane];
-                const float4 c0 = sc0[jc + lane];
-                const float rl = sc1[jc + lane].w;
+            const int jl = jc + lane;
+            if (jl < nb && (PARTS == 1 || (int)(s_cls[jl] % PARTS) == part)) {
+                const float2 c2 = sc2[jl];
+                const float4 c0 = sc0[jl];
+                const float rl = sc1[jl].w;
                 const float ml = 1e-5f * (fabsf(c0.z) + rl + fabsf(lat_lo) + fabsf(lat_hi)) + 1e-30f;
                 const float ma = 1e-5f * (fabsf(c0.w) + c2.x + fabsf(ax_lo) + fabsf(ax_hi)) + 1e-30f;
                 near = c2.y != 0.f && lat_hi >= c0.z - rl - ml && lat_lo <= c0.z + rl + ml &&
@@ -419,11 +443,27 @@ __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float*
                 if (!(quad >= 0.f) || !isfinite(quad)) continue;
                 const float weight = c0.x * expf(-0.5f * quad);
                 if (!isfinite(weight) || weight < weight_min) continue;
-                accum += c0.y * weight;
+                const float v = c0.y * weight;
+                if (PER == 1) {
+                    acc[0] += v;
+                } else {
+                    const int k = s_cls[j] / PARTS;  // this thread's class index
+#pragma unroll
+                    for (int c = 0; c < PER; ++c)
+                        if (c == k) acc[c] += v;
+                }
             }
         }
     }
-    if (valid) image[y * W + x] = accum;
+    // class c's sum sits in part c % PARTS, slot c / PARTS of its accumulators
+#pragma unroll
+    for (int c = 0; c < PER; ++c) s_class_sum[(c * PARTS + part) * npix + slot] = acc[c];
+    __syncthreads();
+    if (part != 0 || !valid) return;
+    float total = s_class_sum[slot];
+#pragma unroll
+    for (int c = 1; c < 4; ++c) total += s_class_sum[c * npix + slot];
+    image[y * W + x] = total;
 }
 
 // ------------------------------------------------------------------------------------
@@ -437,102 +477,129 @@ enum { P_MU_PROBE1 = 0, P_MU_PROBE2, P_SC22, P_MU_E0, P_MU_E1, P_SE00, P_SE01, P
        P_FP_MU2_LAT, P_FP_MU2_AX, P_FP_INV00, P_FP_INV01, P_FP_INV11, P_FP_DET2, P_FP_MU_ELE, P_FP_SC22,
        P_FP_SIGMA_ELE, P_COUNT };
 
-// One block per tile; thread k owns instance k of the tile list and accumulates the
-// per-pixel adjoint of its footprint over the pixels of the tile inside the footprint's
-// bounding box (reference src/shader/us_focus.cu:398-477, 805-966).
-__global__ void __launch_bounds__(256)
-backward_tile_kernel(int H, int W, int tile, int tiles_x, float k_sigma, const float* __restrict__ means,
-                     const float* __restrict__ scales, const float* __restrict__ quats,
-                     const float* __restrict__ opac, const float* __restrict__ inten,
-                     const float* __restrict__ pose, const float* __restrict__ grid,
-                     const float* __restrict__ params, const int* __restrict__ tile_start,
-                     const int* __restrict__ sorted_gid, const int* __restrict__ sorted_inst,
-                     const long long* __restrict__ header, const float* __restrict__ grad_image,
-                     float* __restrict__ partial) {
+// One warp per instance of the sorted instance list (tile by tile): the lanes share the
+// pixels of the footprint's bounding box within the instance's tile and accumulate the
+// per-pixel adjoint of the footprint (reference src/shader/us_focus.cu:398-477, 805-966); the
+// 19 sums are then reduced over the warp in a fixed order. The footprints are the forward's
+// (cached per Gaussian by the preprocess).
+constexpr int BWD_WARPS = 8;  // warps per CTA
+
+__global__ void __launch_bounds__(BWD_WARPS * 32)
+backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restrict__ opac,
+                     const float* __restrict__ inten, const float4* __restrict__ bfp,
+                     const float* __restrict__ grid, const float* __restrict__ params,
+                     const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
+                     const int* __restrict__ sorted_inst, const long long* __restrict__ header,
+                     const float* __restrict__ grad_image, float* __restrict__ partial, int H) {
     if (header[H_FLAGS] != 0) return;
-    const int t = blockIdx.x;
-    const int s0 = tile_start[t], n = tile_start[t + 1] - s0;
-    if (n <= 0) return;
-    const int tx = t % tiles_x, ty = t / tiles_x;
-    const Axes A = axes_from_pose(pose);
+    const int lane = threadIdx.x & 31;
+    const int64_t total = tile_start[T];
     const float det_eps = params[UF_DET_EPS];
     const float det_gamma = params[UF_DET_GAMMA];
     const float weight_min = params[UF_WEIGHT_MIN];
     const float lat_delta = grid[SG_DELTA_LAT_MM], ax_delta = grid[SG_DELTA_AX_MM];
     const float col_off = grid[SG_LAT_COL_OFFSET], near_mm = grid[SG_NEAR_MM];
-    const int x0 = max(0, tx * tile), y0 = max(0, ty * tile);
-    const int x1 = min(W, (tx + 1) * tile), y1 = min(H, (ty + 1) * tile);
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int g = sorted_gid[s0 + k];
+    for (int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < total;
+         k += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        // the instance's tile: the last t with tile_start[t] <= k (empty tiles share a start)
+        int lo = 0, hi = T;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (tile_start[mid] <= k) lo = mid; else hi = mid;
+        }
+        const int t = lo;
+        const int tx = t % tiles_x, ty = t / tiles_x;
+        const int x0 = tx * tile, y0 = ty * tile;
+        const int x1 = min(W, (tx + 1) * tile), y1 = min(H, (ty + 1) * tile);
+        const int g = sorted_gid[k];
+        const float4 f0 = bfp[4 * (int64_t)g], f1 = bfp[4 * (int64_t)g + 1];
+        const float4 f2 = bfp[4 * (int64_t)g + 2], f3 = bfp[4 * (int64_t)g + 3];
+        const float mu2_lat = f0.x, mu2_ax = f0.y, r_lat = f0.z, r_ax = f0.w;
+        const float inv00 = f1.x, inv01 = f1.y, inv11 = f1.z, det2 = f1.w;
+        const float s2_00 = f2.x, s2_01 = f2.y, s2_11 = f2.z, sc22 = f2.w;
+        const float sigma_ele = f3.x, mu_ele = f3.y, mu_ax = f3.z;
         float acc[P_COUNT];
 #pragma unroll
         for (int i = 0; i < P_COUNT; ++i) acc[i] = 0.f;
-        const float* m = means + 3 * (int64_t)g;
-        const float* s = scales + 3 * (int64_t)g;
-        const float* q = quats + 4 * (int64_t)g;
-        Footprint F;
-        if (footprint(m[0], m[1], m[2], s[0], s[1], s[2], q[0], q[1], q[2], q[3], A, near_mm, k_sigma, params, F)) {
-            const int cx0 = max(x0, (int)ceilf((F.mu2_lat - F.r_lat) / lat_delta + col_off));
-            const int cx1 = min(x1, (int)floorf((F.mu2_lat + F.r_lat) / lat_delta + col_off) + 1);
-            const int cy0 = max(y0, (int)ceilf((F.mu2_ax - F.r_ax - near_mm) / ax_delta));
-            const int cy1 = min(y1, (int)floorf((F.mu2_ax + F.r_ax - near_mm) / ax_delta) + 1);
+        if (f3.w != 0.f) {
+            const int cx0 = max(x0, (int)ceilf((mu2_lat - r_lat) / lat_delta + col_off));
+            const int cx1 = min(x1, (int)floorf((mu2_lat + r_lat) / lat_delta + col_off) + 1);
+            const int cy0 = max(y0, (int)ceilf((mu2_ax - r_ax - near_mm) / ax_delta));
+            const int cy1 = min(y1, (int)floorf((mu2_ax + r_ax - near_mm) / ax_delta) + 1);
+            const int bw = cx1 - cx0, npx = bw > 0 && cy1 > cy0 ? bw * (cy1 - cy0) : 0;
             const float o = opac[g], c = inten[g];
-            const float denom_ele = fmaxf(F.sc22 + F.sigma_ele * F.sigma_ele + det_eps, 1e-12f);
-            const float slice_response = expf(-0.5f * F.mu_ele * F.mu_ele / denom_ele);
-            const float norm = det_norm_factor(F.det2 + det_eps, det_gamma);
-            const float depth = fmaxf(F.mu_ax - near_mm, 0.f);
+            const float denom_ele = fmaxf(sc22 + sigma_ele * sigma_ele + det_eps, 1e-12f);
+            const float slice_response = expf(-0.5f * mu_ele * mu_ele / denom_ele);
+            const float norm = det_norm_factor(det2 + det_eps, det_gamma);
+            const float depth = fmaxf(mu_ax - near_mm, 0.f);
             const float se_raw = params[UF_SIGMA_ELE_0] + params[UF_SIGMA_ELE_1] * depth;
-            const float dse_dax = (F.mu_ax > near_mm && se_raw > params[UF_SIGMA_ELE_MIN] &&
+            const float dse_dax = (mu_ax > near_mm && se_raw > params[UF_SIGMA_ELE_MIN] &&
                                    se_raw < params[UF_SIGMA_ELE_MAX]) ? params[UF_SIGMA_ELE_1] : 0.f;
-            const float inv_det_norm = 1.f / fmaxf(F.det2 + det_eps, 1e-12f);
+            const float inv_det_norm = 1.f / fmaxf(det2 + det_eps, 1e-12f);
             const float inv_de = 1.f / denom_ele;
             const float bno_const = slice_response * norm;
-            for (int y = cy0; y < cy1; ++y) {
-                const float xi_ax = static_cast<float>(y) * ax_delta + near_mm;
-                for (int x = cx0; x < cx1; ++x) {
-                    const float xi_lat = (static_cast<float>(x) - col_off) * lat_delta;
-                    if (fabsf(xi_lat - F.mu2_lat) > F.r_lat || fabsf(xi_ax - F.mu2_ax) > F.r_ax) continue;
-                    const float dlat = xi_lat - F.mu2_lat;
-                    const float dax = xi_ax - F.mu2_ax;
-                    const float qlat = F.inv00 * dlat + F.inv01 * dax;
-                    const float qax = F.inv01 * dlat + F.inv11 * dax;
-                    const float quad = dlat * qlat + dax * qax;
-                    if (!(quad >= 0.f) || !isfinite(quad)) continue;
-                    const float phi = expf(-0.5f * quad);
-                    const float bno = bno_const * phi;
-                    const float weight = o * bno;
-                    if (!isfinite(weight) || weight < weight_min) continue;
-                    const float up = grad_image[y * W + x];
-                    const float gw = up * c;
-                    acc[P_INTENSITY] += up * weight;
-                    acc[P_OPACITY] += gw * bno;
-                    const float cm = gw * weight;
-                    acc[P_MU_E0] += cm * qlat;
-                    acc[P_MU_E1] += cm * qax;
-                    acc[P_FP_MU2_LAT] += cm * qlat;
-                    acc[P_FP_MU2_AX] += cm * qax;
-                    acc[P_FP_INV00] += cm * (-0.5f * dlat * dlat);
-                    acc[P_FP_INV01] += cm * (-dlat * dax);
-                    acc[P_FP_INV11] += cm * (-0.5f * dax * dax);
-                    acc[P_FP_DET2] += cm * (-det_gamma * inv_det_norm);
-                    acc[P_SE00] += cm * (0.5f * qlat * qlat - det_gamma * F.s2_11 * inv_det_norm);
-                    acc[P_SE01] += 0.5f * (cm * (qlat * qax + 2.f * det_gamma * F.s2_01 * inv_det_norm));
-                    acc[P_SE11] += cm * (0.5f * qax * qax - det_gamma * F.s2_00 * inv_det_norm);
-                    acc[P_MU_PROBE2] += cm * (-F.mu_ele * inv_de);
-                    acc[P_SC22] += cm * (0.5f * F.mu_ele * F.mu_ele * inv_de * inv_de);
-                    acc[P_MU_PROBE1] += cm * (F.mu_ele * F.mu_ele * dse_dax * inv_de * inv_de);
-                    acc[P_FP_MU_ELE] += cm * (-F.mu_ele * inv_de);
-                    acc[P_FP_SC22] += cm * (0.5f * F.mu_ele * F.mu_ele * inv_de * inv_de);
-                    acc[P_FP_SIGMA_ELE] += cm * (F.mu_ele * F.mu_ele * F.sigma_ele * inv_de * inv_de);
+            // pixel pi = lane + 32 i of the box, row-major: (row, column) stepped without divisions
+            int ry = bw > 0 ? lane / bw : 0, rx = lane - ry * bw;
+            const int step_y = bw > 0 ? 32 / bw : 0, step_x = 32 - step_y * bw;
+            for (int pi = lane; pi < npx; pi += 32) {
+                const int x = cx0 + rx, y = cy0 + ry;
+                rx += step_x;
+                ry += step_y;
+                if (rx >= bw) {
+                    rx -= bw;
+                    ++ry;
                 }
+                const float xi_ax = static_cast<float>(y) * ax_delta + near_mm;
+                const float xi_lat = (static_cast<float>(x) - col_off) * lat_delta;
+                if (fabsf(xi_lat - mu2_lat) > r_lat || fabsf(xi_ax - mu2_ax) > r_ax) continue;
+                const float dlat = xi_lat - mu2_lat;
+                const float dax = xi_ax - mu2_ax;
+                const float qlat = inv00 * dlat + inv01 * dax;
+                const float qax = inv01 * dlat + inv11 * dax;
+                const float quad = dlat * qlat + dax * qax;
+                if (!(quad >= 0.f) || !isfinite(quad)) continue;
+                const float phi = expf(-0.5f * quad);
+                const float bno = bno_const * phi;
+                const float weight = o * bno;
+                if (!isfinite(weight) || weight < weight_min) continue;
+                const float up = grad_image[y * W + x];
+                const float gw = up * c;
+                acc[P_INTENSITY] += up * weight;
+                acc[P_OPACITY] += gw * bno;
+                const float cm = gw * weight;
+                acc[P_MU_E0] += cm * qlat;
+                acc[P_MU_E1] += cm * qax;
+                acc[P_FP_MU2_LAT] += cm * qlat;
+                acc[P_FP_MU2_AX] += cm * qax;
+                acc[P_FP_INV00] += cm * (-0.5f * dlat * dlat);
+                acc[P_FP_INV01] += cm * (-dlat * dax);
+                acc[P_FP_INV11] += cm * (-0.5f * dax * dax);
+                acc[P_FP_DET2] += cm * (-det_gamma * inv_det_norm);
+                acc[P_SE00] += cm * (0.5f * qlat * qlat - det_gamma * s2_11 * inv_det_norm);
+                acc[P_SE01] += 0.5f * (cm * (qlat * qax + 2.f * det_gamma * s2_01 * inv_det_norm));
+                acc[P_SE11] += cm * (0.5f * qax * qax - det_gamma * s2_00 * inv_det_norm);
+                acc[P_MU_PROBE2] += cm * (-mu_ele * inv_de);
+                acc[P_SC22] += cm * (0.5f * mu_ele * mu_ele * inv_de * inv_de);
+                acc[P_MU_PROBE1] += cm * (mu_ele * mu_ele * dse_dax * inv_de * inv_de);
+                acc[P_FP_MU_ELE] += cm * (-mu_ele * inv_de);
+                acc[P_FP_SC22] += cm * (0.5f * mu_ele * mu_ele * inv_de * inv_de);
+                acc[P_FP_SIGMA_ELE] += cm * (mu_ele * mu_ele * sigma_ele * inv_de * inv_de);
             }
         }
-        float4* out = reinterpret_cast<float4*>(partial) + (int64_t)PARTIAL_F4 * sorted_inst[s0 + k];
-        out[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
-        out[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
-        out[2] = make_float4(acc[8], acc[9], acc[10], acc[11]);
-        out[3] = make_float4(acc[12], acc[13], acc[14], acc[15]);
-        out[4] = make_float4(acc[16], acc[17], acc[18], 0.f);
+        // butterfly reduction: every lane ends with the same sums
+#pragma unroll
+        for (int i = 0; i < P_COUNT; ++i) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+        }
+        float4* out = reinterpret_cast<float4*>(partial) + (int64_t)PARTIAL_F4 * sorted_inst[k];
+        if (lane == 0) {
+            out[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+            out[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
+            out[2] = make_float4(acc[8], acc[9], acc[10], acc[11]);
+            out[3] = make_float4(acc[12], acc[13], acc[14], acc[15]);
+            out[4] = make_float4(acc[16], acc[17], acc[18], 0.f);
+        }
     }
 }
 
@@ -853,7 +920,7 @@ extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t 
         preprocess_kernel<<<gb, 256, 0, stream>>>(n_gauss, H, W, tile_size, tx, ty, lateral_spacing, axial_spacing,
                                                   axial_near, k_sigma, sort_by_v, means, scales, quats, opacities,
                                                   intensities, pose, grid_pack, focus_params, w.rects, w.dkey,
-                                                  w.touched, w.tile_count, w.cand);
+                                                  w.touched, w.tile_count, w.cand, w.bfp);
     US3D_CHECK_LAUNCH("gp preprocess");
     US3D_CHECK_CUDA(launch_rect_count(n_gauss, tx, T, RectOf4{w.rects}, w.tile_count, stream));
     US3D_CHECK_CUDA(exclusive_scan(w.touched, n_gauss, w.inst_offset, w.bs_g, w.header + H_SCAN_G, stream));
@@ -863,9 +930,18 @@ extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t 
                                         w.tile_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_gp_sort_attr, stream));
-    forward_kernel<<<(unsigned)T, (tile_size * tile_size + 31) / 32 * 32, 0, stream>>>(H, W, tile_size, tx, grid_pack, focus_params,
-                                                                     w.tile_start, w.sorted_gid, w.header, w.cand,
-                                                                     out_image);
+    // up to four threads per pixel (a whole-warp pixel block of at most 1024 threads)
+    const int npix = (tile_size * tile_size + 31) / 32 * 32;
+    auto launch = [&](auto kernel, int parts) {
+        kernel<<<(unsigned)T, npix * parts, 0, stream>>>(H, W, tile_size, tx, grid_pack, focus_params, w.tile_start,
+                                                        w.sorted_gid, w.header, w.cand, out_image);
+    };
+    if (npix <= 256)
+        launch(forward_kernel<4>, 4);
+    else if (npix <= 512)
+        launch(forward_kernel<2>, 2);
+    else
+        launch(forward_kernel<1>, 1);
     US3D_CHECK_LAUNCH("gp forward");
     prof_end(prof, stream);
     count_launches(1 + (n_gauss > 0) * 3 + 6 + 1 + TILE_SORT_LAUNCHES + 1);
@@ -907,11 +983,14 @@ extern "C" int us3d_gp_backward(void* workspace, int64_t n_gauss, const float* m
     pose_partial = reinterpret_cast<float*>(align_up(reinterpret_cast<uintptr_t>(pose_partial), 256));
     cudaStream_t stream = (cudaStream_t)stream_;
     const int prof = prof_begin("gp_backward", stream);
-    backward_tile_kernel<<<(unsigned)T, 256, 0, stream>>>(H, W, tile_size, tx, k_sigma, means, scales, quats, opacities,
-                                                          intensities, pose, grid_pack, focus_params, w.tile_start,
-                                                          w.sorted_gid, w.sorted_inst, w.header, grad_image, partial);
-    US3D_CHECK_LAUNCH("gp backward tiles");
-    int launches = 1;
+    int launches = 0;
+    if (T > 0) {
+        backward_inst_kernel<<<148 * 8, BWD_WARPS * 32, 0, stream>>>(
+            (int)T, W, tile_size, tx, opacities, intensities, w.bfp, grid_pack, focus_params, w.tile_start,
+            w.sorted_gid, w.sorted_inst, w.header, grad_image, partial, H);
+        US3D_CHECK_LAUNCH("gp backward instances");
+        launches = 1;
+    }
     if (n_gauss > 0) {
         finalize_kernel<<<(unsigned)((n_gauss + 127) / 128), 128, 0, stream>>>(
             n_gauss, k_sigma, w.inst_offset, w.rects, means, scales, quats, pose, grid_pack, focus_params, w.header,
