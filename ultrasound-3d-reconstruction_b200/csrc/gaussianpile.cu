@@ -55,8 +55,9 @@ struct Workspace {
     int* tile_cursor;   // T
     long long* bs_t;
     float4* cand;       // G x 3: (base_weight, intensity, mu2_lat, mu2_ax) (inv00, inv01, inv11, r_lat) (r_ax, valid)
-    float4* bfp;        // G x 4: the forward's footprint for the backward: (mu2_lat, mu2_ax, r_lat, r_ax)
-                        // (inv00, inv01, inv11, det2) (s2_00, s2_01, s2_11, sc22) (sigma_ele, mu_ele, mu_ax, valid)
+    float4* bfp;        // G x 4, what the backward needs of the forward's footprint:
+                        // (mu2_lat, mu2_ax, r_lat (< 0: no footprint), r_ax) (inv00, inv01, inv11, bno_const)
+                        // (s2_00, s2_01, s2_11, 1 / det_norm) (mu_ele, 1 / denom_ele, dsigma_ele/dax, sigma_ele)
     unsigned long long* keys;
     int* slot_inst;
     int* sorted_gid;
@@ -333,10 +334,23 @@ preprocess_kernel(int64_t G, int H, int W, int tile, int tiles_x, int tiles_y, f
     cand[3 * g + 0] = make_float4(bw, inten[g], Ff.mu2_lat, Ff.mu2_ax);
     cand[3 * g + 1] = make_float4(Ff.inv00, Ff.inv01, Ff.inv11, Ff.r_lat);
     cand[3 * g + 2] = make_float4(Ff.r_ax, valid ? 1.f : 0.f, 0.f, 0.f);
-    bfp[4 * g + 0] = make_float4(Ff.mu2_lat, Ff.mu2_ax, Ff.r_lat, Ff.r_ax);
-    bfp[4 * g + 1] = make_float4(Ff.inv00, Ff.inv01, Ff.inv11, Ff.det2);
-    bfp[4 * g + 2] = make_float4(Ff.s2_00, Ff.s2_01, Ff.s2_11, Ff.sc22);
-    bfp[4 * g + 3] = make_float4(Ff.sigma_ele, Ff.mu_ele, Ff.mu_ax, okf ? 1.f : 0.f);
+    // The backward's per-Gaussian factors (reference us_focus.cu:398-477), with the grid's near
+    // plane as the backward uses it.
+    {
+        const float det_eps = params[UF_DET_EPS], det_gamma = params[UF_DET_GAMMA];
+        const float near_b = grid[SG_NEAR_MM];
+        const float denom_ele = fmaxf(Ff.sc22 + Ff.sigma_ele * Ff.sigma_ele + det_eps, 1e-12f);
+        const float slice_response = expf(-0.5f * Ff.mu_ele * Ff.mu_ele / denom_ele);
+        const float norm = det_norm_factor(Ff.det2 + det_eps, det_gamma);
+        const float depth = fmaxf(Ff.mu_ax - near_b, 0.f);
+        const float se_raw = params[UF_SIGMA_ELE_0] + params[UF_SIGMA_ELE_1] * depth;
+        const float dse_dax = (Ff.mu_ax > near_b && se_raw > params[UF_SIGMA_ELE_MIN] &&
+                               se_raw < params[UF_SIGMA_ELE_MAX]) ? params[UF_SIGMA_ELE_1] : 0.f;
+        bfp[4 * g + 0] = make_float4(Ff.mu2_lat, Ff.mu2_ax, okf ? Ff.r_lat : -1.f, Ff.r_ax);
+        bfp[4 * g + 1] = make_float4(Ff.inv00, Ff.inv01, Ff.inv11, slice_response * norm);
+        bfp[4 * g + 2] = make_float4(Ff.s2_00, Ff.s2_01, Ff.s2_11, 1.f / fmaxf(Ff.det2 + det_eps, 1e-12f));
+        bfp[4 * g + 3] = make_float4(Ff.mu_ele, 1.f / denom_ele, dse_dax, Ff.sigma_ele);
+    }
 }
 
 __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
@@ -484,7 +498,7 @@ enum { P_MU_PROBE1 = 0, P_MU_PROBE2, P_SC22, P_MU_E0, P_MU_E1, P_SE00, P_SE01, P
 // (cached per Gaussian by the preprocess).
 constexpr int BWD_WARPS = 8;  // warps per CTA
 
-__global__ void __launch_bounds__(BWD_WARPS * 32)
+__global__ void __launch_bounds__(BWD_WARPS * 32, 4)
 backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restrict__ opac,
                      const float* __restrict__ inten, const float4* __restrict__ bfp,
                      const float* __restrict__ grid, const float* __restrict__ params,
@@ -494,7 +508,6 @@ backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restric
     if (header[H_FLAGS] != 0) return;
     const int lane = threadIdx.x & 31;
     const int64_t total = tile_start[T];
-    const float det_eps = params[UF_DET_EPS];
     const float det_gamma = params[UF_DET_GAMMA];
     const float weight_min = params[UF_WEIGHT_MIN];
     const float lat_delta = grid[SG_DELTA_LAT_MM], ax_delta = grid[SG_DELTA_AX_MM];
@@ -515,29 +528,22 @@ backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restric
         const float4 f0 = bfp[4 * (int64_t)g], f1 = bfp[4 * (int64_t)g + 1];
         const float4 f2 = bfp[4 * (int64_t)g + 2], f3 = bfp[4 * (int64_t)g + 3];
         const float mu2_lat = f0.x, mu2_ax = f0.y, r_lat = f0.z, r_ax = f0.w;
-        const float inv00 = f1.x, inv01 = f1.y, inv11 = f1.z, det2 = f1.w;
-        const float s2_00 = f2.x, s2_01 = f2.y, s2_11 = f2.z, sc22 = f2.w;
-        const float sigma_ele = f3.x, mu_ele = f3.y, mu_ax = f3.z;
-        float acc[P_COUNT];
-#pragma unroll
-        for (int i = 0; i < P_COUNT; ++i) acc[i] = 0.f;
-        if (f3.w != 0.f) {
+        const float inv00 = f1.x, inv01 = f1.y, inv11 = f1.z, bno_const = f1.w;
+        const float s2_00 = f2.x, s2_01 = f2.y, s2_11 = f2.z, inv_det_norm = f2.w;
+        const float mu_ele = f3.x, inv_de = f3.y, dse_dax = f3.z, sigma_ele = f3.w;
+        // Every term of the per-instance partial is a fixed combination of six sums over the
+        // contributing pixels of up * bno (bno = the weight without the opacity) times 1, dlat,
+        // dax, dlat^2, dlat dax, dax^2: the lanes accumulate those and the terms are formed once.
+        float m0 = 0.f, mx = 0.f, my = 0.f, mxx = 0.f, mxy = 0.f, myy = 0.f;
+        float o = 0.f, c = 0.f;
+        if (r_lat >= 0.f) {
             const int cx0 = max(x0, (int)ceilf((mu2_lat - r_lat) / lat_delta + col_off));
             const int cx1 = min(x1, (int)floorf((mu2_lat + r_lat) / lat_delta + col_off) + 1);
             const int cy0 = max(y0, (int)ceilf((mu2_ax - r_ax - near_mm) / ax_delta));
             const int cy1 = min(y1, (int)floorf((mu2_ax + r_ax - near_mm) / ax_delta) + 1);
             const int bw = cx1 - cx0, npx = bw > 0 && cy1 > cy0 ? bw * (cy1 - cy0) : 0;
-            const float o = opac[g], c = inten[g];
-            const float denom_ele = fmaxf(sc22 + sigma_ele * sigma_ele + det_eps, 1e-12f);
-            const float slice_response = expf(-0.5f * mu_ele * mu_ele / denom_ele);
-            const float norm = det_norm_factor(det2 + det_eps, det_gamma);
-            const float depth = fmaxf(mu_ax - near_mm, 0.f);
-            const float se_raw = params[UF_SIGMA_ELE_0] + params[UF_SIGMA_ELE_1] * depth;
-            const float dse_dax = (mu_ax > near_mm && se_raw > params[UF_SIGMA_ELE_MIN] &&
-                                   se_raw < params[UF_SIGMA_ELE_MAX]) ? params[UF_SIGMA_ELE_1] : 0.f;
-            const float inv_det_norm = 1.f / fmaxf(det2 + det_eps, 1e-12f);
-            const float inv_de = 1.f / denom_ele;
-            const float bno_const = slice_response * norm;
+            o = opac[g];
+            c = inten[g];
             // pixel pi = lane + 32 i of the box, row-major: (row, column) stepped without divisions
             int ry = bw > 0 ? lane / bw : 0, rx = lane - ry * bw;
             const int step_y = bw > 0 ? 32 / bw : 0, step_x = 32 - step_y * bw;
@@ -562,35 +568,55 @@ backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restric
                 const float bno = bno_const * phi;
                 const float weight = o * bno;
                 if (!isfinite(weight) || weight < weight_min) continue;
-                const float up = grad_image[y * W + x];
-                const float gw = up * c;
-                acc[P_INTENSITY] += up * weight;
-                acc[P_OPACITY] += gw * bno;
-                const float cm = gw * weight;
-                acc[P_MU_E0] += cm * qlat;
-                acc[P_MU_E1] += cm * qax;
-                acc[P_FP_MU2_LAT] += cm * qlat;
-                acc[P_FP_MU2_AX] += cm * qax;
-                acc[P_FP_INV00] += cm * (-0.5f * dlat * dlat);
-                acc[P_FP_INV01] += cm * (-dlat * dax);
-                acc[P_FP_INV11] += cm * (-0.5f * dax * dax);
-                acc[P_FP_DET2] += cm * (-det_gamma * inv_det_norm);
-                acc[P_SE00] += cm * (0.5f * qlat * qlat - det_gamma * s2_11 * inv_det_norm);
-                acc[P_SE01] += 0.5f * (cm * (qlat * qax + 2.f * det_gamma * s2_01 * inv_det_norm));
-                acc[P_SE11] += cm * (0.5f * qax * qax - det_gamma * s2_00 * inv_det_norm);
-                acc[P_MU_PROBE2] += cm * (-mu_ele * inv_de);
-                acc[P_SC22] += cm * (0.5f * mu_ele * mu_ele * inv_de * inv_de);
-                acc[P_MU_PROBE1] += cm * (mu_ele * mu_ele * dse_dax * inv_de * inv_de);
-                acc[P_FP_MU_ELE] += cm * (-mu_ele * inv_de);
-                acc[P_FP_SC22] += cm * (0.5f * mu_ele * mu_ele * inv_de * inv_de);
-                acc[P_FP_SIGMA_ELE] += cm * (mu_ele * mu_ele * sigma_ele * inv_de * inv_de);
+                const float ub = grad_image[y * W + x] * bno;
+                const float ux = ub * dlat, uy = ub * dax;
+                m0 += ub;
+                mx += ux;
+                my += uy;
+                mxx += ux * dlat;
+                mxy += ux * dax;
+                myy += uy * dax;
             }
         }
         // butterfly reduction: every lane ends with the same sums
 #pragma unroll
-        for (int i = 0; i < P_COUNT; ++i) {
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+        for (int off = 16; off > 0; off >>= 1) {
+            m0 += __shfl_xor_sync(0xffffffffu, m0, off);
+            mx += __shfl_xor_sync(0xffffffffu, mx, off);
+            my += __shfl_xor_sync(0xffffffffu, my, off);
+            mxx += __shfl_xor_sync(0xffffffffu, mxx, off);
+            mxy += __shfl_xor_sync(0xffffffffu, mxy, off);
+            myy += __shfl_xor_sync(0xffffffffu, myy, off);
+        }
+        // The terms of reference us_focus.cu:398-477 (per pixel: up * weight, up c bno and
+        // cm = up c weight times the footprint derivatives) from the six moments.
+        float acc[P_COUNT];
+        {
+            const float co = c * o;  // cm = co * up * bno
+            const float ql = inv00 * mx + inv01 * my, qa = inv01 * mx + inv11 * my;  // sum ub q
+            const float qll = inv00 * inv00 * mxx + 2.f * inv00 * inv01 * mxy + inv01 * inv01 * myy;
+            const float qla = inv00 * inv01 * mxx + (inv00 * inv11 + inv01 * inv01) * mxy + inv01 * inv11 * myy;
+            const float qaa = inv01 * inv01 * mxx + 2.f * inv01 * inv11 * mxy + inv11 * inv11 * myy;
+            const float ele2 = mu_ele * mu_ele * inv_de * inv_de;
+            acc[P_INTENSITY] = o * m0;
+            acc[P_OPACITY] = c * m0;
+            acc[P_MU_E0] = co * ql;
+            acc[P_MU_E1] = co * qa;
+            acc[P_FP_MU2_LAT] = co * ql;
+            acc[P_FP_MU2_AX] = co * qa;
+            acc[P_FP_INV00] = co * (-0.5f * mxx);
+            acc[P_FP_INV01] = co * (-mxy);
+            acc[P_FP_INV11] = co * (-0.5f * myy);
+            acc[P_FP_DET2] = co * m0 * (-det_gamma * inv_det_norm);
+            acc[P_SE00] = co * (0.5f * qll - det_gamma * s2_11 * inv_det_norm * m0);
+            acc[P_SE01] = 0.5f * co * (qla + 2.f * det_gamma * s2_01 * inv_det_norm * m0);
+            acc[P_SE11] = co * (0.5f * qaa - det_gamma * s2_00 * inv_det_norm * m0);
+            acc[P_MU_PROBE2] = co * m0 * (-mu_ele * inv_de);
+            acc[P_SC22] = co * m0 * (0.5f * ele2);
+            acc[P_MU_PROBE1] = co * m0 * (ele2 * dse_dax);
+            acc[P_FP_MU_ELE] = co * m0 * (-mu_ele * inv_de);
+            acc[P_FP_SC22] = co * m0 * (0.5f * ele2);
+            acc[P_FP_SIGMA_ELE] = co * m0 * (ele2 * sigma_ele);
         }
         float4* out = reinterpret_cast<float4*>(partial) + (int64_t)PARTIAL_F4 * sorted_inst[k];
         if (lane == 0) {
