@@ -363,35 +363,35 @@ tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long*
 }
 
 // Second pass: buckets of SORT_SMEM_CAP < n <= SORT_BIG_CAP keys with 192 KB of shared
-// memory. Block b owns a contiguous range of tiles; it inspects them SORT_THREADS at a time
-// and orders the large ones it finds, one after another.
-constexpr int SORT_BIG_GRID = 148;  // one 192 KB block per SM
+// memory. Block b owns the tiles b, b + grid, b + 2 grid, ... (large buckets tend to be
+// neighbours, so they spread over the blocks); it inspects them SORT_BIG_THREADS at a time and
+// orders the large ones it finds, one after another.
+constexpr int SORT_BIG_GRID = 148;      // one 192 KB block per SM
+constexpr int SORT_BIG_THREADS = 1024;  // the whole SM's threads on one large bucket
 
-static __global__ void __launch_bounds__(SORT_THREADS)
+static __global__ void __launch_bounds__(SORT_BIG_THREADS)
 tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
                      unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
                      int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
                      const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask) {
     extern __shared__ __align__(16) unsigned long long s_big_keys[];
     int* s_big_idx = reinterpret_cast<int*>(s_big_keys + SORT_BIG_CAP);
-    __shared__ int s_list[SORT_THREADS];
+    __shared__ int s_list[SORT_BIG_THREADS];
     __shared__ int s_n;
     if (header[H_FLAGS] != 0) return;
-    const int64_t per = (T + gridDim.x - 1) / gridDim.x;
-    const int64_t t0 = (int64_t)blockIdx.x * per;
-    const int64_t t1 = t0 + per < T ? t0 + per : T;
-    for (int64_t c0 = t0; c0 < t1; c0 += SORT_THREADS) {
+    const int64_t stride = gridDim.x;
+    for (int64_t c0 = 0; c0 < T; c0 += stride * SORT_BIG_THREADS) {
         if (threadIdx.x == 0) s_n = 0;
         __syncthreads();
-        const int64_t t = c0 + threadIdx.x;
-        if (t < t1) {
+        const int64_t t = c0 + blockIdx.x + stride * threadIdx.x;
+        if (t < T) {
             const int n = tile_start[t + 1] - tile_start[t];
             if (n > SORT_SMEM_CAP && n <= SORT_BIG_CAP) s_list[atomicAdd(&s_n, 1)] = threadIdx.x;
         }
         __syncthreads();
         const int count = s_n;
         for (int k = 0; k < count; ++k) {
-            const int64_t tt = c0 + s_list[k];
+            const int64_t tt = c0 + blockIdx.x + stride * s_list[k];
             const int s0 = tile_start[tt];
             const int n = tile_start[tt + 1] - s0;
             sort_bucket_smem(s_big_keys, s_big_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask,
@@ -427,7 +427,7 @@ static inline cudaError_t launch_tile_sort(int64_t T, const int* tile_start, con
         if (dev >= 0 && dev < 128) attr_done[dev] = true;
     }
     const unsigned grid = (unsigned)(T < SORT_BIG_GRID ? T : SORT_BIG_GRID);
-    tile_sort_big_kernel<<<grid, SORT_THREADS, tile_sort_big_smem_bytes(), stream>>>(
+    tile_sort_big_kernel<<<grid, SORT_BIG_THREADS, tile_sort_big_smem_bytes(), stream>>>(
         T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
     return cudaGetLastError();
 }
