@@ -41,8 +41,8 @@ BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (param
 # dram__bytes_read.sum + dram__bytes_write.sum of one 4-frame launch of the headline scene
 # (ncu --set full), per frame; the backward stage is backward_kernel + reduce_kernel.
 NCU_TRAFFIC_PER_FRAME = {
-    "ug_backward": (101.160192e6 + 115.272448e6 + 156.033024e6 + 28.610560e6) / 4,
-    "ug_forward": (52.276224e6 + 5.576192e6) / 4,
+    "ug_backward": (101.241856e6 + 116.555008e6 + 156.020480e6 + 26.502656e6) / 4,
+    "ug_forward": (52.280320e6 + 5.839104e6) / 4,
 }
 
 
