@@ -287,6 +287,22 @@ US3D_API int us3d_frames_gather(const us3d_slice_frame* all_frames, int64_t n_al
                                 float* out_pixel_positions, float* out_targets, int32_t* status, void* stream);
 
 /*
+ * Scanline and pose geometry of a batch of dataset frames, replacing the per-frame host work
+ * of NpzUltrasoundDataset._ray_origins / _ray_dirs / _pose_world_to_probe
+ * (pipeline_god_file.py:308-336). For each of the n_batch dataset indices: `width` ray origins
+ * origin + ((u - lateral_col_offset) * lateral_spacing) * axis_lat, u = 0..width-1 (or
+ * all_ray_origins[k], (n_all, width, 3)), `width` ray directions axis_ax (or
+ * all_ray_dirs[k]), and the row-major 4x4 world-to-probe pose [R | -R origin] with R's rows
+ * axis_lat, axis_ax, axis_ele (or all_poses[k], (n_all, 16)). The stored arrays may be NULL.
+ * Outputs: out_ray_origins / out_ray_dirs (n_batch, width, 3), out_pose (n_batch, 16). An
+ * index outside [0, n_all) sets *status bit 0 and takes frame 0. Never synchronises.
+ */
+US3D_API int us3d_frames_geometry(const us3d_slice_frame* all_frames, int64_t n_all, const int64_t* indices,
+                                  int32_t n_batch, int32_t width, const float* all_ray_origins,
+                                  const float* all_ray_dirs, const float* all_poses, float* out_ray_origins,
+                                  float* out_ray_dirs, float* out_pose, int32_t* status, void* stream);
+
+/*
  * Densification statistics of a training step (the refinement the UltraG-Ray paper
  * describes, absent from the reference's code): for each of the n_gauss Gaussians,
  * importance[g] += |dL/dmean_g| (Euclidean norm of its row of grad_means, (G,3)) and

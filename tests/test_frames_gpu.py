@@ -124,3 +124,65 @@ def test_trainer_on_device_batches(cuda_device):
     for a, b in zip(*out):
         assert np.array_equal(a, b)
     assert not np.array_equal(out[0][0], sc.means.numpy())
+
+
+def _ref_rays_and_pose(w, origin, lat, ax, ele, dlat, center_lateral, device):
+    """The reference's generated scanlines and world-to-probe pose (pipeline_god_file.py:308-336),
+    restated with the same PyTorch operations."""
+    u = torch.arange(w, device=device, dtype=torch.float32)
+    center = (w - 1) * 0.5 if center_lateral else 0.0
+    lateral_mm = (u - center) * float(dlat)
+    origins = origin.view(1, 3) + lateral_mm[:, None] * lat.view(1, 3)
+    dirs = ax.view(1, 3).expand(w, 3).contiguous()
+    r = torch.stack([lat, ax, ele], dim=0)
+    t = -r.matmul(origin)
+    pose = torch.eye(4, device=device, dtype=torch.float32)
+    pose[:3, :3] = r
+    pose[:3, 3] = t
+    return origins, dirs, pose
+
+
+@pytest.mark.parametrize("center", [True, False])
+def test_generated_rays_and_poses_match_reference(center, cuda_device):
+    from us3d_b200.frames import DeviceFrameSource
+
+    dev = cuda_device
+    images, g = _dataset()
+    src = DeviceFrameSource(images, g["o"], g["l"], g["a"], g["e"], 0.3, 0.17, 0.0, center, device=dev)
+    idx = torch.tensor([3, 3, 0, 5, 1], dtype=torch.int64, device=dev)
+    origins, dirs, pose = src.geometry(idx)
+    src.check()
+    for f, k in enumerate(idx.tolist()):
+        o = torch.from_numpy(g["o"][k]).to(dev)
+        lat, ax, ele = (_ref_normalize(torch.from_numpy(g[c][k]).to(dev)) for c in ("l", "a", "e"))
+        ro, rd, rp = _ref_rays_and_pose(50, o, lat, ax, ele, 0.3, center, dev)
+        assert torch.equal(origins[f], ro), f
+        assert torch.equal(dirs[f], rd), f
+        assert torch.equal(pose[f, :3, :3], rp[:3, :3]) and torch.equal(pose[f, 3], rp[3]), f
+        # the translation is a 3-term dot product whose summation order the reference leaves to torch
+        torch.testing.assert_close(pose[f, :3, 3], rp[:3, 3], rtol=1e-6, atol=1e-5)
+
+
+def test_stored_rays_and_poses_and_bad_index(cuda_device, tmp_path):
+    from us3d_b200.frames import DeviceFrameSource
+
+    dev = cuda_device
+    images, g = _dataset(n=4, h=9, w=11)
+    rng = np.random.default_rng(3)
+    ro = rng.normal(size=(4, 11, 3)).astype(np.float32)
+    rd = rng.normal(size=(4, 11, 3)).astype(np.float32)
+    pose = rng.normal(size=(4, 4)).astype(np.float32)  # one pose shared by every frame
+    path = tmp_path / "frames.npz"
+    np.savez(path, images=images, probe_origin_world=g["o"], axis_lateral_world=g["l"], axis_axial_world=g["a"],
+             axis_elevational_world=g["e"], ray_origins=ro, ray_dirs=rd, pose_world_to_probe=pose)
+    src = DeviceFrameSource.from_npz(path, 0.3, 0.17, device=dev)
+    idx = torch.tensor([2, 0, 3], dtype=torch.int64, device=dev)
+    origins, dirs, poses = src.geometry(idx)
+    src.check()
+    for f, k in enumerate(idx.tolist()):
+        assert torch.equal(origins[f].cpu(), torch.from_numpy(ro[k]))
+        assert torch.equal(dirs[f].cpu(), torch.from_numpy(rd[k]))
+        assert torch.equal(poses[f].cpu(), torch.from_numpy(pose))
+    src.geometry(torch.tensor([1, 7], dtype=torch.int64, device=dev))
+    with pytest.raises(IndexError):
+        src.check()

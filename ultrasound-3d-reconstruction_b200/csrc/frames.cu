@@ -3,6 +3,8 @@
 // frame geometry exactly as the reference's dataset does) and their target images (with the
 // reference's 8-bit scaling). Replaces the per-frame host work of NpzUltrasoundDataset.get_frame
 // (pipeline_god_file.py:178-245, 292-306) for the batched training step.
+#include <algorithm>
+
 #include "us3d_common.cuh"
 
 namespace us3d {
@@ -69,6 +71,55 @@ gather_kernel(const us3d_slice_frame* __restrict__ all, int64_t n_all, const int
     out_targets[dst] = y;
 }
 
+// Scanline and pose geometry of a batch of frames (reference pipeline_god_file.py:308-336):
+// ray origin u = origin + ((u - centre) * delta_lateral) * lat, each operation rounded on its
+// own as PyTorch's separate kernels do; ray direction = the axial axis; world-to-probe pose
+// [R | -R origin] with R's rows the lateral, axial and elevational axes.
+__global__ void __launch_bounds__(THREADS)
+geometry_kernel(const us3d_slice_frame* __restrict__ all, int64_t n_all, const int64_t* __restrict__ indices, int W,
+                const float* __restrict__ all_origins, const float* __restrict__ all_dirs,
+                const float* __restrict__ all_poses, float* __restrict__ out_origins, float* __restrict__ out_dirs,
+                float* __restrict__ out_pose, int* __restrict__ status) {
+    const int f = blockIdx.y;
+    int64_t k = indices[f];
+    if (k < 0 || k >= n_all) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, 1);
+        k = 0;
+    }
+    const us3d_slice_frame fr = all[k];
+    const int u = blockIdx.x * THREADS + threadIdx.x;
+    if (u < W) {
+        const int64_t dst = 3 * ((int64_t)f * W + u);
+        const int64_t src = 3 * (k * W + u);
+        if (all_origins) {
+            out_origins[dst] = all_origins[src];
+            out_origins[dst + 1] = all_origins[src + 1];
+            out_origins[dst + 2] = all_origins[src + 2];
+        } else {
+            const float lat_mm = __fmul_rn(__fsub_rn((float)u, fr.lateral_col_offset), fr.lateral_spacing);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) out_origins[dst + c] = __fadd_rn(fr.origin[c], __fmul_rn(lat_mm, fr.axis_lat[c]));
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out_dirs[dst + c] = all_dirs ? all_dirs[src + c] : fr.axis_ax[c];
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 16) {
+        const int r = threadIdx.x / 4, c = threadIdx.x % 4;
+        float v;
+        if (all_poses) {
+            v = all_poses[16 * k + threadIdx.x];
+        } else if (r == 3) {
+            v = c == 3 ? 1.0f : 0.0f;
+        } else {
+            const float* row = r == 0 ? fr.axis_lat : (r == 1 ? fr.axis_ax : fr.axis_ele);
+            v = c < 3 ? row[c]
+                      : -__fadd_rn(__fadd_rn(__fmul_rn(row[0], fr.origin[0]), __fmul_rn(row[1], fr.origin[1])),
+                                   __fmul_rn(row[2], fr.origin[2]));
+        }
+        out_pose[16 * (int64_t)f + threadIdx.x] = v;
+    }
+}
+
 }  // namespace frames
 }  // namespace us3d
 
@@ -94,6 +145,26 @@ extern "C" int us3d_frames_gather(const us3d_slice_frame* all_frames, int64_t n_
         all_frames, n_all, indices, height, width, all_pixel_positions, images, image_format, out_frames,
         out_pixel_positions, out_targets, status);
     US3D_CHECK_LAUNCH("frames gather");
+    count_launches(1);
+    return US3D_OK;
+}
+
+extern "C" int us3d_frames_geometry(const us3d_slice_frame* all_frames, int64_t n_all, const int64_t* indices,
+                                    int32_t n_batch, int32_t width, const float* all_ray_origins,
+                                    const float* all_ray_dirs, const float* all_poses, float* out_ray_origins,
+                                    float* out_ray_dirs, float* out_pose, int32_t* status, void* stream_) {
+    US3D_CHECK_ARG(n_all >= 0 && n_batch >= 0 && width >= 0, "negative size");
+    US3D_CHECK_ARG(n_batch <= 65535, "at most 65535 frames per batch");
+    if (n_batch == 0) return US3D_OK;
+    US3D_CHECK_ARG(n_all > 0, "the dataset has no frames");
+    US3D_CHECK_ARG(all_frames && indices && out_pose && status && (width == 0 || (out_ray_origins && out_ray_dirs)),
+                   "pointer is NULL");
+    const dim3 grid((unsigned)std::max<int64_t>(1, ((int64_t)width + frames::THREADS - 1) / frames::THREADS),
+                    (unsigned)n_batch);
+    frames::geometry_kernel<<<grid, frames::THREADS, 0, (cudaStream_t)stream_>>>(
+        all_frames, n_all, indices, width, all_ray_origins, all_ray_dirs, all_poses, out_ray_origins, out_ray_dirs,
+        out_pose, status);
+    US3D_CHECK_LAUNCH("frames geometry");
     count_launches(1);
     return US3D_OK;
 }

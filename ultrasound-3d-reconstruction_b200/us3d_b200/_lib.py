@@ -131,6 +131,11 @@ _SIGNATURES = {
         [c_void_p, c_int64, c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
          c_void_p, c_void_p, c_void_p],
     ),
+    "us3d_frames_geometry": (
+        c_int32,
+        [c_void_p, c_int64, c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_void_p, c_void_p],
+    ),
     "us3d_ug_pixel_csr": (
         c_int32,
         [c_void_p, c_void_p, c_int32, c_int64, c_int64, c_int64, c_int64, c_void_p, c_float, c_float, c_void_p,

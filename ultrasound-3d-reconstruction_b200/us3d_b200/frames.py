@@ -1,12 +1,14 @@
 """Frame batches built on the device from a dataset held in device memory.
 
-The reference's loader (``NpzUltrasoundDataset``, pipeline_god_file.py:172-333) reads one frame
+The reference's loader (``NpzUltrasoundDataset``, pipeline_god_file.py:172-336) reads one frame
 per training step on the host: it scales 8-bit images to [0, 1], normalises the probe axes,
-generates (or reads) the pixel centre positions and copies everything to the GPU. Here the
-dataset is moved to the device once (images kept in their stored 8-bit or float form, axes
-normalised with the reference's ``_normalize``), and a batch of frames is assembled by one
-launch (``us3d_frames_gather``) from a device tensor of dataset indices: frame records,
-pixel positions (gathered, or generated bit-identically to the reference's grid) and targets.
+generates (or reads) the pixel centre positions, the scanlines (ray origins and directions) and
+the world-to-probe pose, and copies everything to the GPU. Here the dataset is moved to the
+device once (images kept in their stored 8-bit or float form, axes normalised with the
+reference's ``_normalize``), and a batch of frames is assembled by one launch
+(``us3d_frames_gather``) from a device tensor of dataset indices: frame records, pixel positions
+(gathered, or generated bit-identically to the reference's grid) and targets;
+``us3d_frames_geometry`` adds the scanlines and poses of the same indices.
 """
 
 from __future__ import annotations
@@ -33,11 +35,13 @@ class DeviceFrameSource:
     as the reference does); origin, axis_lat, axis_ax, axis_ele: (N,3) or (3,) (axes are
     normalised per frame); pixel_positions: optional (N,H*W,3) or (N,H,W,3) mm, otherwise
     generated from the geometry with ``delta_lateral_mm``, ``delta_axial_mm``, ``near_mm`` and
-    the lateral centring of the reference's config."""
+    the lateral centring of the reference's config; ray_origins / ray_dirs: optional (N,W,3) and
+    poses_world_to_probe optional (N,4,4), otherwise generated as the reference does."""
 
     def __init__(self, images, origin, axis_lat, axis_ax, axis_ele, delta_lateral_mm: float,
                  delta_axial_mm: float, near_mm: float = 0.0, center_lateral: bool = True,
-                 pixel_positions=None, device: Optional[torch.device] = None):
+                 pixel_positions=None, device: Optional[torch.device] = None, ray_origins=None, ray_dirs=None,
+                 poses_world_to_probe=None):
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         img = torch.as_tensor(np.asarray(images) if not torch.is_tensor(images) else images)
         if img.ndim == 4:
@@ -73,6 +77,14 @@ class DeviceFrameSource:
         if pixel_positions is not None:
             pp = torch.as_tensor(np.asarray(pixel_positions, dtype=np.float32))
             self.pixel_positions = pp.reshape(self.n, self.height * self.width, 3).to(dev).contiguous()
+        def stored(a, shape):
+            if a is None:
+                return None
+            return torch.as_tensor(np.asarray(a, dtype=np.float32)).reshape(self.n, *shape).to(dev).contiguous()
+
+        self.ray_origins = stored(ray_origins, (self.width, 3))
+        self.ray_dirs = stored(ray_dirs, (self.width, 3))
+        self.poses = stored(poses_world_to_probe, (16,))
         self.device = dev
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
@@ -83,9 +95,13 @@ class DeviceFrameSource:
         optional per-frame geometry and pixel positions)."""
         raw = np.load(path, allow_pickle=False)
         get = (lambda k: raw[k] if k in raw else None)
+        n = raw["images"].shape[0]
+        pose = get("pose_world_to_probe")
+        if pose is not None and not (pose.ndim == 3 and pose.shape[0] == n):
+            pose = np.tile(np.asarray(pose, np.float32).reshape(1, 4, 4), (n, 1, 1))  # one pose for all
         return cls(raw["images"], get("probe_origin_world"), get("axis_lateral_world"), get("axis_axial_world"),
                    get("axis_elevational_world"), delta_lateral_mm, delta_axial_mm, near_mm, center_lateral,
-                   get("pixel_positions_world"), device)
+                   get("pixel_positions_world"), device, get("ray_origins"), get("ray_dirs"), pose)
 
     def frame_table(self, batch_size: int) -> UG.FrameTable:
         """An (unfilled) frame table for batches of ``batch_size`` frames."""
@@ -118,6 +134,21 @@ class DeviceFrameSource:
         targets = torch.empty((F * self.height * self.width,), dtype=torch.float32, device=self.device)
         self.fill(indices, table, pixels, targets)
         return table, pixels, targets
+
+    def geometry(self, indices: torch.Tensor):
+        """(ray_origins (F,W,3), ray_dirs (F,W,3), pose_world_to_probe (F,4,4)) of the dataset
+        ``indices`` (device int64), one launch, no synchronisation."""
+        F = int(indices.numel())
+        if indices.dtype != torch.int64 or indices.device != self.device:
+            raise ValueError("indices must be an int64 tensor on the dataset's device")
+        origins = torch.empty((F, self.width, 3), dtype=torch.float32, device=self.device)
+        dirs = torch.empty((F, self.width, 3), dtype=torch.float32, device=self.device)
+        pose = torch.empty((F, 4, 4), dtype=torch.float32, device=self.device)
+        _lib.check(_lib.call("us3d_frames_geometry", _ptr(self.records), self.n, _ptr(indices.contiguous()), F,
+                             self.width, _ptr(self.ray_origins), _ptr(self.ray_dirs), _ptr(self.poses),
+                             _ptr(origins), _ptr(dirs), _ptr(pose), _ptr(self.status), _stream()),
+                   "us3d_frames_geometry")
+        return origins, dirs, pose
 
     def check(self) -> None:
         """Raises if any index given to ``fill`` was out of range (synchronises)."""
