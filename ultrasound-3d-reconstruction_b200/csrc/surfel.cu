@@ -774,13 +774,24 @@ reduce_preprocess_kernel(Params p, float focal_x, float focal_y, float tan_fovx,
     for (int q = 0; q < 20; ++q) s[q] = 0.f;
     const bool vis = radii[g] > 0 && header[H_FLAGS] == 0;
     if (vis) {
-        for (int i = inst_offset[g]; i < inst_offset[g + 1]; ++i) {
+        auto add = [&](const float4& x, int f) {
+            s[4 * f] += x.x; s[4 * f + 1] += x.y; s[4 * f + 2] += x.z; s[4 * f + 3] += x.w;
+        };
+        const int i1 = inst_offset[g + 1];
+        int i = inst_offset[g];
+        // two instances' loads in flight at a time; the sums keep instance order
+        for (; i + 2 <= i1; i += 2) {
+            const float4* r = partial + (int64_t)PARTIAL_F4 * i;
+            float4 v[2 * PARTIAL_F4];
+#pragma unroll
+            for (int f = 0; f < 2 * PARTIAL_F4; ++f) v[f] = r[f];
+#pragma unroll
+            for (int f = 0; f < 2 * PARTIAL_F4; ++f) add(v[f], f % PARTIAL_F4);
+        }
+        if (i < i1) {
             const float4* r = partial + (int64_t)PARTIAL_F4 * i;
 #pragma unroll
-            for (int f = 0; f < PARTIAL_F4; ++f) {
-                const float4 x = r[f];
-                s[4 * f] += x.x; s[4 * f + 1] += x.y; s[4 * f + 2] += x.z; s[4 * f + 3] += x.w;
-            }
+            for (int f = 0; f < PARTIAL_F4; ++f) add(r[f], f);
         }
     }
     // defaults: everything zero, render sums passed through
