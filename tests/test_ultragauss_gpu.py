@@ -127,6 +127,17 @@ def test_live_reference_parity_dense_tiles(cuda_device):
     _assert_case(out, fx)
 
 
+def test_live_reference_parity_many_gaussians(cuda_device):
+    """More Gaussians than the tile sort packs into one 64-bit word (2^20 - 1): the shared-memory
+    pass sorts keys with their slot payload; keys, ranges, candidate lists, image and gradients
+    against the reference's own build."""
+    REF, REFK = _reference_modules()
+    fx = _scene_case(1100000, 96, 80, 0.25, 13, frame=1)
+    fx.update(_reference_run(REF, REFK, fx, cuda_device))
+    out = run_b200(fx, cuda_device)
+    _assert_case(out, fx)
+
+
 @pytest.mark.parametrize("beta", [1e-12, 5e-11])
 def test_live_reference_parity_windowed(beta, cuda_device):
     """A diagonal offset in (0, 1e-10) (the reference's clamp inside the window radii can then

@@ -189,82 +189,115 @@ static inline cudaError_t launch_rect_scatter(int64_t n, int gx, int64_t n_bucke
 // l holds its elements 2l (x0) and 2l + 1 (x1). A compare-exchange of stride h >= 2 pairs
 // lane l with lane l ^ h/2 (same slot); a mirror pass over blocks of `size` pairs element
 // e with e ^ (size - 1), i.e. slot 0 of lane l with slot 1 of lane l ^ (size/2 - 1).
-struct SortKV {
+template <bool PAY>
+struct SortEl;  // a key with (PAY) or without its int payload
+template <>
+struct SortEl<true> {
     unsigned long long k;
     int v;
 };
+template <>
+struct SortEl<false> {
+    unsigned long long k;
+};
 
-static __device__ __forceinline__ SortKV kv_shfl_xor(const SortKV& x, int mask) {
-    SortKV y;
+template <bool PAY>
+static __device__ __forceinline__ SortEl<PAY> kv_shfl_xor(const SortEl<PAY>& x, int mask) {
+    SortEl<PAY> y;
     y.k = __shfl_xor_sync(0xffffffffu, x.k, mask);
-    y.v = __shfl_xor_sync(0xffffffffu, x.v, mask);
+    if constexpr (PAY) y.v = __shfl_xor_sync(0xffffffffu, x.v, mask);
     return y;
 }
 
 // x becomes the smaller (keep_low) or the larger key of the pair; an equal key keeps x.
-static __device__ __forceinline__ void kv_keep(SortKV& x, const SortKV& y, bool keep_low) {
+template <bool PAY>
+static __device__ __forceinline__ void kv_keep(SortEl<PAY>& x, const SortEl<PAY>& y, bool keep_low) {
     if (keep_low ? (y.k < x.k) : (x.k < y.k)) x = y;
 }
 
-static __device__ __forceinline__ void kv_order(SortKV& a, SortKV& b) {
+template <bool PAY>
+static __device__ __forceinline__ void kv_order(SortEl<PAY>& a, SortEl<PAY>& b) {
     if (b.k < a.k) {
-        const SortKV t = a;
+        const SortEl<PAY> t = a;
         a = b;
         b = t;
     }
 }
 
-static __device__ __forceinline__ void warp_stride_pass(SortKV& x0, SortKV& x1, int h, int lane) {
+template <bool PAY>
+static __device__ __forceinline__ void warp_stride_pass(SortEl<PAY>& x0, SortEl<PAY>& x1, int h, int lane) {
     if (h == 1) {
         kv_order(x0, x1);
         return;
     }
     const int m = h >> 1;
     const bool low = (lane & m) == 0;
-    const SortKV y0 = kv_shfl_xor(x0, m), y1 = kv_shfl_xor(x1, m);
+    const SortEl<PAY> y0 = kv_shfl_xor(x0, m), y1 = kv_shfl_xor(x1, m);
     kv_keep(x0, y0, low);
     kv_keep(x1, y1, low);
 }
 
-static __device__ __forceinline__ void warp_mirror_pass(SortKV& x0, SortKV& x1, int size, int lane) {
+template <bool PAY>
+static __device__ __forceinline__ void warp_mirror_pass(SortEl<PAY>& x0, SortEl<PAY>& x1, int size, int lane) {
     if (size == 2) {
         kv_order(x0, x1);
         return;
     }
     const int m = (size >> 1) - 1;
     const bool low = (lane & (size >> 2)) == 0;
-    const SortKV y0 = kv_shfl_xor(x1, m), y1 = kv_shfl_xor(x0, m);
+    const SortEl<PAY> y0 = kv_shfl_xor(x1, m), y1 = kv_shfl_xor(x0, m);
     kv_keep(x0, y0, low);
     kv_keep(x1, y1, low);
 }
 
+template <bool PAY>
 static __device__ __forceinline__ void seg_load(const unsigned long long* sk, const int* sv, int seg, int lane,
-                                                SortKV& x0, SortKV& x1) {
+                                                SortEl<PAY>& x0, SortEl<PAY>& x1) {
     const ulonglong2 k = reinterpret_cast<const ulonglong2*>(sk)[seg * 32 + lane];
-    const int2 v = reinterpret_cast<const int2*>(sv)[seg * 32 + lane];
-    x0 = {k.x, v.x};
-    x1 = {k.y, v.y};
+    x0.k = k.x;
+    x1.k = k.y;
+    if constexpr (PAY) {
+        const int2 v = reinterpret_cast<const int2*>(sv)[seg * 32 + lane];
+        x0.v = v.x;
+        x1.v = v.y;
+    }
 }
 
+template <bool PAY>
 static __device__ __forceinline__ void seg_store(unsigned long long* sk, int* sv, int seg, int lane,
-                                                 const SortKV& x0, const SortKV& x1) {
+                                                 const SortEl<PAY>& x0, const SortEl<PAY>& x1) {
     reinterpret_cast<ulonglong2*>(sk)[seg * 32 + lane] = make_ulonglong2(x0.k, x1.k);
-    reinterpret_cast<int2*>(sv)[seg * 32 + lane] = make_int2(x0.v, x1.v);
+    if constexpr (PAY) reinterpret_cast<int2*>(sv)[seg * 32 + lane] = make_int2(x0.v, x1.v);
 }
 
-// Ascending sort of the npow (a power of two >= 64) keys with payload in shared memory
-// (16-byte aligned key array, 8-byte aligned payload array), the same mirror network as
-// bitonic_sort: passes that stay inside 64-element segments run in registers with warp
-// shuffles, the others as shared-memory compare-exchanges between block barriers. The
+template <bool PAY>
+static __device__ __forceinline__ void cswap_smem(unsigned long long* k, int* v, int a, int b) {
+    const unsigned long long ka = k[a], kb = k[b];
+    if (kb < ka) {
+        k[a] = kb;
+        k[b] = ka;
+        if constexpr (PAY) {
+            const int t = v[a];
+            v[a] = v[b];
+            v[b] = t;
+        }
+    }
+}
+
+// Ascending sort of the npow (a power of two >= 64) keys, with (PAY) or without an int payload,
+// in shared memory (16-byte aligned key array, 8-byte aligned payload array), the same mirror
+// network as bitonic_sort: passes that stay inside 64-element segments run in registers with
+// warp shuffles, the others as shared-memory compare-exchanges between block barriers. The
 // caller pads the keys past the first n with SORT_PAD_KEY and synchronises first. Every
 // compare-exchange puts the smaller key at the lower index, so the padding never moves and an
 // exchange whose upper index is >= n does nothing: those exchanges, and the 64-element
 // segments lying wholly in the padding, are skipped.
+template <bool PAY>
 static __device__ void block_sort_smem(unsigned long long* sk, int* sv, int npow, int n) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int nseg = (n + 63) >> 6, half_n = npow >> 1;
     for (int s = warp; s < nseg; s += nwarp) {
-        SortKV x0, x1;
+        SortEl<PAY> x0, x1;
         seg_load(sk, sv, s, lane, x0, x1);
 #pragma unroll
         for (int size = 2; size <= 64; size <<= 1) {
@@ -280,19 +313,19 @@ static __device__ void block_sort_smem(unsigned long long* sk, int* sv, int npow
         for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
             const int base = (i >> lh) << ls, off = i & (hs - 1);
             const int b = base + size - 1 - off;
-            if (b < n) cswap(sk, sv, base + off, b);
+            if (b < n) cswap_smem<PAY>(sk, sv, base + off, b);
         }
         __syncthreads();
         for (int l2 = lh - 1; l2 >= 6; --l2) {
             const int h = 1 << l2;
             for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
                 const int a = ((i >> l2) << (l2 + 1)) + (i & (h - 1));
-                if (a + h < n) cswap(sk, sv, a, a + h);
+                if (a + h < n) cswap_smem<PAY>(sk, sv, a, a + h);
             }
             __syncthreads();
         }
         for (int s = warp; s < nseg; s += nwarp) {
-            SortKV x0, x1;
+            SortEl<PAY> x0, x1;
             seg_load(sk, sv, s, lane, x0, x1);
 #pragma unroll
             for (int h = 32; h >= 1; h >>= 1) warp_stride_pass(x0, x1, h, lane);
@@ -302,22 +335,49 @@ static __device__ void block_sort_smem(unsigned long long* sk, int* sv, int npow
     }
 }
 
+// Buckets of at most SORT_SMEM_CAP keys whose element indices (a key's low word) are below
+// SORT_PACK_G can be ordered without a payload: the key (hi << 32 | g) is packed as
+// (hi << 32 | g << 12 | slot), which orders like the key itself (a bucket holds an element
+// once) and carries the bucket slot in its low 12 bits.
+constexpr int64_t SORT_PACK_G = (1 << 20) - 1;
+
 // Orders bucket t (n keys at s0) in shared memory of capacity `cap` (a power of two >= n)
-// and writes the sorted Gaussian indices, instance ids and keys.
+// and writes the sorted Gaussian indices, instance ids and keys; `packed`: every element index
+// of the bucket is below SORT_PACK_G (then buckets of up to SORT_SMEM_CAP keys sort without a
+// payload).
 static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_keys, int* s_idx, int s0, int n,
                                                         unsigned long long* __restrict__ keys,
                                                         const int* __restrict__ slot_inst,
                                                         int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
                                                         const uint16_t* __restrict__ slot_mask,
-                                                        uint16_t* __restrict__ sorted_mask) {
+                                                        uint16_t* __restrict__ sorted_mask, bool packed) {
     int npow = 64;
     while (npow < n) npow <<= 1;
+    if (packed && n <= SORT_SMEM_CAP) {
+        for (int i = threadIdx.x; i < npow; i += blockDim.x) {
+            const unsigned long long k = i < n ? keys[s0 + i] : 0ull;
+            s_keys[i] = i < n ? ((k & 0xffffffff00000000ull) | ((k & 0xfffffull) << 12) | (unsigned long long)i)
+                              : SORT_PAD_KEY;
+        }
+        __syncthreads();
+        block_sort_smem<false>(s_keys, nullptr, npow, n);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned long long k = s_keys[i];
+            const int slot = (int)(k & 0xfffull);
+            const uint32_t g = (uint32_t)((k >> 12) & 0xfffffull);
+            sorted_gid[s0 + i] = (int)g;
+            sorted_inst[s0 + i] = slot_inst[s0 + slot];
+            if (sorted_mask) sorted_mask[s0 + i] = slot_mask[s0 + slot];
+            keys[s0 + i] = (k & 0xffffffff00000000ull) | g;
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < npow; i += blockDim.x) {
         s_keys[i] = i < n ? keys[s0 + i] : SORT_PAD_KEY;
         s_idx[i] = i;
     }
     __syncthreads();
-    block_sort_smem(s_keys, s_idx, npow, n);
+    block_sort_smem<true>(s_keys, s_idx, npow, n);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const unsigned long long k = s_keys[i];
         sorted_gid[s0 + i] = (int)(uint32_t)(k & 0xffffffffull);
@@ -337,7 +397,7 @@ static __global__ void __launch_bounds__(SORT_THREADS, SORT_MIN_BLOCKS)
 tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
                  unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
                  int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
-                 const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask) {
+                 const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask, int packed) {
     __shared__ __align__(16) unsigned long long s_keys[SORT_SMEM_CAP];
     __shared__ __align__(16) int s_idx[SORT_SMEM_CAP];
     const int64_t t = blockIdx.x;
@@ -346,7 +406,8 @@ tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long*
     const int n = tile_start[t + 1] - s0;
     if (n <= 0) return;
     if (n <= SORT_SMEM_CAP) {
-        sort_bucket_smem(s_keys, s_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
+        sort_bucket_smem(s_keys, s_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask,
+                         packed != 0);
     } else if (n > SORT_BIG_CAP) {
         // Oversized bucket: the network directly on global memory (one block owns it), with
         // the slot indices as payload in sorted_inst.
@@ -395,7 +456,7 @@ tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long l
             const int s0 = tile_start[tt];
             const int n = tile_start[tt + 1] - s0;
             sort_bucket_smem(s_big_keys, s_big_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask,
-                             sorted_mask);
+                             sorted_mask, false);
             __syncthreads();
         }
     }
@@ -403,18 +464,20 @@ tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long l
 
 static inline size_t tile_sort_big_smem_bytes() { return SORT_BIG_CAP * (sizeof(unsigned long long) + sizeof(int)); }
 
-// Launches the tile sort on `stream`: the shared-memory pass over all T tiles and, for large
-// buckets, the 96 KB pass. `attr_done` records per device that the second kernel's
+// Launches the tile sort on `stream` for keys whose low word indexes one of n_elems elements:
+// the shared-memory pass over all T tiles and, for large
+// buckets, the 192 KB pass. `attr_done` records per device that the second kernel's
 // shared-memory limit was raised (one array per translation unit, 128 devices). slot_mask /
 // sorted_mask may be NULL.
-static inline cudaError_t launch_tile_sort(int64_t T, const int* tile_start, const long long* header,
-                                           unsigned long long* keys, const int* slot_inst, int* sorted_gid,
-                                           int* sorted_inst, bool* attr_done, cudaStream_t stream,
+static inline cudaError_t launch_tile_sort(int64_t T, int64_t n_elems, const int* tile_start,
+                                           const long long* header, unsigned long long* keys, const int* slot_inst,
+                                           int* sorted_gid, int* sorted_inst, bool* attr_done, cudaStream_t stream,
                                            const uint16_t* slot_mask = nullptr,
                                            uint16_t* sorted_mask = nullptr) {
     if (T <= 0) return cudaSuccess;
+    const int packed = n_elems < SORT_PACK_G ? 1 : 0;
     tile_sort_kernel<<<(unsigned)T, SORT_THREADS, 0, stream>>>(T, tile_start, header, keys, slot_inst, sorted_gid,
-                                                                sorted_inst, slot_mask, sorted_mask);
+                                                                sorted_inst, slot_mask, sorted_mask, packed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int dev = 0;

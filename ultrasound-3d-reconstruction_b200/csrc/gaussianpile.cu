@@ -954,7 +954,7 @@ extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t 
     check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
     US3D_CHECK_CUDA(launch_rect_scatter(n_gauss, tx, T, RectOf4{w.rects}, w.dkey, w.inst_offset, w.tile_start,
                                         w.tile_cursor, w.header, w.keys, w.slot_inst, stream));
-    US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
+    US3D_CHECK_CUDA(launch_tile_sort(T, n_gauss, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_gp_sort_attr, stream));
     // up to four threads per pixel (a whole-warp pixel block of at most 1024 threads)
     const int npix = (tile_size * tile_size + 31) / 32 * 32;

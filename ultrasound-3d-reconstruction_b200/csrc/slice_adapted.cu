@@ -452,7 +452,7 @@ extern "C" int us3d_sa_bounded_forward(void* workspace, size_t workspace_bytes, 
     check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
     US3D_CHECK_CUDA(launch_rect_scatter(n, gw, T, RectOf4{w.rects}, nullptr, w.inst_offset, w.tile_start,
                                         w.tile_cursor, w.header, w.keys, w.slot_inst, stream));
-    US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
+    US3D_CHECK_CUDA(launch_tile_sort(T, n, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_sa_sort_attr, stream));
     forward_kernel<<<(unsigned)T, TILE * TILE, 0, stream>>>(H, W, gw, half_width, half_height, radius_sigma, m2, iv,
                                                             weights, colors, w.tile_start, w.sorted_gid, w.header,

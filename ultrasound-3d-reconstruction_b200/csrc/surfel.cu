@@ -1066,7 +1066,7 @@ extern "C" int us3d_gs_forward(void* workspace, size_t workspace_bytes, int64_t 
     US3D_CHECK_CUDA(launch_rect_scatter(n_gauss, p.gx, T, RectOf4{w.rect}, reinterpret_cast<const uint32_t*>(w.depth),
                                         w.inst_offset, w.tile_start, w.tile_cursor, w.header, w.keys, w.slot_inst,
                                         stream));
-    US3D_CHECK_CUDA(launch_tile_sort(T, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
+    US3D_CHECK_CUDA(launch_tile_sort(T, n_gauss, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_gs_sort_attr, stream));
     forward_kernel<<<(unsigned)T, BLOCK, 0, stream>>>(width, height, p.gx, w.tile_start, w.sorted_gid, w.header, w.rec,
                                                       background, out_color, out_others, w.accum, w.n_contrib);

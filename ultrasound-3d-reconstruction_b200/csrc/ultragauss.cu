@@ -1221,7 +1221,7 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
         verify_kernel<<<(unsigned)((n_tiles + 255) / 256), 256, 0, stream>>>(n_tiles, w.tile_count, w.tile_cursor,
                                                                               w.header);
     if (n_tiles > 0) {
-        US3D_CHECK_CUDA(launch_tile_sort(n_tiles, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid,
+        US3D_CHECK_CUDA(launch_tile_sort(n_tiles, n_gauss, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid,
                                          w.sorted_inst, g_sort_attr_done, stream, w.slot_mask, w.sorted_mask));
     }
     prof_end(prof, stream);

@@ -725,7 +725,7 @@ extern "C" int us3d_ugr_forward(void* workspace, size_t workspace_bytes, int64_t
     check_kernel<<<1, 1, 0, stream>>>(w.header, cap);
     US3D_CHECK_CUDA(launch_rect_scatter(n_gauss, W, W, RangeOf2{w.ray_range}, w.dkey, w.inst_offset, w.ray_start,
                                         w.ray_cursor, w.header, w.keys, w.slot_inst, stream));
-    US3D_CHECK_CUDA(launch_tile_sort(W, w.ray_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
+    US3D_CHECK_CUDA(launch_tile_sort(W, n_gauss, w.ray_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_ugr_sort_attr, stream));
     forward_kernel<<<dim3((unsigned)W, (unsigned)((H + FWD_SAMPLES - 1) / FWD_SAMPLES)), FWD_SAMPLES, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions,
                                                     ray_origins, ray_dirs, axis_ele, ray_perturbations, w.dkey,
