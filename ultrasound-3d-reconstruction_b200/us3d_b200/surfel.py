@@ -90,10 +90,14 @@ def backward(state: Optional[GSState], background, means3D, radii, colors, scale
     P = int(means3D.shape[0])
     M = int(sh.shape[1]) if (sh is not None and sh.numel() > 0 and sh.dim() >= 2) else 0
     z = lambda *s: torch.zeros(s, dtype=torch.float32, device=dev)  # noqa: E731
-    dmeans2D, dcolors, dopacity, dmeans3D = z(P, 3), z(P, 3), z(P, 1), z(P, 3)
-    dtrans, dsh, dscales, drot = z(P, 9), z(P, M, 3), z(P, 2), z(P, 4)
     if P == 0 or state is None:
-        return dmeans2D, dcolors, dopacity, dmeans3D, dtrans, dsh, dscales, drot
+        return z(P, 3), z(P, 3), z(P, 1), z(P, 3), z(P, 9), z(P, M, 3), z(P, 2), z(P, 4)
+    # the backward writes every entry of each gradient it is given; the others stay zero
+    e = lambda *s: torch.empty(s, dtype=torch.float32, device=dev)  # noqa: E731
+    dmeans2D, dcolors, dopacity, dmeans3D, dtrans = e(P, 3), e(P, 3), e(P, 1), e(P, 3), e(P, 9)
+    dsh = e(P, M, 3) if M > 0 and _ptr(sh) else z(P, M, 3)
+    dscales = e(P, 2) if _ptr(scales) else z(P, 2)
+    drot = e(P, 4) if _ptr(rotations) else z(P, 4)
     H, W = int(dL_dout_color.shape[1]), int(dL_dout_color.shape[2])
     scratch = torch.empty(max(int(_lib.call("us3d_gs_backward_scratch_bytes", state.capacity)), 16),
                           dtype=torch.uint8, device=dev)
