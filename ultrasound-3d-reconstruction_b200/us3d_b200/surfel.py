@@ -50,13 +50,17 @@ def forward(background, means3D, colors, opacity, scales, rotations, scale_modif
     P = int(means3D.shape[0])
     H, W = int(image_height), int(image_width)
     M = int(sh.shape[1]) if (sh is not None and sh.numel() > 0 and sh.dim() >= 2) else 0
-    color = torch.zeros((3, H, W), dtype=torch.float32, device=dev)
-    others = torch.zeros((7, H, W), dtype=torch.float32, device=dev)
-    radii = torch.zeros((P,), dtype=torch.int32, device=dev)
+    if P == 0:
+        return (0, torch.zeros((3, H, W), dtype=torch.float32, device=dev),
+                torch.zeros((7, H, W), dtype=torch.float32, device=dev), torch.zeros((0,), dtype=torch.int32, device=dev),
+                None)
+    # a call that returns has written every pixel of both images (the shading kernel covers
+    # all tiles) and every radius (the preprocess writes one per Gaussian)
+    color = torch.empty((3, H, W), dtype=torch.float32, device=dev)
+    others = torch.empty((7, H, W), dtype=torch.float32, device=dev)
+    radii = torch.empty((P,), dtype=torch.int32, device=dev)
     key = (P, W, H)
     cap = int(capacity if capacity is not None else _capacity_hint.get(key, max(4096, 4 * P)))
-    if P == 0:
-        return 0, color, others, radii, None
     for _ in range(3):
         nbytes = int(_lib.call("us3d_gs_workspace_bytes", P, W, H, cap))
         ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
