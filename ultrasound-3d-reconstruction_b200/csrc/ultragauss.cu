@@ -903,7 +903,14 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
             __syncthreads();
         }
 
-        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        // Rounds of THREADS instances; the regrouped order runs from the most marked sub-blocks
+        // to the fewest, so odd rounds hand the warps their slices in reverse (serpentine) and
+        // no warp takes the heaviest slice of every round.
+        for (int r0 = 0; r0 < nc; r0 += THREADS) {
+            const int wi = threadIdx.x >> 5;
+            const int i = r0 + (((r0 / THREADS) & 1) ? (THREADS / 32 - 1 - wi) * 32 + (threadIdx.x & 31)
+                                                     : (int)threadIdx.x);
+            if (i >= nc) continue;
             const int k = s0 + c0 + (culled ? (int)s_perm[i] : i);
             const int g = sorted_gid[k];
             const int inst = sorted_inst[k];
