@@ -742,7 +742,7 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
         // The exponential is evaluated for every pair and the sums are predicated: the lanes of
         // a warp (one 8x4 block) run the pair together anyway.
         const float q = quad_form(d, f1, f2.x, f2.y);
-        const float ah = f0.w * __expf(-0.5f * q);
+        const float ah = f0.w * exp2f(q * kNegHalfLog2e);  // exp(-q/2), as in the backward
         const bool pass = q <= chi2;
         const bool keep = pass && ah > 1e-8f;
         if (keep) {
