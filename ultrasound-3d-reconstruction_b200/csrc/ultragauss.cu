@@ -1014,7 +1014,20 @@ reduce_kernel(int64_t G, const int* __restrict__ inst_offset, const long long* _
 #pragma unroll
             for (int u = 0; u < 4; ++u) add(v[3 * u], v[3 * u + 1], v[3 * u + 2]);
         }
-        for (; i < i1; ++i, src += 3) add(src[0], src[1], src[2]);
+        if (i < i1) {  // the last one to three instances: their loads first, then the sums in order
+            const int rest = i1 - i;
+            float4 v[9];
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                if (u < rest) {
+                    v[3 * u] = src[3 * u];
+                    v[3 * u + 1] = src[3 * u + 1];
+                    v[3 * u + 2] = src[3 * u + 2];
+                }
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                if (u < rest) add(v[3 * u], v[3 * u + 1], v[3 * u + 2]);
+        }
     }
     d_means[3 * g + 0] = a.x;
     d_means[3 * g + 1] = a.y;
