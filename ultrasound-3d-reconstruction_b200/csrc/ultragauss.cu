@@ -712,7 +712,9 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     constexpr int STRIDE = WINDOWED ? 4 : 3;
     __shared__ float4 s_st[STRIDE * BATCH];
     __shared__ blockmask_t s_blocks[BATCH];
-    __shared__ short s_list[TILE_PIX / 32][BATCH];  // per warp: staged Gaussians reaching its block
+    // per warp: byte offsets into s_st of the staged Gaussians reaching its block
+    __shared__ unsigned short s_list[TILE_PIX / 32][BATCH];
+    static_assert((BATCH - 1) * STRIDE * 16 <= 0xffff, "staged offsets must fit 16 bits");
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
     const Geo geo = load_geo(frames + tile_frame[t]);
@@ -732,11 +734,12 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     // sums over the contributing pairs; kc, kd: the pairs the reference leaves out of the image
     // (alpha-hat <= 1e-8) but keeps in the backward's numerator / depth sums
     float sa = 0.f, sc = 0.f, sd = 0.f, kc = 0.f, kd = 0.f;
-    auto shade = [&](int j) {
-        const float4 f0 = s_st[STRIDE * j], f1 = s_st[STRIDE * j + 1], f2 = s_st[STRIDE * j + 2];
+    auto shade = [&](int off) {  // off: byte offset of the staged Gaussian in s_st
+        const float4* f = reinterpret_cast<const float4*>(reinterpret_cast<const char*>(s_st) + off);
+        const float4 f0 = f[0], f1 = f[1], f2 = f[2];
         const float3 d = make_float3(pv.x - f0.x, pv.y - f0.y, pv.z - f0.z);
         if constexpr (WINDOWED) {
-            const float4 f3 = s_st[STRIDE * j + 3];
+            const float4 f3 = f[3];
             if (!window_hit(d, geo.lat, geo.ax, f3.x, f3.y)) return;
         }
         // The exponential is evaluated for every pair and the sums are predicated: the lanes of
@@ -779,7 +782,7 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
         __syncthreads();
         // Lanes of an invalid pixel run along (their sums are never stored).
         if (!culled) {
-            for (int j = 0; j < nb; ++j) shade(j);
+            for (int j = 0; j < nb; ++j) shade(j * (STRIDE * 16));
             continue;
         }
         // Each warp lists, in staging order, the Gaussians whose mask marks one of its two
@@ -789,7 +792,7 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
             const int jl = jc + lane;
             const bool mine = jl < nb && ((s_blocks[jl] >> (2 * warp)) & 3u);
             const unsigned bits = __ballot_sync(0xffffffffu, mine);
-            if (mine) s_list[warp][n_w + __popc(bits & ((1u << lane) - 1u))] = (short)jl;
+            if (mine) s_list[warp][n_w + __popc(bits & ((1u << lane) - 1u))] = (unsigned short)(jl * (STRIDE * 16));
             n_w += __popc(bits);
         }
         __syncwarp();
