@@ -948,13 +948,12 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
                     const float q = quad_form(d, q1, s12, s22);
                     const float2 pb = pb_b[jj];
                     const float w = q <= chi2 ? exp2f(q * kNegHalfLog2e) : 0.0f;
-                    const float ah = o * w;
                     const float dah = pa.w * ci + pb.x + pb.y * dterm;
-                    acc_c += pa.w * ah;
-                    acc_o += dah * w;
-                    acc_e += pb.y * ah;
-                    const float dq = dah * ah;  // dL/dq without its factor -1/2 (applied below)
-                    const float ux = dq * d.x, uy = dq * d.y, uz = dq * d.z;
+                    const float dw = dah * w;  // dL/dopacity term; dL/dq = -o dw / 2 (o, -1/2 applied below)
+                    acc_c += pa.w * w;
+                    acc_o += dw;
+                    acc_e += pb.y * w;
+                    const float ux = dw * d.x, uy = dw * d.y, uz = dw * d.z;
                     sdx += ux;
                     sdy += uy;
                     sdz += uz;
@@ -966,10 +965,13 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
                     szz += uz * d.z;
                 }
             }
-            // The factor -1/2 of dL/dq, applied once: scaling by a power of two commutes with
-            // the roundings of the sums.
-            sdx *= -0.5f; sdy *= -0.5f; sdz *= -0.5f;
-            sxx *= -0.5f; sxy *= -0.5f; sxz *= -0.5f; syy *= -0.5f; syz *= -0.5f; szz *= -0.5f;
+            // The pairs' common factors, applied once per instance: -o/2 of dL/dq, o of the
+            // alpha-hat sums.
+            const float nh = -0.5f * o;
+            sdx *= nh; sdy *= nh; sdz *= nh;
+            sxx *= nh; sxy *= nh; sxz *= nh; syy *= nh; syz *= nh; szz *= nh;
+            acc_c *= o;
+            acc_e *= o;
             // d/dmean = -2 Lambda sum(dq d) + sum(ddw * ah) * ele (reference backward.cu:218-228).
             const float vx = q1.x * sdx + q1.y * sdy + q1.z * sdz;
             const float vy = q1.y * sdx + q1.w * sdy + s12 * sdz;
