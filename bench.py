@@ -41,8 +41,8 @@ BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (param
 # dram__bytes_read.sum + dram__bytes_write.sum of one 4-frame launch of the headline scene
 # (ncu --set full), per frame; the backward stage is backward_kernel + reduce_kernel.
 NCU_TRAFFIC_PER_FRAME = {
-    "ug_backward": (101.241088e6 + 114.438144e6 + 156.020480e6 + 28.401920e6) / 4,
-    "ug_forward": (52.456192e6 + 6.428928e6) / 4,
+    "ug_backward": (100.252416e6 + 114.988544e6 + 156.020480e6 + 28.401920e6) / 4,
+    "ug_forward": (52.274432e6 + 5.454592e6) / 4,
 }
 
 
