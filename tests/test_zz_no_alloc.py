@@ -27,12 +27,16 @@ pytestmark = pytest.mark.gpu
 IMG_TOL = 1e-5
 
 
-def _inputs(device, G, H, W, spacing, seed):
+def _inputs(device, G, H, W, spacing, seed, log_scale_mean=0.0, in_plane=False):
     from us3d_b200 import scenes
     from us3d_b200 import ultragauss as UG
 
-    sc = scenes.make_scene(G, seed=seed).to(device)
+    sc = scenes.make_scene(G, seed=seed, log_scale_mean=log_scale_mean)
     fr = scenes.linear_sweep(4, H, W, spacing, seed=seed)[1]
+    if in_plane:  # every mean moved onto the frame's plane: no Gaussian is culled
+        ele = (sc.means - fr.origin) @ fr.axis_ele
+        sc.means = (sc.means - ele[:, None] * fr.axis_ele[None, :]).contiguous()
+    sc = sc.to(device)
     spec = UG.SliceSpec(H, W, spacing, spacing, 0.0, fr.lateral_col_offset, fr.origin, fr.axis_lat, fr.axis_ax,
                         fr.axis_ele)
     frames = UG.build_frame_table([spec], device)
@@ -88,3 +92,50 @@ def test_noalloc_rejects_oversized_inputs(cuda_device):
     assert "exceed the no-allocation scratch" in msg, msg
     torch.cuda.synchronize()
     assert torch.isnan(img).all()  # nothing was launched
+
+
+def _regular(sc, frames, pixels, sort=True):
+    from us3d_b200 import ultragauss as UG
+
+    b = UG.bin_gaussians(sc.means, sc.precision_tril.contiguous(), sc.opacities, sc.intensities, frames, 7.815, 1e-4,
+                         sort)
+    return b, UG.forward(b, pixels, 1e-6, 0.0)
+
+
+def test_noalloc_instance_overflow_leaves_outputs(cuda_device):
+    from us3d_b200 import _lib
+
+    # 8000 Gaussians of about 12 mm across a 64 mm frame: millions of instances, far more
+    # than the scratch holds, while the sizes themselves fit
+    sc, frames, pixels = _inputs(cuda_device, 8000, 512, 512, 0.125, 3, log_scale_mean=float(np.log(12.0)))
+    b, _ = _regular(sc, frames, pixels)
+    torch.cuda.synchronize()
+    for call in range(2):
+        st, img, alpha, depth, counts, n_inst = _noalloc(sc, frames, pixels)
+        assert st == _lib.US3D_CAPACITY_OVERFLOW, (call, st)
+        msg = _lib.load().us3d_last_error().decode()
+        assert "instances exceed" in msg, msg
+        assert n_inst == b.total, (call, n_inst, b.total)
+        torch.cuda.synchronize()
+        assert torch.isnan(img).all() and torch.isnan(alpha).all() and torch.isnan(depth).all()
+        assert (counts == -1).all()
+
+
+def test_noalloc_single_tile_gaussians(cuda_device):
+    from us3d_b200 import _lib
+
+    # 200k Gaussians of about 0.05 mm on the frame's plane: each reaches one or two 16x16
+    # tiles, so the surviving (Gaussian, frame) pairs are most of the instances
+    sc, frames, pixels = _inputs(cuda_device, 200_000, 512, 512, 0.125, 4, log_scale_mean=float(np.log(0.05)),
+                                 in_plane=True)
+    b, (ref_img, ref_alpha, ref_depth, ref_counts) = _regular(sc, frames, pixels)
+    torch.cuda.synchronize()
+    assert b.total < 2 * 200_000, b.total
+    for call in range(2):
+        st, img, alpha, depth, counts, n_inst = _noalloc(sc, frames, pixels)
+        _lib.check(st, "us3d_ug_render_noalloc")
+        torch.cuda.synchronize()
+        assert n_inst == b.total, (call, n_inst, b.total)
+        assert torch.equal(counts, ref_counts), call
+        for got, ref in ((img, ref_img), (alpha, ref_alpha), (depth, ref_depth)):
+            assert rel_l2(got.cpu().numpy(), ref.cpu().numpy()) <= IMG_TOL, call

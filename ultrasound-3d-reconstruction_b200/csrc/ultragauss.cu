@@ -96,7 +96,10 @@ struct Workspace {
 // with a total that makes the retried capacity large enough.
 static inline int64_t task_capacity(int64_t cap) { return cap / 4 + 4096; }
 
-static Workspace carve(void* base, int64_t G, int64_t T, int64_t P, int64_t cap) {
+// Layout of a workspace. The task arrays, used only while binning, come last, so the
+// shading and export entry points find every other array at the same place whatever the
+// task capacity (tc < 0: the default task_capacity(cap)).
+static Workspace carve(void* base, int64_t G, int64_t T, int64_t P, int64_t cap, int64_t tc = -1) {
     Carver c(base);
     Workspace w;
     w.header = c.take<long long>(H_WORDS);
@@ -105,13 +108,6 @@ static Workspace carve(void* base, int64_t G, int64_t T, int64_t P, int64_t cap)
     w.task_offset = c.take<int>((size_t)G + 1);
     w.bs_g = c.take<long long>((size_t)scan_num_blocks(G) + 1);
     w.inst_offset = c.take<int>((size_t)G + 1);
-    const int64_t tc = task_capacity(cap);
-    w.task_rect = c.take<int4>((size_t)tc);
-    w.task_gf = c.take<int2>((size_t)tc);
-    w.task_v = c.take<float>((size_t)tc);
-    w.task_ntiles = c.take<int>((size_t)tc);
-    w.task_inst = c.take<int>((size_t)tc + 1);
-    w.bs_k = c.take<long long>((size_t)scan_num_blocks(tc) + 1);
     w.tile_count = c.take<int>((size_t)T);
     w.tile_start = c.take<int>((size_t)T + 1);
     w.tile_cursor = c.take<int>((size_t)T);
@@ -126,6 +122,13 @@ static Workspace carve(void* base, int64_t G, int64_t T, int64_t P, int64_t cap)
     w.slot_mask = c.take<blockmask_t>((size_t)cap);
     w.sorted_mask = c.take<blockmask_t>((size_t)cap);
     w.pixel_aux = c.take<float2>((size_t)P);
+    if (tc < 0) tc = task_capacity(cap);
+    w.task_rect = c.take<int4>((size_t)tc);
+    w.task_gf = c.take<int2>((size_t)tc);
+    w.task_v = c.take<float>((size_t)tc);
+    w.task_ntiles = c.take<int>((size_t)tc);
+    w.task_inst = c.take<int>((size_t)tc + 1);
+    w.bs_k = c.take<long long>((size_t)scan_num_blocks(tc) + 1);
     w.bytes = align_up(c.off, 256);
     return w;
 }
@@ -1181,11 +1184,50 @@ static int read_header(const void* workspace, long long hdr[H_WORDS], cudaStream
     return US3D_OK;
 }
 
+namespace us3d {
+namespace ug {
+
+// Workspace bytes with an explicit (Gaussian, frame) task capacity (internal to the library).
+size_t workspace_bytes_with_tasks(int64_t n_gauss, int64_t n_tiles, int64_t n_pixels, int64_t cap, int64_t tc) {
+    if (n_gauss < 0 || n_tiles < 0 || n_pixels < 0 || cap < 0 || tc < 0) return 0;
+    return carve(nullptr, n_gauss, n_tiles, n_pixels, cap, tc).bytes;
+}
+
+// Number of (Gaussian, frame) tasks the last binning of `workspace` found (synchronises).
+int read_task_count(const void* workspace, int64_t* n_tasks, void* stream);
+
+// us3d_ug_bin_ex with an explicit task capacity (tc < 0: task_capacity(cap)). The shading
+// entry points take the same workspace whatever tc was.
+int bin_with_task_capacity(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames, int32_t n_frames,
+                           int64_t n_tiles, int64_t n_pixels, int64_t n_gauss, const float* means, const float* tril,
+                           const float* opac, const float* inten, float chi2, float beta, int32_t sort_by_depth,
+                           int64_t cap, int64_t task_cap, const float* pixels, int32_t flags, void* stream_);
+
+}  // namespace ug
+}  // namespace us3d
+
 extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames,
                               int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
                               const float* means, const float* tril, const float* opac, const float* inten,
                               float chi2, float beta, int32_t sort_by_depth, int64_t cap, const float* pixels,
                               int32_t flags, void* stream_) {
+    return bin_with_task_capacity(workspace, workspace_bytes, frames, n_frames, n_tiles, n_pixels, n_gauss, means,
+                                  tril, opac, inten, chi2, beta, sort_by_depth, cap, -1, pixels, flags, stream_);
+}
+
+int us3d::ug::read_task_count(const void* workspace, int64_t* n_tasks, void* stream) {
+    long long hdr[H_WORDS];
+    int st = read_header(workspace, hdr, (cudaStream_t)stream);
+    if (st != US3D_OK) return st;
+    *n_tasks = hdr[H_NTASK];
+    return US3D_OK;
+}
+
+int us3d::ug::bin_with_task_capacity(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames,
+                                     int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
+                                     const float* means, const float* tril, const float* opac, const float* inten,
+                                     float chi2, float beta, int32_t sort_by_depth, int64_t cap, int64_t task_cap,
+                                     const float* pixels, int32_t flags, void* stream_) {
     int st = check_common(frames, n_frames, n_tiles, n_pixels, n_gauss);
     const int slice_cull = (flags & US3D_UG_BIN_SLICE_CULL) ? 1 : 0;
     US3D_CHECK_ARG((flags & ~(US3D_UG_BIN_SLICE_CULL | US3D_UG_BIN_LOGIT_ATTRIBUTES)) == 0,
@@ -1197,7 +1239,9 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
     US3D_CHECK_ARG(n_gauss == 0 || (means && tril && opac && inten), "Gaussian parameter pointer is NULL");
     US3D_CHECK_ARG((reinterpret_cast<uintptr_t>(tril) & 7) == 0, "precision_tril must be 8-byte aligned");
     US3D_CHECK_ARG(chi2 > 0.f && beta > 0.f, "chi2_threshold and diag_beta must be > 0");
-    const Workspace w = carve(workspace, n_gauss, n_tiles, n_pixels, cap);
+    US3D_CHECK_ARG(task_cap <= 0x7fffffffLL, "task capacity must be below 2^31");
+    const int64_t tc = task_cap < 0 ? task_capacity(cap) : task_cap;
+    const Workspace w = carve(workspace, n_gauss, n_tiles, n_pixels, cap, tc);
     US3D_CHECK_ARG(workspace_bytes >= w.bytes, "workspace too small: %zu < %zu bytes", workspace_bytes, w.bytes);
     cudaStream_t stream = (cudaStream_t)stream_;
 
@@ -1212,7 +1256,6 @@ extern "C" int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3
                                                                     w.tile_dev, w.frame_dev);
     const unsigned* tdev = slice_cull ? w.frame_dev : nullptr;
     const int gb = (int)((n_gauss + 255) / 256);
-    const int64_t tc = task_capacity(cap);
     const unsigned tb = (unsigned)std::min<int64_t>((tc + 127) / 128, 148 * 16);
     if (n_gauss > 0) {
         pack_kernel<<<gb, 256, 0, stream>>>(n_gauss, means, tril, opac, inten,
