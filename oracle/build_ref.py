@@ -11,7 +11,7 @@ covariance.cuh, whose four functions are defined there from the mathematics thei
 sites imply). Two harnesses in ``oracle/ref_harness`` expose internal binning results.
 The reference's setup.py files are not run.
 
-Usage: python oracle/build_ref.py [--reference /path/to/reference]
+Usage: python oracle/build_ref.py [--reference /path/to/reference]  (default: $US3D_REFERENCE)
 """
 
 from __future__ import annotations
@@ -25,7 +25,8 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT_DIR = HERE / "_ref"
 SHIM = HERE / "ref_shim"
-DEFAULT_REFERENCE = Path("/root/reference")
+# The reference checkout: $US3D_REFERENCE, else the path this machine keeps it at.
+DEFAULT_REFERENCE = Path(os.environ.get("US3D_REFERENCE") or "/root/reference")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -9,6 +9,7 @@ tree; usage from the repository root:
 from __future__ import annotations
 
 import argparse
+import os
 import importlib.util
 import sys
 from pathlib import Path
@@ -21,7 +22,9 @@ ROOT = Path(__file__).resolve().parents[2]
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", type=Path, default=Path("/root/reference"))
+    ap.add_argument("--reference", type=Path, default=os.environ.get("US3D_REFERENCE"),
+                    required=not os.environ.get("US3D_REFERENCE"),
+                    help="reference checkout (default: $US3D_REFERENCE)")
     ap.add_argument("--out", type=Path, default=Path(__file__).resolve().parent)
     a = ap.parse_args()
     spec = importlib.util.spec_from_file_location("pipeline_god_file", a.reference / "pipeline_god_file.py")

@@ -13,6 +13,7 @@ callable on their own. Usage from the repository root, where the reference tree 
 from __future__ import annotations
 
 import argparse
+import os
 import importlib.util
 import math
 from pathlib import Path
@@ -100,7 +101,9 @@ def run(adapter, G, seed, st, focal_depth=10.0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", type=Path, default=Path("/root/reference"))
+    ap.add_argument("--reference", type=Path, default=os.environ.get("US3D_REFERENCE"),
+                    required=not os.environ.get("US3D_REFERENCE"),
+                    help="reference checkout (default: $US3D_REFERENCE)")
     ap.add_argument("--out", type=Path, default=HERE)
     a = ap.parse_args()
     adapter = load_adapter(a.reference)

@@ -13,9 +13,14 @@ import torch.nn as nn
 from us3d_b200 import surfel as _gs
 
 
-def cpu_deep_copy_tuple(input_tuple):
-    copied_tensors = [item.cpu().clone() if isinstance(item, torch.Tensor) else item for item in input_tuple]
-    return tuple(copied_tensors)
+def _snapshot_on_host(values):
+    """Host copies of the tensors among ``values`` (detached, never aliasing device or host
+    inputs), other entries passed through: what a debug-mode call saves when it fails."""
+    return tuple(v.detach().to("cpu", copy=True) if torch.is_tensor(v) else v for v in values)
+
+
+# the reference package exports its snapshot helper under this name
+cpu_deep_copy_tuple = _snapshot_on_host
 
 
 def rasterize_gaussians(means3D, means2D, sh, colors_precomp, opacities, scales, rotations, cov3Ds_precomp,
@@ -53,7 +58,7 @@ class _RasterizeGaussians(torch.autograd.Function):
             return out
 
         if s.debug:
-            cpu_args = cpu_deep_copy_tuple(args)
+            cpu_args = _snapshot_on_host(args)
             try:
                 num_rendered, color, depth, radii, state = run()
             except Exception as ex:
@@ -87,7 +92,7 @@ class _RasterizeGaussians(torch.autograd.Function):
                                 s.sh_degree, cam)
 
         if s.debug:
-            cpu_args = cpu_deep_copy_tuple(args[:-1])
+            cpu_args = _snapshot_on_host(args[:-1])
             try:
                 out = run()
             except Exception as ex:
