@@ -44,6 +44,17 @@ NCU_TRAFFIC_PER_FRAME = {
     "ug_backward": (100.252416e6 + 114.988544e6 + 156.020480e6 + 28.401920e6) / 4,
     "ug_forward": (52.274432e6 + 5.454592e6) / 4,
 }
+# Warp instructions executed per frame by each stage's kernels (smsp__inst_executed.sum of the
+# same 4-frame capture, per frame): the shading kernels are bound by instruction issue, whose
+# ceiling is 148 SMs x 4 schedulers x one warp instruction per clock.
+# (per frame, per launch): the per-Gaussian gradient reduction runs once per launch.
+NCU_WARP_INST_PER_FRAME = {
+    "ug_forward": (547342384 / 4, 0.0),
+    "ug_backward": (594881545 / 4, 21e6),
+}
+# Share of cycles the FMA pipe was busy in that capture (sm__pipe_fma_cycles_active).
+NCU_FMA_PIPE = {"ug_forward": 0.5172, "ug_backward": 0.6857}
+SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 
 def parse():
@@ -327,6 +338,7 @@ def run_b200(a):
     step_gbs = b_frame * frames_total / (ms_batched / 1e3) / 1e9
     roofline["step"] = {"bytes_per_frame": int(b_frame), "achieved": round(step_gbs, 2),
                         "frac": round(step_gbs / peak, 4)}
+    roofline["issue"] = issue_roofline(stage_ms, F, clocks)
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -364,6 +376,29 @@ def run_b200(a):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def issue_roofline(stage_ms, frames_per_launch, clocks):
+    """The bound the shading kernels actually meet: warp instructions issued per second
+    against the GPU's issue ceiling (148 SMs x 4 schedulers x 1 warp instruction per clock at
+    the median SM clock sampled during the timed region), per stage, from the instruction
+    counts of the committed ncu capture scaled to the launch's frames and this run's
+    CUDA-event stage times."""
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    ceiling = SM_COUNT * SCHEDULERS_PER_SM * mhz * 1e6  # warp instructions / s
+    out = {"bound": "instruction issue", "unit": "warp inst/s", "sm_mhz": mhz, "peak": ceiling,
+           "source": "smsp__inst_executed.sum per frame of a 4-frame ncu capture (profiles/) x frames per launch "
+                     "/ CUDA-event stage time; peak = 148 SMs x 4 schedulers x median SM clock"}
+    for stage, (per_frame, per_launch) in NCU_WARP_INST_PER_FRAME.items():
+        ms = stage_ms.get(stage)
+        if not ms:
+            continue
+        inst = per_frame * frames_per_launch + per_launch
+        achieved = inst / (ms / 1e3)
+        out[stage] = {"achieved": round(achieved, 1), "frac": round(achieved / ceiling, 4),
+                      "warp_inst_per_launch": int(inst), "stage_ms": round(ms, 4),
+                      "fma_pipe_busy": NCU_FMA_PIPE.get(stage)}
+    return out
 
 
 def measure_train_step(a, params, specs, batches, F, world, timed):
@@ -587,6 +622,63 @@ def cpu_baseline_dense(frames: int = 2):
                       f"CPU fallback (restated) + autograd backward, {dt:.1f} s"}
 
 
+def reference_cuda(a, sc, specs, frames: int = 8, warm: int = 2):
+    """The reference's own UltraGauss CUDA (its sources built for sm_100a into oracle/_ref)
+    on this box's GPU, one frame per call as its pipeline renders: mapper, forward and
+    backward of each frame with an L1 upstream gradient, timed with CUDA events on the
+    current stream (the reference's host synchronisations inside each call included)."""
+    import torch
+
+    ref_dir = ROOT / "oracle" / "_ref"
+    if not torch.cuda.is_available() or not any(ref_dir.glob("ultragauss_ref_C*.so")):
+        return {"unavailable": "no GPU or no reference build in oracle/_ref"}
+    sys.path.insert(0, str(ref_dir))
+    import ultragauss_ref_C as REF
+
+    from us3d_b200 import scenes
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    pad = lambda x: torch.nn.functional.pad(x, (0, 1)).contiguous()  # noqa: E731
+    mp = pad(sc.means.to(dev))
+    tril = sc.precision_tril.to(dev).contiguous()
+    attr = torch.stack([sc.opacities, sc.intensities], 1).to(dev).contiguous()
+    g = torch.Generator().manual_seed(5)
+    inputs = []
+    for s in specs[:max(1, min(frames, len(specs)))]:
+        v = lambda x: torch.as_tensor(x, dtype=torch.float32).to(dev).contiguous()  # noqa: E731
+        pix = scenes.slice_pixels(s.origin, s.axis_lat, s.axis_ax, s.height, s.width, s.lateral_spacing,
+                                  s.axial_spacing, s.axial_near, s.lateral_col_offset)
+        tgt = torch.rand((s.height * s.width,), generator=g).to(dev)
+        inputs.append((s, pad(pix.to(dev)), v(s.origin), v(s.axis_lat), v(s.axis_ax), v(s.axis_ele), tgt))
+
+    def frame(i):
+        s, pp, o, l, ax, e, tgt = inputs[i % len(inputs)]
+        counts, offsets, indices = REF.MapperForwardCUDA(pp, mp, tril, o, l, ax, e, s.height, s.width,
+                                                         s.lateral_spacing, s.axial_spacing, s.axial_near,
+                                                         s.lateral_col_offset, 7.815, True, 1e-4)
+        image, alpha, depth, sic = REF.ShaderForwardCUDA(attr, mp, tril, pp, o, e, offsets, counts, indices, 1e-6,
+                                                         0.0, 7.815, 1e-4)
+        dI = torch.sign(image.reshape(-1) - tgt) / tgt.numel()
+        z = torch.zeros_like(dI)
+        REF.ShaderBackwardCUDA(dI, z, z, attr, mp, tril, pp, o, e, offsets, counts, indices, sic, alpha, 1e-6, 0.0,
+                               7.815, 1e-4)
+
+    for i in range(warm):
+        frame(i)
+    torch.cuda.synchronize()
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st.record()
+    for i in range(frames):
+        frame(i)
+    en.record()
+    en.synchronize()
+    ms = st.elapsed_time(en)
+    return {"value": round(frames / (ms / 1e3), 3), "unit": UNIT, "frames": frames, "ms_per_frame": round(ms / frames, 3),
+            "kind": "the reference's own UltraGauss CUDA (MapperForwardCUDA + ShaderForwardCUDA + ShaderBackwardCUDA), "
+                    "built for sm_100a from its sources, one frame per call, CUDA events on the current stream"}
+
+
 def run_reference(a):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -600,9 +692,7 @@ def run_reference(a):
     sweep = scenes.linear_sweep(max(a.steps + a.warmup, 1), a.size, a.size, a.spacing, seed=0)
     specs = [UG.SliceSpec(f.height, f.width, f.lateral_spacing, f.axial_spacing, f.axial_near, f.lateral_col_offset,
                           f.origin, f.axis_lat, f.axis_ax, f.axis_ele) for f in sweep]
-    for _ in range(a.warmup):
-        pass  # the oracle has no warm-up state; one untimed frame is enough to page code in
-    if a.warmup:
+    if a.warmup:  # the oracle has no warm-up state; one untimed frame pages its code in
         cpu_baseline(a, sc, specs[:1], frames=1)
     times = []
     for i in range(a.steps):
@@ -612,16 +702,42 @@ def run_reference(a):
     cb = {"value": round(value, 5), "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
           "sample": f"{a.steps} step(s) of 1 full frame each ({a.gaussians} Gaussians, {a.size}^2 px): C restatement "
                     "of the reference UltraGauss mapper + forward + backward on all host threads"}
+    # one frame per step: the reference renders one frame per call
+    cfg = workload_config(a, 1)
+    cfg["frames_per_step"] = 1
+    cfg["workload"] = cfg["workload"].replace(f"{a.frames_per_step} frames/step per GPU", "1 frame per step")
     out = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
            "warmup": a.warmup, "ms_per_step": round(1e3 * sum(times) / a.steps, 2), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded headline scene",
-           "config": workload_config(a, 1), "impl": "reference", "cpu_baseline": cb,
+           "config": cfg, "impl": "reference", "cpu_baseline": cb,
            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        out["reference_cuda"] = reference_cuda(a, sc, specs)
+    except Exception as ex:  # the CPU arm stands on its own; say why the GPU number is missing
+        out["reference_cuda"] = {"unavailable": f"{type(ex).__name__}: {ex}"[:300]}
     print(json.dumps(out), flush=True)
+
+
+def relaunch_multi_gpu(a) -> int:
+    """`python bench.py --gpus N` outside a launcher: start N ranks (one per GPU) with
+    torch.distributed.run on this node, each running this script with the same arguments,
+    and return its exit status. Frames are sharded across the ranks (replicas, no collective
+    on the data path); rank 0 prints the line."""
+    import socket
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={a.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.call(cmd)
 
 
 def main():
     a = parse()
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch_multi_gpu(a))
     if a.impl == "reference":
         run_reference(a)
     else:

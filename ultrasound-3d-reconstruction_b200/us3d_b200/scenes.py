@@ -154,3 +154,187 @@ def linear_sweep(n_frames: int, H: int, W: int, spacing_mm: float, seed: int = 0
         pix = slice_pixels(origin, lat0, ax, H, W, spacing_mm, spacing_mm, 0.0, col_off)
         out.append(Slice(H, W, spacing_mm, spacing_mm, 0.0, col_off, origin, lat0.clone(), ax, ele, pix))
     return out
+
+
+def _unit_quaternions(n: int, g: torch.Generator) -> torch.Tensor:
+    q = torch.randn((n, 4), generator=g).double()
+    return q / (q[:, 0] * q[:, 0] + q[:, 1] * q[:, 1] + q[:, 2] * q[:, 2] + q[:, 3] * q[:, 3]).sqrt().clamp_min(1e-12)[:, None]
+
+
+def make_clustered_scene(n: int, seed: int = 0, extent_mm=(100.0, 60.0, 80.0), n_clusters: int = 20,
+                         background: float = 0.1, log_scale_mean: float = math.log(0.8), log_scale_std: float = 0.4,
+                         opacity_mu: float = -1.0, opacity_std: float = 1.0, semi_axes_mm=(3.0, 12.0),
+                         beta: float = 1e-4) -> GaussianScene:
+    """Tissue-like scene: ``n`` Gaussians in a box of ``extent_mm``, a mixture of
+    ``n_clusters`` ellipsoidal clusters plus a fraction ``background`` drawn uniformly in the
+    box. Cluster c has a centre uniform in the inner 80 % of the box, semi-axes U(semi_axes_mm)
+    and a random orientation; its members are uniform inside the ellipsoid (clamped to the
+    box). Per Gaussian: log-scales N(log_scale_mean, log_scale_std), random unit quaternions,
+    intensity U(0,1), opacity sigmoid(N(opacity_mu, opacity_std)).
+
+    Draw order from one generator: cluster centres, semi-axes, orientations; the cluster of
+    every clustered Gaussian; its direction and radius in the unit ball; the background means;
+    then scales, quaternions, intensities and opacities as in make_scene."""
+    g = torch.Generator().manual_seed(seed)
+    ext = torch.tensor(extent_mm, dtype=torch.float64)
+    n_bg = int(round(background * n))
+    n_cl = n - n_bg
+    centres = (0.1 + 0.8 * torch.rand((n_clusters, 3), generator=g).double()) * ext
+    lo, hi = semi_axes_mm
+    semi = lo + (hi - lo) * torch.rand((n_clusters, 3), generator=g).double()
+    rot = quat_to_rot(_unit_quaternions(n_clusters, g))
+    which = torch.randint(0, n_clusters, (n_cl,), generator=g)
+    d = torch.randn((n_cl, 3), generator=g).double()
+    d = d / (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2]).sqrt().clamp_min(1e-12)[:, None]
+    r = torch.rand((n_cl,), generator=g).double().pow(1.0 / 3.0)
+    local = d * r[:, None] * semi[which]
+    Rw = rot[which]  # elementwise products: no batched BLAS, whose rounding can vary between processes
+    pts = centres[which] + torch.stack([Rw[:, i, 0] * local[:, 0] + Rw[:, i, 1] * local[:, 1]
+                                        + Rw[:, i, 2] * local[:, 2] for i in range(3)], dim=1)
+    pts = torch.minimum(torch.maximum(pts, torch.zeros(3, dtype=torch.float64)), ext)
+    bg = torch.rand((n_bg, 3), generator=g).double() * ext
+    means = torch.cat([pts, bg]).float().contiguous()
+    scales64 = torch.exp(log_scale_mean + log_scale_std * torch.randn((n, 3), generator=g).double())
+    q = _unit_quaternions(n, g)
+    intensities = torch.rand((n,), generator=g)
+    opacities = torch.sigmoid(opacity_mu + opacity_std * torch.randn((n,), generator=g).double()).float()
+    tril = precision_tril_from_scales_quats(scales64, q, beta)
+    return GaussianScene(means, scales64.float(), q.float(), opacities, intensities, tril)
+
+
+def _axis_angle(axis: torch.Tensor, angle: float) -> torch.Tensor:
+    """Rotation matrix (float64) about a unit axis (Rodrigues)."""
+    x, y, z = (float(v) for v in axis)
+    K = torch.tensor([[0.0, -z, y], [z, 0.0, -x], [-y, x, 0.0]], dtype=torch.float64)
+    return torch.eye(3, dtype=torch.float64) + math.sin(angle) * K + (1.0 - math.cos(angle)) * (K @ K)
+
+
+def random_walk_sweep(n_frames: int, H: int, W: int, spacing_mm: float, seed: int = 0,
+                      extent_mm=(100.0, 60.0, 80.0), step_mm: float = 1.5, step_deg: float = 1.0) -> List[Slice]:
+    """Freehand-like sweep: the probe pose is a cumulative random walk, each frame moved by
+    ``step_mm`` along a random direction and turned by ``step_deg`` about a random axis
+    (both uniform on the sphere) from the previous one. The first frame stands in the middle
+    of the box: lateral axis x, axial axis y (depth from the box's top face), elevation z,
+    the image centred laterally and its top row ``(extent_y - H * spacing) / 2`` below the
+    top face. Pixel centres as slice_pixels (column offset (W - 1) / 2)."""
+    g = torch.Generator().manual_seed(seed + 2_000_003)
+    ext = torch.tensor(extent_mm, dtype=torch.float64)
+    R = torch.eye(3, dtype=torch.float64)  # columns: lateral, axial, elevational axes
+    depth = H * spacing_mm
+    origin = torch.tensor([ext[0] * 0.5, max(0.0, (float(ext[1]) - depth) * 0.5), ext[2] * 0.5], dtype=torch.float64)
+    col_off = (W - 1) * 0.5
+    out = []
+    for f in range(n_frames):
+        if f > 0:
+            t = torch.randn((3,), generator=g).double()
+            a = torch.randn((3,), generator=g).double()
+            origin = origin + step_mm * t / t.norm().clamp_min(1e-12)
+            R = _axis_angle(a / a.norm().clamp_min(1e-12), math.radians(step_deg)) @ R
+        lat, ax, ele = (R[:, i].float().contiguous() for i in range(3))
+        o = origin.float()
+        pix = slice_pixels(o, lat, ax, H, W, spacing_mm, spacing_mm, 0.0, col_off)
+        out.append(Slice(H, W, spacing_mm, spacing_mm, 0.0, col_off, o, lat, ax, ele, pix))
+    return out
+
+
+# Attenuation of the B-mode workload: 0.5 dB/cm/MHz at 5 MHz, two-way (echo path), i.e.
+# 0.5 dB per mm of depth.
+BMODE_DB_PER_MM = 2.0 * 0.5 * 5.0 / 10.0
+
+
+def bmode_attenuation_logit(n_gauss: int, volume_mm3: float, sigma_mm: float = 1.0, window_mm: float = 2.0,
+                            db_per_mm: float = BMODE_DB_PER_MM) -> float:
+    """Attenuation logit tau_raw of the ray-integral renderer that makes a scene of n_gauss
+    Gaussians in volume_mm3 attenuate like tissue of db_per_mm.
+
+    The renderer multiplies, for every Gaussian a ray has passed, T = tau + (1 - tau) e^-psi,
+    tau = sigmoid(tau_raw), psi the integral of the Gaussian's profile along the ray over its
+    quadrature window. A ray meets on average rho * 2 pi sigma^2 Gaussians of scale sigma per
+    mm of depth (rho = n_gauss / volume_mm3), so each stands for delta = 1 / (rho 2 pi sigma^2)
+    mm of tissue and should transmit T* = 10^(-db_per_mm delta / 20) on a central crossing,
+    where psi0 = sqrt(2 pi) sigma erf(window / (sigma sqrt 2)). Solving for tau gives the
+    logit. It only sets inputs; the renderer's arithmetic is the reference's."""
+    rho = n_gauss / volume_mm3
+    delta = 1.0 / (rho * 2.0 * math.pi * sigma_mm * sigma_mm)
+    t_star = 10.0 ** (-db_per_mm * delta / 20.0)
+    psi0 = math.sqrt(2.0 * math.pi) * sigma_mm * math.erf(window_mm / (sigma_mm * math.sqrt(2.0)))
+    e0 = math.exp(-psi0)
+    tau = (t_star - e0) / (1.0 - e0)
+    return math.log(tau / (1.0 - tau))
+
+
+@dataclass
+class BModeScene:
+    means: torch.Tensor        # (G,3)
+    scales: torch.Tensor       # (G,3)
+    quats: torch.Tensor        # (G,4) wxyz, unit
+    attenuations: torch.Tensor  # (G,) logits
+    sh: torch.Tensor           # (G,4) degree-1 echo coefficients (reflectivity c0, c1..c3)
+
+    def to(self, device) -> "BModeScene":
+        return BModeScene(*(getattr(self, f).to(device) for f in ("means", "scales", "quats", "attenuations", "sh")))
+
+
+def make_bmode_scene(n: int, seed: int = 0, aperture_mm: float = 40.0, depth_mm: float = 60.0,
+                     sweep_mm: float = 64.0, log_scale_mean: float = 0.0, log_scale_std: float = 0.3,
+                     strong_fraction: float = 0.05, window_mm: float = 2.0) -> BModeScene:
+    """Scene of the ray-integral B-mode workload: n Gaussians uniform in a box of
+    aperture_mm (lateral, x) x depth_mm (axial, y) x sweep_mm (elevation, z); per-axis
+    log-scales N(log_scale_mean, log_scale_std) (1 mm median), random unit quaternions;
+    reflectivity c0 ~ U(0, 1) with a fraction strong_fraction of strong reflectors U(5, 10),
+    c1..c3 = 0; attenuation logits from bmode_attenuation_logit (0.5 dB/cm/MHz at 5 MHz).
+    Draw order: means, log-scales, quaternions, reflectivity, strong-reflector choice and value."""
+    g = torch.Generator().manual_seed(seed)
+    ext = torch.tensor([aperture_mm, depth_mm, sweep_mm])
+    means = torch.rand((n, 3), generator=g) * ext
+    scales64 = torch.exp(log_scale_mean + log_scale_std * torch.randn((n, 3), generator=g).double())
+    q = _unit_quaternions(n, g)
+    refl = torch.rand((n,), generator=g)
+    strong = torch.rand((n,), generator=g) < strong_fraction
+    strong_val = 5.0 + 5.0 * torch.rand((n,), generator=g)
+    refl = torch.where(strong, strong_val, refl)
+    sh = torch.zeros((n, 4))
+    sh[:, 0] = refl
+    logit = bmode_attenuation_logit(n, float(ext.prod()), sigma_mm=math.exp(log_scale_mean), window_mm=window_mm)
+    att = torch.full((n,), logit, dtype=torch.float32)
+    return BModeScene(means.contiguous(), scales64.float(), q.float(), att, sh)
+
+
+@dataclass
+class ScanlineFrame:
+    """One B-mode frame of a linear array: W scanlines of H samples."""
+    origin: torch.Tensor      # (3,) probe origin (centre of the array face)
+    axis_lat: torch.Tensor
+    axis_ax: torch.Tensor
+    axis_ele: torch.Tensor
+    width_mm: float           # aperture
+    depth_mm: float
+    ray_origins: torch.Tensor  # (W,3)
+    ray_dirs: torch.Tensor     # (W,3)
+    pixels: torch.Tensor       # (W,H,3) sample positions, ray-major
+    col_offset: float
+
+
+def bmode_sweep(n_frames: int, W: int = 512, H: int = 1024, aperture_mm: float = 40.0, depth_mm: float = 60.0,
+                sweep_mm: float = 64.0) -> List[ScanlineFrame]:
+    """Linear array translated along the elevational axis through the box of make_bmode_scene
+    (frames evenly spaced over sweep_mm): lateral axis x, axial axis y (depth), elevation z;
+    scanline x at lateral offset (x - (W-1)/2) * aperture / W from the array centre, samples
+    at depths (y + 0.5) * depth / H."""
+    out = []
+    lat = torch.tensor([1.0, 0.0, 0.0])
+    ax = torch.tensor([0.0, 1.0, 0.0])
+    ele = torch.tensor([0.0, 0.0, 1.0])
+    col_off = (W - 1) * 0.5
+    spacing = aperture_mm / W
+    xs = (torch.arange(W, dtype=torch.float64) - col_off) * spacing
+    zs = (torch.arange(H, dtype=torch.float64) + 0.5) * (depth_mm / H)
+    for f in range(n_frames):
+        z = (f + 0.5) * sweep_mm / n_frames
+        o = torch.tensor([aperture_mm * 0.5, 0.0, z], dtype=torch.float64)
+        ro = o[None, :] + xs[:, None] * lat.double()[None, :]
+        pix = ro[:, None, :] + zs[None, :, None] * ax.double()[None, None, :]
+        out.append(ScanlineFrame(o.float(), lat.clone(), ax.clone(), ele.clone(), aperture_mm, depth_mm,
+                                 ro.float().contiguous(), ax.repeat(W, 1).contiguous(), pix.float().contiguous(),
+                                 col_off))
+    return out
