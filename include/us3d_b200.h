@@ -576,11 +576,16 @@ US3D_API int us3d_gs_mark_visible(int64_t n_gauss, const float* means3D, const f
  * it runs). Does us3d_ug_bin + us3d_ug_forward with the workspace taken from one
  * file-scope device array of US3D_UG_NOALLOC_BYTES bytes that every GPU loading this
  * library holds until exit. Sizes whose workspace does not fit are rejected
- * (US3D_INVALID_ARG); an instance total beyond what fits returns US3D_CAPACITY_OVERFLOW.
- * SYNCHRONISES `stream` once (to read the instance total, also returned in
- * *out_instances if not NULL). The first call on a device resolves the array's address
- * and should come before any stream capture on that device. All calls on a device share
- * the array and keep the last call's contents there: calls that overlap on one GPU race.
+ * (US3D_INVALID_ARG) before anything is launched. The rest of the array is split between
+ * (Gaussian, frame) pairs surviving the cull and (tile, Gaussian) instances; more of
+ * either than fits returns US3D_CAPACITY_OVERFLOW and writes no output. SYNCHRONISES
+ * `stream` once (twice on an overflow) to read the instance total, also returned in
+ * *out_instances if not NULL; when the surviving pairs overflowed first, the instances
+ * were not counted and *out_instances is the number of pairs, a lower bound of the
+ * instance total. The first call on a device resolves the array's address and should
+ * come before any stream capture on that device (a call failing with US3D_CUDA_ERROR
+ * forgets it, so the next call resolves it again). All calls on a device share the array
+ * and keep the last call's contents there: calls that overlap on one GPU race.
  */
 #define US3D_UG_NOALLOC_BYTES (32 * 1024 * 1024)
 US3D_API int us3d_ug_render_noalloc(const us3d_slice_frame* frames_dev, int32_t n_frames, int64_t n_tiles,
