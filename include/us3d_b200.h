@@ -371,16 +371,21 @@ US3D_API int us3d_gp_read_status(const void* workspace, int64_t* total_instances
                                  void* stream);
 
 /* Backward: gradients w.r.t. means (G,3), scales (G,3), quats (G,4), opacities,
- * intensities and, if pose_grad, the pose (4x4). Scale and quaternion gradients are the
- * reference's central differences (step 1e-3) of the footprint/adjoint dot product;
- * gradients are NaN-sanitised and clamped to +-1e3 as in the reference. Deterministic.
+ * intensities and, with US3D_GP_GRAD_POSE in grad_flags, the pose (4x4). Scale and
+ * quaternion gradients are, by default, the reference's central differences (step 1e-3) of
+ * the footprint/adjoint dot product; with US3D_GP_GRAD_SHAPE_ANALYTIC they are the exact
+ * derivative instead (the probe-frame covariance adjoint carried through R diag(s^2) R^T
+ * and the quaternion normalisation; no counterpart in the reference). Gradients are
+ * NaN-sanitised and clamped to +-1e3 as in the reference. Deterministic.
  * Replaces ProjectedSliceBackwardCUDA (wrapper_shader.cu:218-416; kernels
  * src/shader/us_focus.cu:479-966). */
+#define US3D_GP_GRAD_POSE 1
+#define US3D_GP_GRAD_SHAPE_ANALYTIC 2
 US3D_API int us3d_gp_backward(void* workspace, int64_t n_gauss, const float* means, const float* scales,
                               const float* quats, const float* opacities, const float* intensities,
                               const float* pose, const float* grid_pack, const float* focus_params,
                               int32_t height, int32_t width, int32_t tile_size, float k_sigma,
-                              int64_t instance_capacity, const float* grad_image, int32_t pose_grad,
+                              int64_t instance_capacity, const float* grad_image, int32_t grad_flags,
                               void* scratch, size_t scratch_bytes, float* d_means, float* d_scales,
                               float* d_quats, float* d_opacities, float* d_intensities, float* d_pose,
                               void* stream);

@@ -680,6 +680,76 @@ __device__ float shape_fd(const float* m, const float* s, const float* q, bool i
     return (lp - lm) / (2.f * eps);
 }
 
+// Exact shape gradient (analytic mode; the reference has only the central differences
+// above): the adjoint of the probe-frame covariance, g_Sc (from the same chain through Se and
+// Lc that gives the mean and pose gradients), is carried back through
+// Sc = A^T Sigma_w A + 1e-6 I, Sigma_w = R diag(s^2) R^T and R = rot(q / |q|):
+//   dL/dSigma_w = sum_ij g_Sc[i][j] a_i a_j^T, dL/ds_k = 2 s_k (R^T G R)_kk (0 where the
+//   1e-6 floor of the scale is active), dL/dR = (G + G^T) R diag(s^2), and dL/dq through the
+//   rotation of the normalised quaternion and the normalisation.
+__device__ void shape_analytic(const float* s, const float* q, const Axes& A, const float g_Sc[9], float d_s[3],
+                               float d_q[4]) {
+    const float3 ax[3] = {A.lat, A.ax, A.ele};
+    float G[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float acc = 0.f;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const float ai = r == 0 ? ax[i].x : (r == 1 ? ax[i].y : ax[i].z);
+                    const float aj = c == 0 ? ax[j].x : (c == 1 ? ax[j].y : ax[j].z);
+                    acc += g_Sc[i * 3 + j] * ai * aj;
+                }
+            G[r * 3 + c] = acc;
+        }
+    float R[9];
+    quat_rot(q[0], q[1], q[2], q[3], R);
+    const float sv[3] = {s[0], s[1], s[2]};
+    float D[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float sk = fmaxf(sv[k], 1e-6f);
+        D[k] = sk * sk;
+        float rgr = 0.f;  // (R^T G R)_kk
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) rgr += R[a * 3 + k] * G[a * 3 + b] * R[b * 3 + k];
+        d_s[k] = sv[k] > 1e-6f ? 2.f * sk * rgr : 0.f;
+    }
+    float gR[9];  // dL/dR = (G + G^T) R D
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float acc = 0.f;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) acc += (G[a * 3 + b] + G[b * 3 + a]) * R[b * 3 + k];
+            gR[a * 3 + k] = acc * D[k];
+        }
+    // R of the unit quaternion (w, x, y, z) as in quat_rot; derivative per component
+    const float n2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    const float nq = rsqrtf(fmaxf(1e-12f, n2));
+    const float w = q[0] * nq, x = q[1] * nq, y = q[2] * nq, z = q[3] * nq;
+    const float gw = 2.f * (-z * gR[1] + y * gR[2] + z * gR[3] - x * gR[5] - y * gR[6] + x * gR[7]);
+    const float gx = 2.f * (y * gR[1] + z * gR[2] + y * gR[3] - 2.f * x * gR[4] - w * gR[5] + z * gR[6] + w * gR[7] -
+                            2.f * x * gR[8]);
+    const float gy = 2.f * (-2.f * y * gR[0] + x * gR[1] + w * gR[2] + x * gR[3] + z * gR[5] - w * gR[6] + z * gR[7] -
+                            2.f * y * gR[8]);
+    const float gz = 2.f * (-2.f * z * gR[0] - w * gR[1] + x * gR[2] + w * gR[3] - 2.f * z * gR[4] + y * gR[5] +
+                            x * gR[6] + y * gR[7]);
+    // through the normalisation u = q / |q| (no normalisation term where the 1e-12 floor is active)
+    const float dot = (n2 > 1e-12f) ? (w * gw + x * gx + y * gy + z * gz) : 0.f;
+    d_q[0] = nq * (gw - w * dot);
+    d_q[1] = nq * (gx - x * dot);
+    d_q[2] = nq * (gy - y * dot);
+    d_q[3] = nq * (gz - z * dot);
+}
+
 __device__ __forceinline__ float3 normalize3_bwd(const float3 raw, const float3 n, const float3 g) {
     const float len = sqrtf(fmaxf(1e-12f, f3_dot(raw, raw)));
     const float il = 1.f / len;
@@ -695,7 +765,7 @@ finalize_kernel(int64_t G, float k_sigma, const int* __restrict__ inst_offset, c
                 const float* __restrict__ means, const float* __restrict__ scales, const float* __restrict__ quats,
                 const float* __restrict__ pose, const float* __restrict__ grid, const float* __restrict__ params,
                 const long long* __restrict__ header, const float* __restrict__ partial, int pose_grad,
-                float* __restrict__ d_means, float* __restrict__ d_scales, float* __restrict__ d_quats,
+                int shape_analytic_mode, float* __restrict__ d_means, float* __restrict__ d_scales, float* __restrict__ d_quats,
                 float* __restrict__ d_opac, float* __restrict__ d_inten, float* __restrict__ pose_partial) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
@@ -787,10 +857,17 @@ finalize_kernel(int64_t G, float k_sigma, const int* __restrict__ inst_offset, c
     d_opac[g] = sanitize(acc[P_OPACITY]);
     const FpAdjoint adj = {acc[P_FP_MU2_LAT], acc[P_FP_MU2_AX], acc[P_FP_INV00], acc[P_FP_INV01], acc[P_FP_INV11],
                            acc[P_FP_DET2], acc[P_FP_MU_ELE], acc[P_FP_SC22], acc[P_FP_SIGMA_ELE]};
-    for (int k = 0; k < 3; ++k)
-        d_scales[3 * g + k] = sanitize(shape_fd(m, s, q, false, k, 1e-3f, A, near_mm, k_sigma, params, adj));
-    for (int k = 0; k < 4; ++k)
-        d_quats[4 * g + k] = sanitize(shape_fd(m, s, q, true, k, 1e-3f, A, near_mm, k_sigma, params, adj));
+    if (shape_analytic_mode) {
+        float ds[3], dq[4];
+        shape_analytic(s, q, A, g_Sc, ds, dq);
+        for (int k = 0; k < 3; ++k) d_scales[3 * g + k] = sanitize(ds[k]);
+        for (int k = 0; k < 4; ++k) d_quats[4 * g + k] = sanitize(dq[k]);
+    } else {
+        for (int k = 0; k < 3; ++k)
+            d_scales[3 * g + k] = sanitize(shape_fd(m, s, q, false, k, 1e-3f, A, near_mm, k_sigma, params, adj));
+        for (int k = 0; k < 4; ++k)
+            d_quats[4 * g + k] = sanitize(shape_fd(m, s, q, true, k, 1e-3f, A, near_mm, k_sigma, params, adj));
+    }
     const float3 g_delta = make_float3(g_mu_probe[0] * A.lat.x + g_mu_probe[1] * A.ax.x + g_mu_probe[2] * A.ele.x,
                                        g_mu_probe[0] * A.lat.y + g_mu_probe[1] * A.ax.y + g_mu_probe[2] * A.ele.y,
                                        g_mu_probe[0] * A.lat.z + g_mu_probe[1] * A.ax.z + g_mu_probe[2] * A.ele.z);
@@ -989,9 +1066,13 @@ extern "C" int us3d_gp_backward(void* workspace, int64_t n_gauss, const float* m
                                 const float* quats, const float* opacities, const float* intensities,
                                 const float* pose, const float* grid_pack, const float* focus_params, int32_t H,
                                 int32_t W, int32_t tile_size, float k_sigma, int64_t cap, const float* grad_image,
-                                int32_t pose_grad, void* scratch, size_t scratch_bytes, float* d_means,
+                                int32_t grad_flags, void* scratch, size_t scratch_bytes, float* d_means,
                                 float* d_scales, float* d_quats, float* d_opacities, float* d_intensities,
                                 float* d_pose, void* stream_) {
+    US3D_CHECK_ARG((grad_flags & ~(US3D_GP_GRAD_POSE | US3D_GP_GRAD_SHAPE_ANALYTIC)) == 0,
+                   "unknown gradient flags 0x%x", (unsigned)grad_flags);
+    const int pose_grad = (grad_flags & US3D_GP_GRAD_POSE) ? 1 : 0;
+    const int shape_analytic_mode = (grad_flags & US3D_GP_GRAD_SHAPE_ANALYTIC) ? 1 : 0;
     int tx, ty;
     int st = gp_sizes(H, W, tile_size, &tx, &ty);
     if (st != US3D_OK) return st;
@@ -1020,7 +1101,8 @@ extern "C" int us3d_gp_backward(void* workspace, int64_t n_gauss, const float* m
     if (n_gauss > 0) {
         finalize_kernel<<<(unsigned)((n_gauss + 127) / 128), 128, 0, stream>>>(
             n_gauss, k_sigma, w.inst_offset, w.rects, means, scales, quats, pose, grid_pack, focus_params, w.header,
-            partial, pose_grad, d_means, d_scales, d_quats, d_opacities, d_intensities, pose_partial);
+            partial, pose_grad, shape_analytic_mode, d_means, d_scales, d_quats, d_opacities, d_intensities,
+            pose_partial);
         US3D_CHECK_LAUNCH("gp finalize");
         ++launches;
     }

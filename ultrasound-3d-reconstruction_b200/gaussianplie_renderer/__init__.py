@@ -5,6 +5,7 @@ __init__.py:1-27).
 """
 
 from .api import GaussianPlieRenderer
+from .autograd import SHAPE_GRADIENTS, get_shape_gradients, set_shape_gradients
 from .check import should_validate_inputs, validate_render_inputs
 from .grid_geometry import build_slice_grid_pack
 from .reference import build_covariance, focus_project, quat_to_matrix_wxyz, render_reference, world_to_camera
@@ -14,6 +15,9 @@ GAUSSIANPLIE_RENDERER_TAG = "gaussianplie_single_alpha_v2"
 
 __all__ = [
     "GAUSSIANPLIE_RENDERER_TAG",
+    "SHAPE_GRADIENTS",
+    "get_shape_gradients",
+    "set_shape_gradients",
     "GaussianPlieRenderer",
     "GaussianPlieRenderConfig",
     "build_covariance",

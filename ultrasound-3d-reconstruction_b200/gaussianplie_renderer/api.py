@@ -19,6 +19,9 @@ class GaussianPlieRenderer(nn.Module):
         self.config = config
         self._slice_grid_geometry = None
         self._delegate = None
+        # "finite_difference" (the reference's scale / quaternion gradients), "analytic" (their
+        # exact derivative) or None (the process-wide default, set_shape_gradients)
+        self.shape_gradients = None
 
     def _ensure_delegate(self):
         if self._delegate is None and self.config.backend == "ultragauss_lowmem":
@@ -74,7 +77,8 @@ class GaussianPlieRenderer(nn.Module):
         if self._slice_grid_geometry is None:
             raise RuntimeError("GaussianPlieRenderer requires slice_grid_geometry; call set_slice_grid_geometry().")
         return render_gaussianpile_projected_slice(self.config, gauss_means, gauss_scales, gauss_quats, gauss_alphas,
-                                                   pose_probe_to_world, self._slice_grid_geometry)
+                                                   pose_probe_to_world, self._slice_grid_geometry,
+                                                   shape_gradients=self.shape_gradients)
 
     def set_slice_grid_geometry(self, slice_grid_geometry: torch.Tensor) -> None:
         self._slice_grid_geometry = slice_grid_geometry

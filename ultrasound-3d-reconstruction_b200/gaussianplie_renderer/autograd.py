@@ -46,12 +46,34 @@ def _us_focus_params_vector(config: GaussianPlieRenderConfig, device: torch.devi
     return torch.tensor(vals, dtype=torch.float32, device=device)
 
 
+# How scale and quaternion gradients are formed: "finite_difference" is the reference's
+# central difference (step 1e-3) of the footprint/adjoint dot product; "analytic" is its exact
+# derivative (no counterpart in the reference), which a caller optimising shapes may prefer.
+SHAPE_GRADIENTS = _gp.SHAPE_GRADIENTS
+_default_shape_gradients = "finite_difference"
+
+
+def set_shape_gradients(mode: str) -> None:
+    """Process-wide default for renderers whose ``shape_gradients`` attribute is None."""
+    global _default_shape_gradients
+    if mode not in SHAPE_GRADIENTS:
+        raise ValueError(f"shape_gradients must be one of {SHAPE_GRADIENTS}, got {mode!r}")
+    _default_shape_gradients = mode
+
+
+def get_shape_gradients() -> str:
+    return _default_shape_gradients
+
+
 class _GaussianPileProjectedSliceCudaFunction(torch.autograd.Function):
-    """Same inputs as the reference function of this name (autograd.py:58-137)."""
+    """Same inputs as the reference function of this name (autograd.py:58-137), plus an
+    optional tenth: the shape-gradient mode (default: the process-wide setting)."""
 
     @staticmethod
     def forward(ctx, gauss_means, gauss_scales, gauss_quats, gauss_opacities, gauss_intensities,
-                pose_probe_to_world, slice_grid_geometry, meta, us_focus_params):
+                pose_probe_to_world, slice_grid_geometry, meta, us_focus_params, shape_gradients=None):
+        ctx.shape_gradients = shape_gradients or _default_shape_gradients
+        ctx.mode_given = shape_gradients is not None
         if not gauss_means.is_cuda:
             raise RuntimeError("gaussianplie_renderer requires CUDA tensors: the B200 kernels are the only compute path")
         dev = gauss_means.device
@@ -81,23 +103,26 @@ class _GaussianPileProjectedSliceCudaFunction(torch.autograd.Function):
         b = ctx.b
         if grad_colors_hw is None:
             grad_colors_hw = torch.zeros((b.H, b.W), device=b.workspace.device)
-        dm, ds, dq, do, di, dp = _gp.backward(b, grad_colors_hw, bool(ctx.needs_input_grad[5]))
+        dm, ds, dq, do, di, dp = _gp.backward(b, grad_colors_hw, bool(ctx.needs_input_grad[5]),
+                                              shape_gradients=ctx.shape_gradients)
         grid, meta, params = ctx.aux_shapes
         md, sd, qd, od, idt = ctx.dtypes
-        return (dm.to(md), ds.to(sd), dq.to(qd), do.reshape(ctx.shapes[0]).to(od), di.reshape(ctx.shapes[1]).to(idt),
-                dp.to(ctx.pose_dtype), torch.zeros_like(grid), torch.zeros_like(meta), torch.zeros_like(params))
+        grads = (dm.to(md), ds.to(sd), dq.to(qd), do.reshape(ctx.shapes[0]).to(od), di.reshape(ctx.shapes[1]).to(idt),
+                 dp.to(ctx.pose_dtype), torch.zeros_like(grid), torch.zeros_like(meta), torch.zeros_like(params))
+        return grads + (None,) if ctx.mode_given else grads
 
 
 def render_gaussianpile_projected_slice(config: GaussianPlieRenderConfig, gauss_means: torch.Tensor,
                                         gauss_scales: torch.Tensor, gauss_quats: torch.Tensor,
                                         gauss_alphas: torch.Tensor, pose_probe_to_world: torch.Tensor,
-                                        slice_grid_geometry: torch.Tensor) -> torch.Tensor:
+                                        slice_grid_geometry: torch.Tensor, shape_gradients=None) -> torch.Tensor:
     """(H, W) additive image; intensities are fixed to one, as in the reference
-    (autograd.py:218-246)."""
+    (autograd.py:218-246). ``shape_gradients`` ("finite_difference" / "analytic", None: the
+    process-wide default) chooses how the backward forms scale and quaternion gradients."""
     if not gauss_means.is_cuda:
         raise RuntimeError("GaussianPile requires CUDA tensors; the B200 kernels are the only compute path.")
     device = gauss_means.device
     return _GaussianPileProjectedSliceCudaFunction.apply(
         gauss_means, gauss_scales, gauss_quats, gauss_alphas, torch.ones_like(gauss_alphas), pose_probe_to_world,
         slice_grid_geometry.to(device=device, dtype=torch.float32), _meta_vector(config, device),
-        _us_focus_params_vector(config, device))
+        _us_focus_params_vector(config, device), shape_gradients)

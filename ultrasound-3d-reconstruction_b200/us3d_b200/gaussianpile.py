@@ -61,8 +61,19 @@ def forward(means, scales, quats, opac, inten, pose, grid, params, H, W, lateral
     raise RuntimeError("us3d_gp_forward: capacity retry failed")
 
 
-def backward(b: GPBinning, grad_image: torch.Tensor, pose_grad: bool = False):
-    """(d_means, d_scales, d_quats, d_opacity, d_intensity, d_pose)."""
+GRAD_POSE = 1
+GRAD_SHAPE_ANALYTIC = 2
+SHAPE_GRADIENTS = ("finite_difference", "analytic")
+
+
+def backward(b: GPBinning, grad_image: torch.Tensor, pose_grad: bool = False,
+             shape_gradients: str = "finite_difference"):
+    """(d_means, d_scales, d_quats, d_opacity, d_intensity, d_pose). ``shape_gradients``:
+    "finite_difference" gives the reference's central differences (step 1e-3) for scales and
+    quaternions, "analytic" their exact derivative."""
+    if shape_gradients not in SHAPE_GRADIENTS:
+        raise ValueError(f"shape_gradients must be one of {SHAPE_GRADIENTS}, got {shape_gradients!r}")
+    flags = (GRAD_POSE if pose_grad else 0) | (GRAD_SHAPE_ANALYTIC if shape_gradients == "analytic" else 0)
     means, scales, quats, opac, inten, pose, grid, params = b.tensors
     G = b.n_gauss
     dev = means.device
@@ -76,7 +87,7 @@ def backward(b: GPBinning, grad_image: torch.Tensor, pose_grad: bool = False):
     dp = torch.zeros((4, 4), dtype=torch.float32, device=dev)
     gi = grad_image.reshape(-1).contiguous().float()
     st = _lib.call("us3d_gp_backward", b.workspace.data_ptr(), G, *(t.data_ptr() for t in b.tensors), b.H, b.W, b.tile,
-                   b.k_sigma, b.capacity, gi.data_ptr(), int(bool(pose_grad)), scratch.data_ptr(), scratch.numel(),
+                   b.k_sigma, b.capacity, gi.data_ptr(), flags, scratch.data_ptr(), scratch.numel(),
                    dm.data_ptr(), ds.data_ptr(), dq.data_ptr(), do.data_ptr(), di.data_ptr(), dp.data_ptr(), _stream())
     _lib.check(st, "us3d_gp_backward")
     return dm, ds, dq, do, di, dp
