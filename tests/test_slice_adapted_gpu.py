@@ -97,3 +97,106 @@ def test_slice_adapted_oracle_and_api(cuda_device):
     assert img.shape == (H * W, 3) and alpha.shape == (H * W, 1)
     ((img * torch.as_tensor(fx["grad_image"]).to(dev)).sum() + (alpha * torch.as_tensor(fx["grad_alpha"]).to(dev)).sum()).backward()
     assert rel_l2(ps[0].grad.cpu().numpy(), fx["ref_d_means"]) <= 1e-4
+
+
+def _fd_check(loss, base, analytic, names, h=1e-4, picks=24, seed=0, tol=1e-4):
+    """Central differences (step h, FP64) of loss(*base) against the GPU adjoint for a random
+    sample of each parameter array; a pick whose differences at h and at h/8 disagree (the
+    step crossed a cut of the forward) is left out."""
+    rng = np.random.default_rng(seed)
+    for which, name in enumerate(names):
+        arr = base[which]
+        idx = rng.choice(arr.size, size=min(picks, arr.size), replace=False)
+        fd, an = [], []
+        for fi in idx:
+            d = []
+            for step in (h, h / 8):
+                plus = [b.copy() for b in base]
+                minus = [b.copy() for b in base]
+                plus[which].reshape(-1)[fi] += step
+                minus[which].reshape(-1)[fi] -= step
+                d.append((loss(*plus) - loss(*minus)) / (2 * step))
+            if abs(d[0] - d[1]) > 1e-3 * max(abs(d[0]), 1e-8):
+                continue
+            fd.append(d[0])
+            an.append(analytic[which].reshape(-1)[fi])
+        assert len(fd) >= min(picks, arr.size) * 2 // 3, (name, len(fd))
+        e = rel_l2(np.array(an), np.array(fd))
+        assert e <= tol, (name, e)
+
+
+def test_slice_adapted_gradients_fd64(cuda_device):
+    """The bounded splat's GPU backward against central differences (step 1e-4) of the FP64
+    oracle's image and alpha, on a small case with a 9-sigma cut-off (the box and the
+    q <= r^2 test then change the image by less than 1e-17)."""
+    from oracle import slice_adapted_oracle as SO
+
+    H, W, hw, hh, rs = 40, 48, 6.0, 5.0, 9.0
+    g = torch.Generator().manual_seed(17)
+    N = 150
+    means = torch.stack([(torch.rand(N, generator=g) * 2 - 1) * hw, (torch.rand(N, generator=g) * 2 - 1) * hh], 1)
+    ang = torch.rand(N, generator=g) * np.pi
+    sd = torch.exp(torch.randn(N, 2, generator=g) * 0.3) * 0.5
+    c, s = torch.cos(ang), torch.sin(ang)
+    R = torch.stack([torch.stack([c, -s], -1), torch.stack([s, c], -1)], -2)
+    inv = torch.linalg.inv(R @ torch.diag_embed(sd * sd) @ R.transpose(1, 2))
+    weights = torch.rand(N, 1, generator=g) * 0.5 + 0.1
+    colors = torch.rand(N, 3, generator=g)
+    gi = torch.randn(H * W, 3, generator=g)
+    ga = 0.3 * torch.randn(H * W, 1, generator=g)
+    fx = dict(H=H, W=W, half_width=np.float32(hw), half_height=np.float32(hh), radius_sigma=np.float32(rs),
+              means2d=means.float().numpy(), inv2d=inv.float().numpy(), weights=weights.float().numpy(),
+              colors=colors.float().numpy(), grad_image=gi.numpy(), grad_alpha=ga.numpy())
+    out = run_b200_sa(fx, cuda_device)
+    wi, wa = gi.double().numpy(), ga.double().numpy()
+
+    def loss(m, iv, w, col):
+        st = SO.render(H, W, hw, hh, m, iv, w, col, rs, precision="f64")
+        return float((st["image"].reshape(-1, 3) * wi).sum() + (st["alpha"].reshape(-1, 1) * wa).sum())
+
+    base = [fx[k].astype(np.float64) for k in ("means2d", "inv2d", "weights", "colors")]
+    _fd_check(loss, base, [out["d_means"], out["d_inv"], out["d_weights"], out["d_colors"]],
+              ("d_means", "d_inv", "d_weights", "d_colors"))
+
+
+def test_slice_projection_gradients_fd64(cuda_device):
+    """The fused slice projection's GPU VJP (3D means, scales, quaternions, opacities, colours)
+    against central differences (step 1e-4, FP64) of the numpy restatement of the adapter's
+    projection, for a seeded linear functional of its kept outputs (the kept set is checked to
+    stay fixed under every step)."""
+    from oracle import slice_projection_oracle as PO
+    from us3d_b200 import slice_adapted as SA
+
+    g = torch.Generator().manual_seed(23)
+    G = 80
+    means = (torch.rand(G, 3, generator=g) - 0.5) * torch.tensor([20.0, 16.0, 1.0])
+    scales = torch.exp(torch.randn(G, 3, generator=g) * 0.3) * 0.8
+    quats = torch.randn(G, 4, generator=g)
+    opac = torch.rand(G, 1, generator=g) * 0.8 + 0.1
+    colors = torch.rand(G, 3, generator=g)
+    V = torch.eye(4)
+    st = SA.ProjectionSettings(focal_depth=0.0, slice_thickness=0.3, cull_std=3.0, thickness_scale=1.0,
+                               min_covariance=1e-4, normalize_by_footprint=True)
+    dev = cuda_device
+    t = [x.float().contiguous().to(dev) for x in (means, scales, quats, opac, colors)]
+    m2, inv2, w2, c2, keep_idx, keep = SA.project(*t, V.to(dev), st)
+    n = keep_idx.shape[0]
+    assert 0 < n < G
+    wm = torch.randn(n, 2, generator=g)
+    wi = torch.randn(n, 2, 2, generator=g)
+    ww = torch.randn(n, 1, generator=g)
+    wc = torch.randn(n, 3, generator=g)
+    grads = SA.project_backward(keep_idx, t[0], t[1], t[2], t[3].reshape(-1), V.to(dev), st, wm.to(dev), wi.to(dev),
+                                ww.to(dev), wc.to(dev))
+    kept = keep_idx.cpu().numpy()
+
+    def loss(mm, ss, qq, oo, cc):
+        pr = PO.project(mm, ss, qq, oo, cc, V.numpy(), 0.0, 0.3, 3.0, 1.0, 1e-4, True)
+        assert np.array_equal(np.nonzero(pr["keep"])[0], kept)
+        return float((pr["means2d"] * wm.double().numpy()).sum() + (pr["inv2d"] * wi.double().numpy()).sum()
+                     + (pr["weights"] * ww.double().numpy()).sum() + (pr["colors"] * wc.double().numpy()).sum())
+
+    base = [x.double().numpy() for x in (means, scales, quats, opac, colors)]
+    an = [x.cpu().numpy() for x in grads]
+    _fd_check(loss, base, [an[0], an[1], an[2], an[3].reshape(-1, 1), an[4]],
+              ("d_means", "d_scales", "d_quats", "d_opacities", "d_colors"))

@@ -146,3 +146,53 @@ def test_dropin_rasterizer_autograd(cuda_device):
     pc = (scene["viewmatrix"].astype(np.float64).T @ np.c_[scene["means"], np.ones(len(scene["means"]))].T)[2]
     clear = np.abs(pc - 0.2) > 1e-5
     np.testing.assert_array_equal(vis[clear], (pc > 0.2)[clear])
+
+
+def test_ultrags_gradients_fd64(cuda_device):
+    """The surfel rasteriser's GPU backward against central differences (step 1e-4) of the
+    FP64 oracle's colour image, for the parameters whose reference gradient is the derivative
+    of its forward (3D means, scales, rotations, opacities, degree-0 SH; the screen-space
+    means2D gradient is the reference's densification statistic, not a derivative). A pick
+    whose differences at h and h/8 disagree crossed one of the forward's cuts (the alpha
+    threshold 1/255, the bounding box, the 0.99 clamp) and is left out."""
+    import math
+
+    from oracle import surfel_oracle as SO
+
+    # tan(fov / 2) = 0.5 and a square image: the image size the backward recovers from the
+    # focal length, int(focal * tan_fov * 2), is then exactly the forward's
+    scene = make_scene(40, 48, 48, 31, sh_degree=0, scale_range=(0.08, 0.3), fovx_deg=math.degrees(2 * math.atan(0.5)))
+    scene["grad_others"] = np.zeros_like(scene["grad_others"])
+    out = run_b200_gs(scene, cuda_device)
+    wc = scene["grad_color"].astype(np.float64)
+    keys = ("means", "scales", "quats", "opacities", "shs")
+    s64 = {k: (v.astype(np.float64) if isinstance(v, np.ndarray) else v) for k, v in scene.items()}
+
+    def loss(*arrs):
+        sc = dict(s64)
+        sc.update(dict(zip(keys, arrs)))
+        return float((SO.render(sc, "f64")["color"] * wc).sum())
+
+    rng = np.random.default_rng(2)
+    h = 1e-4
+    for which, (k, gk) in enumerate(zip(keys, ("d_means3D", "d_scales", "d_rot", "d_opacity", "d_sh"))):
+        base = [s64[x].copy() for x in keys]
+        an_all = out[gk].reshape(-1)
+        live = np.nonzero(np.abs(an_all) > 0)[0]
+        idx = rng.choice(live, size=min(24, live.size), replace=False)
+        fd, an = [], []
+        for fi in idx:
+            d = []
+            for step in (h, h / 8):
+                plus = [b.copy() for b in base]
+                minus = [b.copy() for b in base]
+                plus[which].reshape(-1)[fi] += step
+                minus[which].reshape(-1)[fi] -= step
+                d.append((loss(*plus) - loss(*minus)) / (2 * step))
+            if abs(d[0] - d[1]) > 1e-3 * max(abs(d[0]), 1e-8):
+                continue
+            fd.append(d[0])
+            an.append(an_all[fi])
+        assert len(fd) >= 12, (k, len(fd))
+        e = rel_l2(np.array(an), np.array(fd))
+        assert e <= 1e-4, (k, e)
