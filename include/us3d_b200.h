@@ -86,8 +86,8 @@ typedef struct us3d_slice_frame {
     int32_t tiles_y;
     int32_t pixel_offset;
     int32_t tile_offset;
-    int32_t reserved0;
-    int32_t reserved1;
+    int32_t gauss_offset;     /* with US3D_UG_BIN_GAUSSIAN_SETS: first Gaussian of this */
+    int32_t gauss_count;      /* frame's set and its size (otherwise 0, 0: all of them) */
 } us3d_slice_frame; /* 96 bytes */
 
 /* ------------------------------------------------------------------------------------
@@ -147,6 +147,17 @@ US3D_API int us3d_ug_bin(void* workspace, size_t workspace_bytes, const us3d_sli
  * 368-372, torch.sigmoid), so that a training step needs no separate activation pass.
  */
 #define US3D_UG_BIN_LOGIT_ATTRIBUTES 2
+/*
+ * flags |= US3D_UG_BIN_GAUSSIAN_SETS: every frame renders only its own Gaussians, the range
+ * [gauss_offset, gauss_offset + gauss_count) of the parameter arrays, so that independent
+ * sweeps with their own Gaussian sets (of any sizes, with frames of any sizes) bin, shade and
+ * differentiate in one launch sequence over the concatenated parameters. The frames of one
+ * set must be contiguous in the table and the sets must appear in increasing gauss_offset
+ * order without overlapping (each Gaussian then belongs to at most one set; gradients of a
+ * Gaussian sum over its set's frames). No counterpart in the reference (one frame and one
+ * parameter set per call).
+ */
+#define US3D_UG_BIN_GAUSSIAN_SETS 4
 US3D_API int us3d_ug_bin_ex(void* workspace, size_t workspace_bytes, const us3d_slice_frame* frames_dev,
                             int32_t n_frames, int64_t n_tiles, int64_t n_pixels, int64_t n_gauss,
                             const float* means, const float* precision_tril, const float* opacities,

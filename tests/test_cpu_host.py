@@ -118,3 +118,32 @@ def test_device_frame_source_records_on_host():
     flat = DeviceFrameSource(images.astype(np.float32) / 255.0, None, None, None, None, 1.0, 1.0,
                              device=torch.device("cpu"))
     assert flat.image_format == _lib.IMAGES_F32
+
+
+def test_frame_table_gaussian_sets_validation():
+    import dataclasses
+
+    import pytest
+    import torch
+
+    from us3d_b200 import scenes
+    from us3d_b200 import ultragauss as UG
+
+    fr = scenes.linear_sweep(4, 16, 16, 1.0, seed=0, cube_mm=16.0)
+    base = [UG.SliceSpec(f.height, f.width, f.lateral_spacing, f.axial_spacing, f.axial_near, f.lateral_col_offset,
+                         f.origin, f.axis_lat, f.axis_ax, f.axis_ele) for f in fr]
+    cpu = torch.device("cpu")
+    sets = [(0, 10), (0, 10), (10, 5), (20, 1)]
+    t = UG.build_frame_table([dataclasses.replace(s, gaussian_set=x) for s, x in zip(base, sets)], cpu)
+    assert t.gaussian_sets
+    ints = t.table[:, 16:24].contiguous().view(torch.int32)
+    assert ints[:, 6].tolist() == [0, 0, 10, 20] and ints[:, 7].tolist() == [10, 10, 5, 1]
+    assert not UG.build_frame_table(base, cpu).gaussian_sets
+    bad = [
+        [(0, 10), (5, 10), (20, 1), (30, 1)],   # overlapping sets
+        [(0, 10), (10, 5), (0, 10), (30, 1)],   # a set's frames not contiguous
+        [(0, 10), None, (10, 5), (20, 1)],      # some frames without a set
+    ]
+    for sets in bad:
+        with pytest.raises(ValueError):
+            UG.build_frame_table([dataclasses.replace(s, gaussian_set=x) for s, x in zip(base, sets)], cpu)

@@ -457,8 +457,37 @@ tile_dev_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
 // instance's key. Instance ids are the exclusive scan of the tasks' tile counts in (g, f)
 // order, hence Gaussian-major and deterministic.
 
+// Frames [f0, f1) that render Gaussian g. With Gaussian sets (frames grouped by set, sets in
+// increasing gauss_offset order) two binary searches over the frame table find g's set's
+// frames; otherwise every frame renders every Gaussian.
+__device__ __forceinline__ void gaussian_frames(const us3d_slice_frame* __restrict__ frames, int F, int64_t g,
+                                                int sets, int& f0, int& f1) {
+    f0 = 0;
+    f1 = F;
+    if (!sets) return;
+    int lo = 0, hi = F;  // first frame whose set starts after g
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((int64_t)frames[mid].gauss_offset <= g) lo = mid + 1; else hi = mid;
+    }
+    const int last = lo - 1;
+    if (last < 0 || g >= (int64_t)frames[last].gauss_offset + frames[last].gauss_count) {
+        f1 = 0;  // in no set
+        return;
+    }
+    const int off = frames[last].gauss_offset;
+    lo = 0;
+    hi = last;  // first frame of that set
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (frames[mid].gauss_offset < off) lo = mid + 1; else hi = mid;
+    }
+    f0 = lo;
+    f1 = last + 1;
+}
+
 __global__ void __launch_bounds__(256)
-cull_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, int F,
+cull_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames, int F, int sets,
             const float4* __restrict__ pack, float chi2, float beta, const int* __restrict__ task_offset,
             int64_t cap, int* __restrict__ gtasks, int4* __restrict__ task_rect, int2* __restrict__ task_gf,
             float* __restrict__ task_v) {
@@ -467,7 +496,9 @@ cull_kernel(int64_t G, int64_t T, int64_t P, const us3d_slice_frame* __restrict_
     const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
     int k = task_offset ? task_offset[g] : 0;
     int n = 0;
-    for (int f = 0; f < F; ++f) {
+    int fa, fb;
+    gaussian_frames(frames, F, g, sets, fa, fb);
+    for (int f = fa; f < fb; ++f) {
         if (!frame_ok(frames + f, T, P)) continue;
         const Geo geo = load_geo(frames + f);
         int4 r;
@@ -1230,8 +1261,9 @@ int us3d::ug::bin_with_task_capacity(void* workspace, size_t workspace_bytes, co
                                      const float* pixels, int32_t flags, void* stream_) {
     int st = check_common(frames, n_frames, n_tiles, n_pixels, n_gauss);
     const int slice_cull = (flags & US3D_UG_BIN_SLICE_CULL) ? 1 : 0;
-    US3D_CHECK_ARG((flags & ~(US3D_UG_BIN_SLICE_CULL | US3D_UG_BIN_LOGIT_ATTRIBUTES)) == 0,
+    US3D_CHECK_ARG((flags & ~(US3D_UG_BIN_SLICE_CULL | US3D_UG_BIN_LOGIT_ATTRIBUTES | US3D_UG_BIN_GAUSSIAN_SETS)) == 0,
                    "unknown binning flags 0x%x", (unsigned)flags);
+    const int sets = (flags & US3D_UG_BIN_GAUSSIAN_SETS) ? 1 : 0;
     US3D_CHECK_ARG(!slice_cull || n_pixels == 0 || pixels != nullptr, "slice cull needs the pixel positions");
     if (st != US3D_OK) return st;
     US3D_CHECK_ARG(workspace != nullptr, "workspace is NULL");
@@ -1260,7 +1292,7 @@ int us3d::ug::bin_with_task_capacity(void* workspace, size_t workspace_bytes, co
     if (n_gauss > 0) {
         pack_kernel<<<gb, 256, 0, stream>>>(n_gauss, means, tril, opac, inten,
                                             (flags & US3D_UG_BIN_LOGIT_ATTRIBUTES) ? 1 : 0, w.pack);
-        cull_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta, nullptr,
+        cull_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, sets, w.pack, chi2, beta, nullptr,
                                             tc, w.gtasks, w.task_rect, w.task_gf, w.task_v);
         US3D_CHECK_LAUNCH("ug cull");
     }
@@ -1268,7 +1300,7 @@ int us3d::ug::bin_with_task_capacity(void* workspace, size_t workspace_bytes, co
     task_check_kernel<<<1, 1, 0, stream>>>(w.header, tc);
     US3D_CHECK_CUDA(cudaMemsetAsync(w.task_ntiles, 0, sizeof(int) * (size_t)tc, stream));
     if (n_gauss > 0) {
-        cull_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, w.pack, chi2, beta,
+        cull_kernel<<<gb, 256, 0, stream>>>(n_gauss, n_tiles, n_pixels, frames, n_frames, sets, w.pack, chi2, beta,
                                             w.task_offset, tc, w.gtasks, w.task_rect, w.task_gf, w.task_v);
         task_count_kernel<<<tb, 128, 0, stream>>>(w.header, frames, w.pack, chi2, beta, tdev, w.task_rect, w.task_gf,
                                                   w.task_ntiles, w.tile_count);

@@ -45,8 +45,8 @@ class SliceFrame(ctypes.Structure):
         ("tiles_y", c_int32),
         ("pixel_offset", c_int32),
         ("tile_offset", c_int32),
-        ("reserved0", c_int32),
-        ("reserved1", c_int32),
+        ("gauss_offset", c_int32),
+        ("gauss_count", c_int32),
     ]
 
 
@@ -73,6 +73,7 @@ ADAM_IDENTITY = 0
 ADAM_LOGISTIC = 1
 UG_BIN_SLICE_CULL = 1
 UG_BIN_LOGIT_ATTRIBUTES = 2
+UG_BIN_GAUSSIAN_SETS = 4
 IMAGES_F32, IMAGES_F32_DIV255, IMAGES_U8, IMAGES_U8_DIV255 = 0, 1, 2, 3
 
 # name -> (restype, argtypes)

@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass
-from typing import List, Optional, Sequence
+from typing import List, Optional, Sequence, Tuple
 
 import torch
 
@@ -46,6 +46,10 @@ class SliceSpec:
     axis_lat: torch.Tensor
     axis_ax: torch.Tensor
     axis_ele: torch.Tensor
+    # (first Gaussian, count) of the Gaussian set this frame renders; None: all Gaussians.
+    # Frames of independent sweeps, each with its own Gaussians, then render in one call over
+    # the concatenated parameters.
+    gaussian_set: Optional[Tuple[int, int]] = None
 
 
 @dataclass
@@ -58,6 +62,7 @@ class FrameTable:
     tile_counts: List[int]
     pixel_offsets: List[int]
     sizes: List[tuple]
+    gaussian_sets: bool = False
 
 
 def build_frame_table(specs: Sequence[SliceSpec], device: torch.device) -> FrameTable:
@@ -67,10 +72,24 @@ def build_frame_table(specs: Sequence[SliceSpec], device: torch.device) -> Frame
     scal = torch.zeros((F, 4), dtype=torch.float32)
     t_off = p_off = 0
     tile_offsets, tile_counts, pixel_offsets, sizes = [], [], [], []
+    sets = [getattr(s, "gaussian_set", None) for s in specs]
+    use_sets = any(x is not None for x in sets)
+    if use_sets:
+        if any(x is None for x in sets):
+            raise ValueError("either every frame names its Gaussian set or none does")
+        prev = None
+        for i, (off, cnt) in enumerate(sets):
+            if off < 0 or cnt < 0 or off + cnt > 0x7FFFFFFF:
+                raise ValueError(f"frame {i}: bad Gaussian set ({off}, {cnt})")
+            if prev is not None and (off, cnt) != prev and off < prev[0] + prev[1]:
+                raise ValueError(f"frame {i}: Gaussian sets must be contiguous runs in increasing, "
+                                 f"non-overlapping order (set ({off}, {cnt}) after {prev})")
+            prev = (off, cnt)
     for i, s in enumerate(specs):
         H, W = int(s.height), int(s.width)
         tx, ty = (W + TILE - 1) // TILE, (H + TILE - 1) // TILE
-        ints[i, :6] = torch.tensor([H, W, tx, ty, p_off, t_off], dtype=torch.int32)
+        go, gc = sets[i] if use_sets else (0, 0)
+        ints[i, :8] = torch.tensor([H, W, tx, ty, p_off, t_off, go, gc], dtype=torch.int32)
         scal[i] = torch.tensor([s.lateral_spacing, s.axial_spacing, s.axial_near, s.lateral_col_offset],
                                dtype=torch.float32)
         tile_offsets.append(t_off)
@@ -88,7 +107,7 @@ def build_frame_table(specs: Sequence[SliceSpec], device: torch.device) -> Frame
         table = torch.cat([axes, host_tail], dim=1).contiguous()
     else:
         table = torch.zeros((0, 24), dtype=torch.float32, device=device)
-    return FrameTable(table, F, t_off, p_off, tile_offsets, tile_counts, pixel_offsets, sizes)
+    return FrameTable(table, F, t_off, p_off, tile_offsets, tile_counts, pixel_offsets, sizes, use_sets)
 
 
 # Capacity hints per (G, n_tiles): the last instance total seen, so that steady-state calls
@@ -145,7 +164,8 @@ def bin_gaussians(means: torch.Tensor, tril: torch.Tensor, opac: torch.Tensor, i
             "us3d_ug_bin_ex", _ptr(ws), int(nbytes), _ptr(frames.table), frames.n_frames, frames.n_tiles,
             frames.n_pixels, G, _ptr(means), _ptr(tril), _ptr(opac), _ptr(inten), float(chi2), float(beta),
             int(bool(sort_by_depth)), cap, _ptr(slice_cull_pixels) if cull else None,
-            (_lib.UG_BIN_SLICE_CULL if cull else 0) | (_lib.UG_BIN_LOGIT_ATTRIBUTES if logit_attributes else 0), _stream(),
+            (_lib.UG_BIN_SLICE_CULL if cull else 0) | (_lib.UG_BIN_LOGIT_ATTRIBUTES if logit_attributes else 0)
+            | (_lib.UG_BIN_GAUSSIAN_SETS if frames.gaussian_sets else 0), _stream(),
         )
         _lib.check(st, "us3d_ug_bin_ex")
         b = UGBinning(ws, cap, -1, frames, G, float(chi2), float(beta), bool(sort_by_depth), cull)
