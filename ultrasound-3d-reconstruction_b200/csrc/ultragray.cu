@@ -53,6 +53,16 @@ struct Workspace {
     int* sorted_gid;
     int* sorted_inst;
     float4* pixel_state;  // P: T_final, sum I w, sum w, t_pixel
+    // Transmittance checkpoints (quadrature window radius > 0, full transmission):
+    float* t_pix;         // P: sample depth t along its ray (ray-major)
+    int* mono;            // W: 1 if the ray's sample depths never decrease
+    float4* aux;          // cap: per instance (t_gauss, echo radius, far factor F, first far sample)
+    long long* far_log;   // P: fixed-point sum of log F of the instances whose far zone starts at the
+                          //    sample, then (in place) its prefix along the ray
+    float* t_far;         // P: product of the far factors of every instance settled at the sample
+    float4* b_pos;        // P: backward: sample position, t
+    float4* b_coef;       // P: backward: dL/dT, T, dL/dnum, dL/dw (zero for skipped samples)
+    float* b_suffix;      // P: backward: sum over the ray's samples y' >= y of dL/dT * T
     size_t bytes;
 };
 
@@ -75,6 +85,14 @@ static Workspace carve(void* base, int64_t G, int64_t W, int64_t P, int64_t cap)
     w.sorted_gid = c.take<int>((size_t)cap);
     w.sorted_inst = c.take<int>((size_t)cap);
     w.pixel_state = c.take<float4>((size_t)P);
+    w.t_pix = c.take<float>((size_t)P);
+    w.mono = c.take<int>((size_t)W);
+    w.aux = c.take<float4>((size_t)cap);
+    w.far_log = c.take<long long>((size_t)P);
+    w.t_far = c.take<float>((size_t)P);
+    w.b_pos = c.take<float4>((size_t)P);
+    w.b_coef = c.take<float4>((size_t)P);
+    w.b_suffix = c.take<float>((size_t)P);
     w.bytes = align_up(c.off, 256);
     return w;
 }
@@ -315,8 +333,8 @@ forward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __res
                const long long* __restrict__ header, const float4* __restrict__ rec,
                const float* __restrict__ pixels, const float* __restrict__ ray_o, const float* __restrict__ ray_d,
                const float* __restrict__ a_ele, const float* __restrict__ pert, const uint32_t* __restrict__ dkey,
-               float k_sigma, float wr, int local_only, float max_win, float* __restrict__ image,
-               float4* __restrict__ pixel_state) {
+               float k_sigma, float wr, int local_only, float max_win, const int* __restrict__ ckpt_rays,
+               float* __restrict__ image, float4* __restrict__ pixel_state) {
     __shared__ float4 s_rec[BATCH * REC_F4];
     __shared__ float s_tg[BATCH];
     __shared__ float s_depth[BATCH];
@@ -324,6 +342,7 @@ forward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __res
     __shared__ float s_far[BATCH];   // its factor tau + (1 - tau) exp(-psi) for pixels at or past it
     if (header[H_FLAGS] != 0) return;
     const int x = blockIdx.x;
+    if (ckpt_rays && ckpt_rays[x]) return;  // rendered by the checkpointed path
     const int s0 = ray_start[x], n = ray_start[x + 1] - s0;
     const RayGeo rg = ray_geo(x, ray_o, ray_d, a_ele, pert);
     // blockIdx.y: which blockDim.x samples of the ray this block shades
@@ -406,6 +425,233 @@ forward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __res
     }
 }
 
+// ------------------------------------------------------------------------------------
+// Transmittance checkpoints (quadrature window radius wr > 0, full transmission)
+// ------------------------------------------------------------------------------------
+//
+// With wr > 0 the transmission factor of instance k at a sample of depth t no longer depends on
+// t once t >= tcw_k = tc_k + wr (and t > t_gauss, t > 0): it is the instance's far factor F_k
+// (the reference evaluates the same integral, over the same window, at every such sample).
+// Along a ray whose sample depths never decrease, instance k is therefore "settled" from its
+// first far sample y_far(k) on. The product of the settled factors at every sample is a
+// checkpoint: log F_k is added, in 2^-32 fixed point (exact, order-free integer sums), at
+// y_far(k), a prefix sum along the ray gives each sample's sum, and T_far = exp(sum) (double).
+// A sample's transmittance is then T_far times the factors of the instances it is still inside
+// the window of (t_gauss < t < tcw), evaluated as the reference does, in list order; the
+// forward of a tile of samples walks only the instances near or echoing in that tile. The
+// backward reads the same checkpoints: the far part of an instance's gradient is the suffix
+// sum over the ray's samples of dL/dT * T divided by F_k, and only the samples inside its
+// window or echo range are visited. Rays whose sample depths decrease somewhere keep the
+// per-sample path above.
+
+constexpr double FAR_LOG_SCALE = 4294967296.0;  // 2^32
+constexpr double FAR_LOG_MIN = -1000.0;          // log F below this (F < 1e-434) counts as -1000
+
+// Sample depths of every ray (as the forward computes them) and whether they never decrease.
+__global__ void __launch_bounds__(256)
+ray_depth_kernel(int W, int H, const long long* __restrict__ header, const float* __restrict__ pixels,
+                 const float* __restrict__ ray_o, const float* __restrict__ ray_d, const float* __restrict__ a_ele,
+                 const float* __restrict__ pert, float* __restrict__ t_pix, int* __restrict__ mono) {
+    const int x = blockIdx.x;
+    if (x >= W) return;
+    const RayGeo rg = ray_geo(x, ray_o, ray_d, a_ele, pert);
+    for (int y = threadIdx.x; y < H; y += blockDim.x) {
+        const float* pp = pixels + ((int64_t)x * H + y) * 3;
+        const float3 p = make_float3(pp[0], pp[1], pp[2]);
+        t_pix[(int64_t)x * H + y] = fmaxf(0.0f, v_dot(v_sub(p, rg.o), rg.d));
+    }
+    __syncthreads();
+    int ok = 1;
+    for (int y = threadIdx.x + 1; y < H; y += blockDim.x)
+        ok &= t_pix[(int64_t)x * H + y] >= t_pix[(int64_t)x * H + y - 1];
+    ok = __syncthreads_and(ok);
+    if (threadIdx.x == 0) mono[x] = (header[H_FLAGS] == 0 && ok) ? 1 : 0;
+}
+
+// First sample index in [0, H) of a nondecreasing depth array whose depth satisfies pred
+// (monotone in the index), H if none.
+template <typename Pred>
+__device__ __forceinline__ int first_sample(const float* __restrict__ t, int H, Pred pred) {
+    int lo = 0, hi = H;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (pred(t[mid])) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+// Per instance of a checkpointed ray: depth, echo radius, far factor and first far sample;
+// the fixed-point log of the far factor is added to that sample's slot.
+__global__ void __launch_bounds__(128)
+far_prep_kernel(int W, int H, const int* __restrict__ ray_start, const int* __restrict__ sorted_gid,
+                const long long* __restrict__ header, const float4* __restrict__ rec,
+                const float* __restrict__ ray_o, const float* __restrict__ ray_d, const float* __restrict__ a_ele,
+                const float* __restrict__ pert, const int* __restrict__ mono, const float* __restrict__ t_pix,
+                float k_sigma, float wr, float4* __restrict__ aux, long long* __restrict__ far_log) {
+    if (header[H_FLAGS] != 0) return;
+    const int x = blockIdx.x;
+    if (!mono[x]) return;
+    const int s0 = ray_start[x], n = ray_start[x + 1] - s0;
+    const RayGeo rg = ray_geo(x, ray_o, ray_d, a_ele, pert);
+    const float* t = t_pix + (int64_t)x * H;
+    for (int k = blockIdx.y * blockDim.x + threadIdx.x; k < n; k += gridDim.y * blockDim.x) {
+        Rec r;
+        load_rec(rec + (int64_t)REC_F4 * sorted_gid[s0 + k], r);
+        const float t_gauss = v_dot(v_sub(r.mu, rg.o), rg.d);
+        float tcw = 3.0e38f;
+        const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, 3.0e38f, wr, &tcw);
+        const float F = r.tau + (1.0f - r.tau) * __expf(-psi);
+        const int y_far = first_sample(t, H, [&](float tp) { return tp > 0.0f && tp > t_gauss && tp >= tcw; });
+        aux[s0 + k] = make_float4(t_gauss, r.smax * k_sigma, F, __int_as_float(y_far));
+        if (y_far < H) {
+            const double lf = F > 0.0f ? fmax(log((double)F), FAR_LOG_MIN) : FAR_LOG_MIN;
+            atomicAdd(reinterpret_cast<unsigned long long*>(far_log + (int64_t)x * H + y_far),
+                      (unsigned long long)llrint(lf * FAR_LOG_SCALE));
+        }
+    }
+}
+
+// Prefix of the fixed-point far logs along each checkpointed ray (one warp per ray) and the
+// far transmittance of every sample.
+__global__ void __launch_bounds__(32)
+far_prefix_kernel(int W, int H, const long long* __restrict__ header, const int* __restrict__ mono,
+                  long long* __restrict__ far_log, float* __restrict__ t_far) {
+    const int x = blockIdx.x;
+    if (x >= W || header[H_FLAGS] != 0 || !mono[x]) return;
+    const int lane = threadIdx.x;
+    long long carry = 0;
+    for (int y0 = 0; y0 < H; y0 += 32) {
+        const int y = y0 + lane;
+        long long v = y < H ? far_log[(int64_t)x * H + y] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+        }
+        v += carry;
+        if (y < H) {
+            far_log[(int64_t)x * H + y] = v;
+            t_far[(int64_t)x * H + y] = (float)exp((double)v / FAR_LOG_SCALE);
+        }
+        carry = __shfl_sync(0xffffffffu, v, 31);
+    }
+}
+
+// Forward of a checkpointed ray: block (x, y) shades samples [FWD_SAMPLES y, ...) of ray x.
+// The ray's instances that are still inside their window somewhere in the tile, or echo in it,
+// are listed in list order (chunks of LIST_CAP), their records staged, and every sample
+// multiplies its checkpoint T_far by the window factors of the listed instances it has passed
+// but not left (t_gauss < t < tcw) and adds their echo terms, as the reference does.
+constexpr int LIST_CAP = 192;
+
+__global__ void __launch_bounds__(FWD_SAMPLES)
+forward_ckpt_kernel(int W, int H, const int* __restrict__ ray_start, const int* __restrict__ sorted_gid,
+                    const long long* __restrict__ header, const float4* __restrict__ rec,
+                    const float* __restrict__ pixels, const float* __restrict__ ray_o, const float* __restrict__ ray_d,
+                    const float* __restrict__ a_ele, const float* __restrict__ pert, const int* __restrict__ mono,
+                    const float* __restrict__ t_pix, const float4* __restrict__ aux, const float* __restrict__ t_far,
+                    float wr, float* __restrict__ image, float4* __restrict__ pixel_state) {
+    __shared__ float4 s_rec[LIST_CAP * REC_F4];
+    __shared__ float4 s_aux[LIST_CAP];
+    __shared__ int s_list[LIST_CAP + FWD_SAMPLES];
+    __shared__ int s_n;
+    __shared__ int s_warp[FWD_SAMPLES / 32];
+    if (header[H_FLAGS] != 0) return;
+    const int x = blockIdx.x;
+    if (!mono[x]) return;
+    const int y0 = blockIdx.y * FWD_SAMPLES;
+    if (y0 >= H) return;
+    const int y1 = min(H, y0 + FWD_SAMPLES);
+    const int s0 = ray_start[x], n = ray_start[x + 1] - s0;
+    const float* t = t_pix + (int64_t)x * H;
+    const float t_lo = t[y0], t_hi = t[y1 - 1];
+    const RayGeo rg = ray_geo(x, ray_o, ray_d, a_ele, pert);
+    const int y = y0 + threadIdx.x;
+    const bool valid = y < H;
+    float3 p = make_float3(0.f, 0.f, 0.f);
+    float t_pixel = 0.f, trans = 1.0f;
+    if (valid) {
+        const float* pp = pixels + ((int64_t)x * H + y) * 3;
+        p = make_float3(pp[0], pp[1], pp[2]);
+        t_pixel = t[y];
+        trans = t_far[(int64_t)x * H + y];
+    }
+    float num = 0.0f, den = 0.0f, sacc = 0.0f;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    for (int k0 = 0; k0 < n; k0 += FWD_SAMPLES) {
+        // list the instances of this chunk that matter to the tile (order kept)
+        const int k = k0 + threadIdx.x;
+        bool keep = false;
+        if (k < n) {
+            const float4 a = aux[s0 + k];
+            const int y_far = __float_as_int(a.w);
+            keep = (y_far > y0 && a.x < t_hi) || (a.x + a.y >= t_lo && a.x - a.y <= t_hi);
+        }
+        const unsigned bits = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_warp[warp] = __popc(bits);
+        __syncthreads();
+        int base = s_n;
+        for (int w2 = 0; w2 < warp; ++w2) base += s_warp[w2];
+        if (keep) s_list[base + __popc(bits & ((1u << lane) - 1u))] = k;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tot = s_n;
+            for (int w2 = 0; w2 < FWD_SAMPLES / 32; ++w2) tot += s_warp[w2];
+            s_n = tot;
+        }
+        __syncthreads();
+        const int nl = s_n;
+        const bool last = k0 + FWD_SAMPLES >= n;
+        if (nl < LIST_CAP && !last) continue;
+        // stage and shade the listed instances (at most LIST_CAP at a time, in list order)
+        for (int b0 = 0; b0 < nl; b0 += LIST_CAP) {
+            const int nb = min(LIST_CAP, nl - b0);
+            for (int j = threadIdx.x; j < nb * REC_F4; j += blockDim.x) {
+                const int e = j / REC_F4, f = j - e * REC_F4;
+                s_rec[j] = rec[(int64_t)REC_F4 * sorted_gid[s0 + s_list[b0 + e]] + f];
+            }
+            for (int e = threadIdx.x; e < nb; e += blockDim.x) s_aux[e] = aux[s0 + s_list[b0 + e]];
+            __syncthreads();
+            if (valid) {
+                for (int e = 0; e < nb; ++e) {
+                    const float4 a = s_aux[e];
+                    const float t_gauss = a.x;
+                    const bool need_t = t_gauss < t_pixel && y < __float_as_int(a.w);  // passed, not yet far
+                    const bool need_e = fabsf(t_gauss - t_pixel) <= a.y;
+                    if (!need_t && !need_e) continue;
+                    Rec r;
+                    load_rec(s_rec + e * REC_F4, r);
+                    if (need_t) {
+                        const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, t_pixel, wr);
+                        trans *= r.tau + (1.0f - r.tau) * __expf(-psi);
+                    }
+                    if (need_e) {
+                        const float wgt = gauss_weight(p, r.mu, r.P);
+                        const float I = r.sh.x + r.sh.y * rg.d.x + r.sh.z * rg.d.y + r.sh.w * rg.d.z;
+                        num += I * wgt;
+                        den += wgt;
+                        sacc += wgt;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+    }
+    if (!valid) return;
+    float out = 0.0f;
+    if (n > 0) {
+        const float gamma = 1.0f - __expf(-sacc);
+        const float echo = num / (den + 1e-6f);
+        out = trans * (gamma * echo);
+    }
+    image[(int64_t)y * W + x] = out;
+    pixel_state[(int64_t)x * H + y] = make_float4(trans, num, den, sacc);
+}
+
 // VJP of ray_integral w.r.t. the Gaussian (mean, scales, rotation), the quadrature nodes held
 // fixed (reference backward.cu:26-108), accumulated into ds, dmu, dR; l is the pixel depth.
 // With wr > 0, *tcw_out (if not NULL) receives the window end tc + wr it uses.
@@ -467,6 +713,190 @@ __device__ __forceinline__ void psi_vjp(const RayGeo& rg, const Rec& r, float t_
 // Backward
 // ------------------------------------------------------------------------------------
 
+// End of an instance's backward: the far-field VJP applied once with the summed scalar adjoint
+// far_dT, dL/dP (symmetric sum over pixels) -> dL/dR, dL/ds, dL/dR -> dL/dq, and the partial.
+__device__ __forceinline__ void instance_epilogue(const RayGeo& rg, const Rec& r, float wr, float far_dT, float far_exp,
+                                                  float dP[9], float dR[9], float ds[3], float dmu[3], float dtau_raw,
+                                                  const float dsh[4], const float* __restrict__ quats, int g,
+                                                  float4* __restrict__ out) {
+    if (far_dT != 0.0f) {
+        dtau_raw += far_dT * (1.0f - far_exp) * (r.tau * (1.0f - r.tau));
+        psi_vjp(rg, r, 3.0e38f, wr, far_dT * (1.0f - r.tau) * far_exp * (-1.0f), ds, dmu, dR);
+    }
+    dP[3] = dP[1];
+    dP[6] = dP[2];
+    dP[7] = dP[5];
+    {
+        const float d[3] = {1.f / (r.s.x * r.s.x), 1.f / (r.s.y * r.s.y), 1.f / (r.s.z * r.s.z)};
+#pragma unroll
+        for (int rr = 0; rr < 3; ++rr)
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk)
+                dR[rr * 3 + kk] += 2.0f * (dP[rr * 3 + 0] * r.R[kk] + dP[rr * 3 + 1] * r.R[3 + kk] + dP[rr * 3 + 2] * r.R[6 + kk]) * d[kk];
+        const float sv[3] = {r.s.x, r.s.y, r.s.z};
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+            float a = 0.f;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) a += r.R[i * 3 + kk] * dP[i * 3 + j] * r.R[j * 3 + kk];
+            ds[kk] += -2.f * a * d[kk] / sv[kk];
+        }
+    }
+    const float4 q = make_float4(quats[4 * (int64_t)g], quats[4 * (int64_t)g + 1], quats[4 * (int64_t)g + 2],
+                                 quats[4 * (int64_t)g + 3]);
+    const float4 dq = quat_grad(q, dR);
+    out[0] = make_float4(dmu[0], dmu[1], dmu[2], dtau_raw);
+    out[1] = make_float4(ds[0], ds[1], ds[2], dsh[0]);
+    out[2] = make_float4(dsh[1], dsh[2], dsh[3], 0.f);
+    out[3] = dq;
+}
+
+// One instance's transmission term at a sample inside its window, and its echo term.
+__device__ __forceinline__ void near_terms(const RayGeo& rg, const Rec& r, float wr, const float4 pt, const float4 cf,
+                                           bool need_t, bool need_e, float dP[9], float dR[9], float ds[3],
+                                           float dmu[3], float& dtau_raw, float dsh[4]) {
+    const float t_pixel = pt.w;
+    if (need_t) {
+        const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, t_pixel, wr);
+        const float exp_psi = __expf(-psi);
+        const float T_i = r.tau + (1.0f - r.tau) * exp_psi;
+        float dTi = 0.0f;
+        if (T_i > 1e-6f) dTi = cf.x * (cf.y / T_i);
+        dtau_raw += dTi * (1.0f - exp_psi) * (r.tau * (1.0f - r.tau));
+        const float dpsi = dTi * (1.0f - r.tau) * exp_psi * (-1.0f);
+        psi_vjp(rg, r, t_pixel, wr, dpsi, ds, dmu, dR);
+    }
+    if (need_e) {
+        const float3 p = make_float3(pt.x, pt.y, pt.z);
+        const float wgt = gauss_weight(p, r.mu, r.P);
+        const float I = r.sh.x + r.sh.y * rg.d.x + r.sh.z * rg.d.y + r.sh.w * rg.d.z;
+        const float a = cf.z * wgt;
+        dsh[0] += a;
+        dsh[1] += a * rg.d.x;
+        dsh[2] += a * rg.d.y;
+        dsh[3] += a * rg.d.z;
+        const float dw = (cf.z * I) + cf.w;
+        const float dQ = dw * wgt * (-0.5f);
+        const float dx = p.x - r.mu.x, dy = p.y - r.mu.y, dz = p.z - r.mu.z;
+        const float v0 = r.P[0] * dx + r.P[1] * dy + r.P[2] * dz;
+        const float v1 = r.P[3] * dx + r.P[4] * dy + r.P[5] * dz;
+        const float v2 = r.P[6] * dx + r.P[7] * dy + r.P[8] * dz;
+        dmu[0] += dQ * (-2.0f * v0);
+        dmu[1] += dQ * (-2.0f * v1);
+        dmu[2] += dQ * (-2.0f * v2);
+        const float ux = dQ * dx, uy = dQ * dy, uz = dQ * dz;
+        dP[0] += ux * dx; dP[1] += ux * dy; dP[2] += ux * dz;
+        dP[4] += uy * dy; dP[5] += uy * dz;
+        dP[8] += uz * dz;
+    }
+}
+
+// Backward of a checkpointed ray, per sample: the adjoint coefficients the per-sample path
+// stages (zero for samples whose |dL/dB| < 1e-6, which the reference skips), and the suffix sums
+// along the ray of dL/dT * T (in double, fixed order; one warp per ray).
+__global__ void __launch_bounds__(32)
+ckpt_coef_kernel(int W, int H, const long long* __restrict__ header, const int* __restrict__ mono,
+                 const float* __restrict__ pixels, const float* __restrict__ t_pix,
+                 const float4* __restrict__ pixel_state, const float* __restrict__ grad_image,
+                 float4* __restrict__ b_pos, float4* __restrict__ b_coef, float* __restrict__ b_suffix) {
+    const int x = blockIdx.x;
+    if (x >= W || header[H_FLAGS] != 0 || !mono[x]) return;
+    const int lane = threadIdx.x;
+    double carry = 0.0;
+    const int nchunks = (H + 31) / 32;
+    for (int c = nchunks - 1; c >= 0; --c) {  // from the deepest samples up: suffix sums
+        const int y = c * 32 + lane;
+        double v = 0.0;
+        if (y < H) {
+            const int64_t pi = (int64_t)x * H + y;
+            const float* pp = pixels + pi * 3;
+            const float gB = grad_image[(int64_t)y * W + x];
+            const float4 st = pixel_state[pi];  // T, num, den, S
+            const float gamma = 1.0f - __expf(-st.w);
+            const float eps = 1e-6f;
+            const float e_raw = st.y / (st.z + eps);
+            const float e_val = gamma * e_raw;
+            const float dT = gB * e_val;
+            const float dE = gB * st.x;
+            const float dgam = dE * e_raw;
+            const float de_raw = dE * gamma;
+            const float dS = dgam * __expf(-st.w);
+            const float dnum = de_raw * (1.0f / (st.z + eps));
+            const float dden = de_raw * (-st.y / ((st.z + eps) * (st.z + eps)));
+            const bool active = !(fabsf(gB) < 1e-6f);
+            b_pos[pi] = make_float4(pp[0], pp[1], pp[2], t_pix[pi]);
+            b_coef[pi] = active ? make_float4(dT, st.x, dnum, dden + dS) : make_float4(0.f, 0.f, 0.f, 0.f);
+            v = active ? (double)dT * (double)st.x : 0.0;
+        }
+        // inclusive suffix within the chunk: lane l sums lanes l..31
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double u = __shfl_down_sync(0xffffffffu, v, o);
+            if (lane + o < 32) v += u;
+        }
+        v += carry;
+        if (y < H) b_suffix[(int64_t)x * H + y] = (float)v;
+        carry = __shfl_sync(0xffffffffu, v, 0);
+    }
+}
+
+// Thread per instance of a checkpointed ray: the far part of its gradient from the suffix sum at
+// its first far sample, the samples inside its window [first sample past t_gauss, first far
+// sample) and its echo range |t - t_gauss| <= radius visited in sample order.
+__global__ void __launch_bounds__(128)
+backward_ckpt_kernel(int W, int H, const int* __restrict__ ray_start, const int* __restrict__ sorted_gid,
+                     const int* __restrict__ sorted_inst, const long long* __restrict__ header,
+                     const float4* __restrict__ rec, const float* __restrict__ quats, const float* __restrict__ ray_o,
+                     const float* __restrict__ ray_d, const float* __restrict__ a_ele, const float* __restrict__ pert,
+                     const int* __restrict__ mono, const float* __restrict__ t_pix, const float4* __restrict__ aux,
+                     const float4* __restrict__ b_pos, const float4* __restrict__ b_coef,
+                     const float* __restrict__ b_suffix, float wr, float4* __restrict__ partial) {
+    if (header[H_FLAGS] != 0) return;
+    const int x = blockIdx.x;
+    if (!mono[x]) return;
+    const int s0 = ray_start[x], n = ray_start[x + 1] - s0;
+    const RayGeo rg = ray_geo(x, ray_o, ray_d, a_ele, pert);
+    const float* t = t_pix + (int64_t)x * H;
+    const int64_t row = (int64_t)x * H;
+    for (int k = blockIdx.y * blockDim.x + threadIdx.x; k < n; k += gridDim.y * blockDim.x) {
+        Rec r;
+        const int g = sorted_gid[s0 + k];
+        load_rec(rec + (int64_t)REC_F4 * g, r);
+        const float4 a = aux[s0 + k];
+        const float t_gauss = a.x, radius = a.y;
+        const int y_far = __float_as_int(a.w);
+        float dmu[3] = {0.f, 0.f, 0.f}, ds[3] = {0.f, 0.f, 0.f}, dR[9], dP[9], dtau_raw = 0.f;
+        float dsh[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            dR[i] = 0.f;
+            dP[i] = 0.f;
+        }
+        // the far factor, as the per-sample path evaluates it
+        const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, 3.0e38f, wr);
+        const float far_exp = __expf(-psi);
+        const float far_T = r.tau + (1.0f - r.tau) * far_exp;
+        const int y_t = first_sample(t, H, [&](float tp) { return tp > t_gauss; });
+        const int y_e0 = first_sample(t, H, [&](float tp) { return tp >= t_gauss - radius; });
+        const int y_e1 = first_sample(t, H, [&](float tp) { return tp > t_gauss + radius; });
+        const int ya = min(y_t, y_e0), yb = max(y_far, y_e1);
+        for (int y = ya; y < yb; ++y) {
+            const float4 cf = b_coef[row + y];
+            if (cf.x == 0.0f && cf.z == 0.0f && cf.w == 0.0f) continue;  // skipped sample: every term is zero
+            const float4 pt = b_pos[row + y];
+            const bool need_t = y >= y_t && y < y_far;
+            const bool need_e = fabsf(t_gauss - pt.w) <= radius;
+            if (need_t || need_e) near_terms(rg, r, wr, pt, cf, need_t, need_e, dP, dR, ds, dmu, dtau_raw, dsh);
+        }
+        float far_dT = 0.0f;
+        if (y_far < H && far_T > 1e-6f) far_dT = b_suffix[row + y_far] / far_T;
+        instance_epilogue(rg, r, wr, far_dT, far_exp, dP, dR, ds, dmu, dtau_raw, dsh, quats, g,
+                          partial + (int64_t)PARTIAL_F4 * sorted_inst[s0 + k]);
+    }
+}
+
 // Blocks (x, *) share ray x's instances; a thread owns one instance at a time and sweeps
 // the ray's pixels in chunks whose adjoint coefficients are staged in shared memory
 // (reference backward.cu:138-325).
@@ -477,12 +907,14 @@ backward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __re
                 const float* __restrict__ ray_o, const float* __restrict__ ray_d, const float* __restrict__ a_ele,
                 const float* __restrict__ pert, const uint32_t* __restrict__ dkey,
                 const float4* __restrict__ pixel_state, const float* __restrict__ grad_image, float k_sigma,
-                float wr, int local_only, float max_win, float4* __restrict__ partial) {
+                float wr, int local_only, float max_win, const int* __restrict__ ckpt_rays,
+                float4* __restrict__ partial) {
     __shared__ float4 s_p[PIX_CHUNK];   // pixel position, t_pixel
     __shared__ float4 s_c[PIX_CHUNK];   // dL/dT, T_final, dL/dnum, dL/dw_common (den + gamma terms)
     __shared__ int s_active[PIX_CHUNK];
     if (header[H_FLAGS] != 0) return;
     const int x = blockIdx.x;
+    if (ckpt_rays && ckpt_rays[x]) return;  // differentiated by the checkpointed path
     const int s0 = ray_start[x], n = ray_start[x + 1] - s0;
     if (n <= 0) return;
     const RayGeo rg = ray_geo(x, ray_o, ray_d, a_ele, pert);
@@ -592,42 +1024,8 @@ backward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __re
             }
         }
         if (!own) continue;
-        if (far_dT != 0.0f) {
-            dtau_raw += far_dT * (1.0f - far_exp) * (r.tau * (1.0f - r.tau));
-            psi_vjp(rg, r, 3.0e38f, wr, far_dT * (1.0f - r.tau) * far_exp * (-1.0f), ds, dmu, dR);
-        }
-        // dL/dP (symmetric sum over pixels) -> dL/dR, dL/ds; dL/dR -> dL/dq.
-        dP[3] = dP[1];
-        dP[6] = dP[2];
-        dP[7] = dP[5];
-        {
-            const float d[3] = {1.f / (r.s.x * r.s.x), 1.f / (r.s.y * r.s.y), 1.f / (r.s.z * r.s.z)};
-#pragma unroll
-            for (int rr = 0; rr < 3; ++rr)
-#pragma unroll
-                for (int kk = 0; kk < 3; ++kk)
-                    dR[rr * 3 + kk] += 2.0f * (dP[rr * 3 + 0] * r.R[kk] + dP[rr * 3 + 1] * r.R[3 + kk] + dP[rr * 3 + 2] * r.R[6 + kk]) * d[kk];
-            const float sv[3] = {r.s.x, r.s.y, r.s.z};
-#pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-                float a = 0.f;
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) a += r.R[i * 3 + kk] * dP[i * 3 + j] * r.R[j * 3 + kk];
-                ds[kk] += -2.f * a * d[kk] / sv[kk];
-            }
-        }
-        // dL/dR -> dL/dq through R(q/|q|) (linear in dL/dR, so per instance).
-        const int g = sorted_gid[s0 + k];
-        const float4 q = make_float4(quats[4 * (int64_t)g], quats[4 * (int64_t)g + 1], quats[4 * (int64_t)g + 2],
-                                     quats[4 * (int64_t)g + 3]);
-        const float4 dq = quat_grad(q, dR);
-        float4* out = partial + (int64_t)PARTIAL_F4 * sorted_inst[s0 + k];
-        out[0] = make_float4(dmu[0], dmu[1], dmu[2], dtau_raw);
-        out[1] = make_float4(ds[0], ds[1], ds[2], dsh[0]);
-        out[2] = make_float4(dsh[1], dsh[2], dsh[3], 0.f);
-        out[3] = dq;
+        instance_epilogue(rg, r, wr, far_dT, far_exp, dP, dR, ds, dmu, dtau_raw, dsh, quats, sorted_gid[s0 + k],
+                          partial + (int64_t)PARTIAL_F4 * sorted_inst[s0 + k]);
     }
 }
 
@@ -680,6 +1078,16 @@ using namespace us3d::ugr;
 
 static bool g_ugr_sort_attr[128];
 
+// The transmittance checkpoints apply with a quadrature window (its far factor is constant) and
+// full transmission (the local-window mode bounds the product differently); forward and
+// backward take the same decision from the same arguments.
+static inline bool uses_checkpoints(int H, float wr, int local_only) { return H > 0 && wr > 0.0f && !local_only; }
+
+// Blocks per ray for the per-instance kernels: enough to give every SM several (a frame has few rays).
+static inline unsigned per_ray_blocks(int W) {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(64, (148 * 8 + W - 1) / std::max<int64_t>(W, 1)));
+}
+
 extern "C" size_t us3d_ugr_workspace_bytes(int64_t n_gauss, int32_t W, int32_t H, int64_t cap) {
     if (n_gauss < 0 || W <= 0 || H < 0 || cap < 0) return 0;
     return carve(nullptr, n_gauss, W, (int64_t)W * H, cap).bytes;
@@ -727,13 +1135,34 @@ extern "C" int us3d_ugr_forward(void* workspace, size_t workspace_bytes, int64_t
                                         w.ray_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(W, n_gauss, w.ray_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_ugr_sort_attr, stream));
-    forward_kernel<<<dim3((unsigned)W, (unsigned)((H + FWD_SAMPLES - 1) / FWD_SAMPLES)), FWD_SAMPLES, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions,
+    const unsigned tiles_y = (unsigned)((H + FWD_SAMPLES - 1) / FWD_SAMPLES);
+    const int* ckpt_rays = nullptr;
+    int launches = 1 + 3 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1;
+    if (uses_checkpoints(H, quadrature_window_radius_mm, local_window_only)) {
+        const unsigned by = per_ray_blocks(W);
+        ray_depth_kernel<<<(unsigned)W, 256, 0, stream>>>(W, H, w.header, pixel_positions, ray_origins, ray_dirs,
+                                                          axis_ele, ray_perturbations, w.t_pix, w.mono);
+        US3D_CHECK_CUDA(cudaMemsetAsync(w.far_log, 0, sizeof(long long) * (size_t)P, stream));
+        far_prep_kernel<<<dim3((unsigned)W, by), 128, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec,
+                                                                  ray_origins, ray_dirs, axis_ele, ray_perturbations,
+                                                                  w.mono, w.t_pix, k_sigma, quadrature_window_radius_mm,
+                                                                  w.aux, w.far_log);
+        far_prefix_kernel<<<(unsigned)W, 32, 0, stream>>>(W, H, w.header, w.mono, w.far_log, w.t_far);
+        forward_ckpt_kernel<<<dim3((unsigned)W, tiles_y), FWD_SAMPLES, 0, stream>>>(
+            W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions, ray_origins, ray_dirs, axis_ele,
+            ray_perturbations, w.mono, w.t_pix, w.aux, w.t_far, quadrature_window_radius_mm, out_image,
+            w.pixel_state);
+        US3D_CHECK_LAUNCH("ugr checkpointed forward");
+        ckpt_rays = w.mono;
+        launches += 4;
+    }
+    forward_kernel<<<dim3((unsigned)W, tiles_y), FWD_SAMPLES, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.header, w.rec, pixel_positions,
                                                     ray_origins, ray_dirs, axis_ele, ray_perturbations, w.dkey,
                                                     k_sigma, quadrature_window_radius_mm, local_window_only ? 1 : 0,
-                                                    local_max_window_mm, out_image, w.pixel_state);
+                                                    local_max_window_mm, ckpt_rays, out_image, w.pixel_state);
     US3D_CHECK_LAUNCH("ugr forward");
     prof_end(prof, stream);
-    count_launches(1 + 3 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
+    count_launches(launches);
     return US3D_OK;
 }
 
@@ -766,20 +1195,32 @@ extern "C" int us3d_ugr_backward(void* workspace, int64_t n_gauss, const float* 
     cudaStream_t stream = (cudaStream_t)stream_;
     float4* partial = reinterpret_cast<float4*>(scratch);
     const int prof = prof_begin("ugr_backward", stream);
-    // enough blocks per ray to give every SM several (a frame has few rays)
-    const unsigned by = (unsigned)std::max<int64_t>(1, std::min<int64_t>(64, (148 * 8 + W - 1) / std::max<int64_t>(W, 1)));
+    const unsigned by = per_ray_blocks(W);
+    const int* ckpt_rays = nullptr;
+    int launches = 1 + (n_gauss > 0);
+    if (uses_checkpoints(H, quadrature_window_radius_mm, local_window_only)) {
+        ckpt_coef_kernel<<<(unsigned)W, 32, 0, stream>>>(W, H, w.header, w.mono, pixel_positions, w.t_pix,
+                                                         w.pixel_state, grad_image, w.b_pos, w.b_coef, w.b_suffix);
+        backward_ckpt_kernel<<<dim3((unsigned)W, by), 128, 0, stream>>>(
+            W, H, w.ray_start, w.sorted_gid, w.sorted_inst, w.header, w.rec, quats, ray_origins, ray_dirs, axis_ele,
+            ray_perturbations, w.mono, w.t_pix, w.aux, w.b_pos, w.b_coef, w.b_suffix, quadrature_window_radius_mm,
+            partial);
+        US3D_CHECK_LAUNCH("ugr checkpointed backward");
+        ckpt_rays = w.mono;
+        launches += 2;
+    }
     backward_kernel<<<dim3((unsigned)W, by), 128, 0, stream>>>(W, H, w.ray_start, w.sorted_gid, w.sorted_inst, w.header, w.rec,
                                                      quats, pixel_positions, ray_origins, ray_dirs, axis_ele,
                                                      ray_perturbations, w.dkey, w.pixel_state, grad_image, k_sigma,
                                                      quadrature_window_radius_mm, local_window_only ? 1 : 0,
-                                                     local_max_window_mm, partial);
+                                                     local_max_window_mm, ckpt_rays, partial);
     if (n_gauss > 0)
         reduce_kernel<<<(unsigned)((n_gauss + 255) / 256), 256, 0, stream>>>(n_gauss, w.inst_offset, w.header, partial,
                                                                               d_means, d_scales, d_quats,
                                                                               d_attenuations, d_sh);
     US3D_CHECK_LAUNCH("ugr backward");
     prof_end(prof, stream);
-    count_launches(1 + (n_gauss > 0));
+    count_launches(launches);
     return US3D_OK;
 }
 
