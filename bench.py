@@ -71,7 +71,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-train", action="store_true", help="skip the training-step measurement")
     ap.add_argument("--launch-shape", default=None,
-                    help="forward batch / backward threads, e.g. 512/256, instead of autotuning")
+                    help="forward batch / backward threads [/ backward variant 0 scalar, 1 packed], e.g. "
+                         "512/256/1, instead of autotuning")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -249,11 +250,14 @@ def run_b200(a):
         return max_over_ranks(st.elapsed_time(en), device=dev)
 
     # -- launch-shape autotuning on the first batch (untimed; changes no result) --
-    from us3d_b200.batch import autotune_launch, set_launch_config
+    from us3d_b200.batch import autotune_launch, set_backward_variant, set_launch_config
 
     if a.launch_shape:
         launch_shape = tuple(int(x) for x in a.launch_shape.split("/"))
-        set_launch_config(*launch_shape)
+        if len(launch_shape) == 2:
+            launch_shape = (*launch_shape, 1)
+        set_launch_config(launch_shape[0], launch_shape[1])
+        set_backward_variant(launch_shape[2])
         tuned = {}
     else:
         tuned = autotune_launch(batches[0][0], params, batches[0][1])
@@ -349,7 +353,8 @@ def run_b200(a):
         "clocks": clocks, "gpu_launches": gpu_launches,
         "batched_form": "CUDA-graph replay of bin + forward + L1 gradient + backward per 16-frame batch",
         "launch_config": {"forward_batch": launch_shape[0], "backward_threads": launch_shape[1],
-                          "autotune_ms_per_step": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in tuned.items()}},
+                          "backward_variant": ["scalar fp32", "packed fp32x2"][launch_shape[2]],
+                          "autotune_ms_per_step": {f"{k[0]}/{k[1]}/{k[2]}": round(v, 3) for k, v in tuned.items()}},
         "uncaptured": {"value": round(uncaptured_value, 3), "unit": UNIT,
                        "note": "same step launched from Python with one instance-total readback; "
                                "the roofline stage times come from this run's CUDA events"},

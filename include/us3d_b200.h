@@ -213,6 +213,14 @@ US3D_API int us3d_ug_backward(void* workspace, const us3d_slice_frame* frames_de
 US3D_API int us3d_ug_set_launch_config(int32_t forward_batch, int32_t backward_threads);
 US3D_API int us3d_ug_get_launch_config(int32_t* forward_batch, int32_t* backward_threads);
 
+/* Backward kernel variant of the UltraGauss shading adjoint (process-wide, read at every
+ * launch): 0 = one pixel per FP32 instruction, 1 = two pixels per packed FP32 instruction
+ * (sm_100 f32x2; same pair selection, each lane rounding as the scalar instruction, sums
+ * of even and odd pixels kept apart and added once per instance). Both are deterministic;
+ * they differ in summation order only. Default 0. No counterpart in the reference. */
+US3D_API int us3d_ug_set_backward_variant(int32_t variant);
+US3D_API int us3d_ug_get_backward_variant(int32_t* variant);
+
 /*
  * Per-frame image loss of the reference's training step (image_loss in
  * pipeline_god_file.py:606-617 with simple_ssim at :627-637): for each frame f of the table,

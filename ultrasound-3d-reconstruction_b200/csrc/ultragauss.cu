@@ -1029,6 +1029,248 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
     }
 }
 
+// ------------------------------------------------------------------------------------
+// Backward with packed FP32 pairs (sm_100 f32x2): two pixels per instruction
+// ------------------------------------------------------------------------------------
+//
+// Same work split and pair selection as backward_kernel (window implied by the chi-square
+// test), but each thread sweeps the two horizontally adjacent pixels of a sub-block row pair
+// at once: the pixels' positions and adjoint coefficients are staged as lane pairs, the
+// instance's constants are broadcast into pairs, and the quadratic form, the adjoint products
+// and the twelve gradient sums run as fma/mul/add.rn.ftz.f32x2, each lane rounding exactly as
+// the scalar instruction. The quadratic form keeps the reference's term order with the
+// contractions of the compiled scalar expression (QUAD_ORDER), so each lane's q, and hence the
+// q <= chi2 decision, is bit-identical to the forward's. The sums of even and odd pixels are
+// kept apart and added once per instance (deterministic; a different but fixed summation
+// order from backward_kernel's).
+
+#ifndef US3D_UG_QUAD_ORDER
+#define US3D_UG_QUAD_ORDER 1
+#endif
+
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pk2(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void up2(f32x2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 r;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+// a*b + c*d + e*f with the compiled scalar expression's contractions
+__device__ __forceinline__ f32x2 tri2(f32x2 a, f32x2 b, f32x2 c, f32x2 d, f32x2 e, f32x2 f) {
+#if US3D_UG_QUAD_ORDER == 1
+    return fma2(e, f, fma2(c, d, mul2(a, b)));
+#else
+    return fma2(e, f, fma2(a, b, mul2(c, d)));
+#endif
+}
+
+template <bool LOSS, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
+backward_packed_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames,
+                       const int* __restrict__ tile_frame, const int* __restrict__ tile_start,
+                       const int* __restrict__ sorted_gid, const int* __restrict__ sorted_inst,
+                       const blockmask_t* __restrict__ sorted_mask, const long long* __restrict__ header,
+                       const float4* __restrict__ pack, const float* __restrict__ pixels,
+                       const float* __restrict__ d_image, const float* __restrict__ d_alpha,
+                       const float* __restrict__ d_depth, const float* __restrict__ saved_alpha,
+                       const float2* __restrict__ pixel_aux, float chi2, float beta, float bg_alpha,
+                       float bg_intensity, const float* __restrict__ loss_image, const float* __restrict__ loss_target,
+                       const float4* __restrict__ loss_coef, float4* __restrict__ partial) {
+    constexpr int PAIRS = TILE_PIX / 2;       // 128 pixel pairs per tile
+    constexpr int SUB_PAIRS = SUB_PIX / 2;    // 8 per sub-block
+    // Per sub-block c, entries [16 c, 16 c + 16) hold its 8 pairs twice, so that the sweep
+    // rotated by c mod 8 reads 8 consecutive entries from 16 c + (c mod 8).
+    __shared__ float4 s_a[2 * PAIRS];  // (x0, x1, y0, y1)
+    __shared__ float4 s_b[2 * PAIRS];  // (z0, z1, dnum0, dnum1)
+    __shared__ float4 s_c[2 * PAIRS];  // (dtot0, dtot1, ddw0, ddw1)
+    __shared__ short s_perm[BWD_CHUNK];
+    __shared__ int s_class[NSUB + 1];
+    const int64_t t = blockIdx.x;
+    if (t >= T || header[H_FLAGS] != 0) return;
+    const int s0 = tile_start[t];
+    const int n = tile_start[t + 1] - s0;
+    if (n <= 0 || tile_frame[t] < 0) return;
+    const Geo geo = load_geo(frames + tile_frame[t]);
+    int tx, ty;
+    find_tile_coords(geo, t, tx, ty);
+    for (int ps = threadIdx.x; ps < PAIRS; ps += THREADS) {
+        const int sc = ps / SUB_PAIRS, wp = ps % SUB_PAIRS;
+        float px[2], py[2], pz[2], dn[2], dt[2], dd[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int within = 2 * wp + h;
+            const int r = (sc / (TILE / SUB)) * SUB + within / SUB, c = (sc % (TILE / SUB)) * SUB + within % SUB;
+            const int64_t p = (int64_t)geo.pix_off + (int64_t)(ty * TILE + r) * geo.W + (tx * TILE + c);
+            px[h] = py[h] = pz[h] = dn[h] = dt[h] = dd[h] = 0.f;  // outside the frame: every term vanishes
+            if (ty * TILE + r < geo.H && tx * TILE + c < geo.W && p < P) {
+                // Per-pixel adjoint coefficients (reference src/shader/backward.cu:175-197).
+                const float sum_alpha = saved_alpha[p] - bg_alpha;
+                const float2 aux = pixel_aux[p];
+                const float alpha_total = sum_alpha + bg_alpha;
+                const float inv_alpha = 1.0f / fmaxf(alpha_total, 1e-8f);
+                const float num = aux.x + bg_alpha * bg_intensity;
+                float gI, gA, gD;
+                if (LOSS) {
+                    const float x = loss_image[p], y = loss_target[p];
+                    const float4 k = loss_coef[tile_frame[t]];
+                    gI = k.x * (float)((x > y) - (x < y)) + k.y + k.z * x + k.w * y;
+                    gA = 0.f;
+                    gD = 0.f;
+                } else {
+                    gI = d_image[p];
+                    gA = d_alpha[p];
+                    gD = d_depth[p];
+                }
+                const float inv_sa = 1.0f / fmaxf(sum_alpha, 1e-8f);
+                px[h] = pixels[3 * p];
+                py[h] = pixels[3 * p + 1];
+                pz[h] = pixels[3 * p + 2];
+                dn[h] = gI * inv_alpha;
+                dt[h] = (gA - gI * num * inv_alpha * inv_alpha) + (-gD * aux.y * inv_sa * inv_sa);
+                dd[h] = gD * inv_sa;
+            }
+        }
+        const int e0 = sc * (2 * SUB_PAIRS) + wp, e1 = e0 + SUB_PAIRS;
+        s_a[e0] = s_a[e1] = make_float4(px[0], px[1], py[0], py[1]);
+        s_b[e0] = s_b[e1] = make_float4(pz[0], pz[1], dn[0], dn[1]);
+        s_c[e0] = s_c[e1] = make_float4(dt[0], dt[1], dd[0], dd[1]);
+    }
+    const bool culled = header[H_MODE] != 0;
+    const f32x2 zero2 = pk2(0.f, 0.f);
+
+    for (int c0 = 0; c0 < n; c0 += BWD_CHUNK) {
+        const int nc = min(BWD_CHUNK, n - c0);
+        if (threadIdx.x <= NSUB) s_class[threadIdx.x] = 0;
+        __syncthreads();
+        if (culled) {
+            for (int k = threadIdx.x; k < nc; k += blockDim.x)
+                atomicAdd(&s_class[NSUB - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int acc = 0;
+                for (int i = 0; i <= NSUB; ++i) {
+                    const int v = s_class[i];
+                    s_class[i] = acc;
+                    acc += v;
+                }
+            }
+            __syncthreads();
+            for (int k = threadIdx.x; k < nc; k += blockDim.x)
+                s_perm[atomicAdd(&s_class[NSUB - __popc((unsigned)sorted_mask[s0 + c0 + k])], 1)] = (short)k;
+            __syncthreads();
+        }
+        for (int r0 = 0; r0 < nc; r0 += THREADS) {
+            const int wi = threadIdx.x >> 5;
+            const int i = r0 + (((r0 / THREADS) & 1) ? (THREADS / 32 - 1 - wi) * 32 + (threadIdx.x & 31)
+                                                     : (int)threadIdx.x);
+            if (i >= nc) continue;
+            const int k = s0 + c0 + (culled ? (int)s_perm[i] : i);
+            const int g = sorted_gid[k];
+            const int inst = sorted_inst[k];
+            const unsigned blocks = sorted_mask[k];
+            const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+            float4 q1;
+            float s12, s22;
+            precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
+            const float dterm = f3_dot(f3_sub(make_float3(a.x, a.y, a.z), geo.o), geo.ele);
+            const float o = a.w, ci = c.z;
+            const f32x2 MX = pk2(a.x, a.x), MY = pk2(a.y, a.y), MZ = pk2(a.z, a.z);
+            const f32x2 Q0 = pk2(q1.x, q1.x), Q1 = pk2(q1.y, q1.y), Q2 = pk2(q1.z, q1.z), Q3 = pk2(q1.w, q1.w);
+            const f32x2 S12 = pk2(s12, s12), S22 = pk2(s22, s22), CI = pk2(ci, ci), DT = pk2(dterm, dterm);
+            f32x2 acc_c = zero2, acc_o = zero2, acc_e = zero2, sdx = zero2, sdy = zero2, sdz = zero2;
+            f32x2 sxx = zero2, sxy = zero2, sxz = zero2, syy = zero2, syz = zero2, szz = zero2;
+            for (unsigned mb = blocks; mb != 0u; mb &= mb - 1u) {
+                const int blk = __ffs(mb) - 1;
+                const int base = blk * (2 * SUB_PAIRS) + (blk & (SUB_PAIRS - 1));
+#pragma unroll
+                for (int jj = 0; jj < SUB_PAIRS; ++jj) {
+                    const float4 va = s_a[base + jj], vb = s_b[base + jj], vc = s_c[base + jj];
+                    const f32x2 dx = sub2(pk2(va.x, va.y), MX), dy = sub2(pk2(va.z, va.w), MY),
+                                dz = sub2(pk2(vb.x, vb.y), MZ);
+                    const f32x2 dn = pk2(vb.z, vb.w), gx = pk2(vc.x, vc.y), gy = pk2(vc.z, vc.w);
+                    // quadratic form in the reference's term order (quad_form), per lane
+                    const f32x2 t0 = tri2(Q0, dx, Q1, dy, Q2, dz);
+                    const f32x2 t1 = tri2(Q1, dx, Q3, dy, S12, dz);
+                    const f32x2 t2 = tri2(Q2, dx, S12, dy, S22, dz);
+                    const f32x2 q = tri2(t0, dx, t1, dy, t2, dz);
+                    float q0, q1v;
+                    up2(q, q0, q1v);
+                    const float w0 = q0 <= chi2 ? exp2f(q0 * kNegHalfLog2e) : 0.0f;
+                    const float w1 = q1v <= chi2 ? exp2f(q1v * kNegHalfLog2e) : 0.0f;
+                    const f32x2 w = pk2(w0, w1);
+                    const f32x2 dah = fma2(gy, DT, fma2(dn, CI, gx));
+                    const f32x2 dw = mul2(dah, w);
+                    acc_c = fma2(dn, w, acc_c);
+                    acc_o = add2(acc_o, dw);
+                    acc_e = fma2(gy, w, acc_e);
+                    const f32x2 ux = mul2(dw, dx), uy = mul2(dw, dy), uz = mul2(dw, dz);
+                    sdx = add2(sdx, ux);
+                    sdy = add2(sdy, uy);
+                    sdz = add2(sdz, uz);
+                    sxx = fma2(ux, dx, sxx);
+                    sxy = fma2(ux, dy, sxy);
+                    sxz = fma2(ux, dz, sxz);
+                    syy = fma2(uy, dy, syy);
+                    syz = fma2(uy, dz, syz);
+                    szz = fma2(uz, dz, szz);
+                }
+            }
+            auto fold = [](f32x2 v) {
+                float lo, hi;
+                up2(v, lo, hi);
+                return lo + hi;
+            };
+            // The pairs' common factors, applied once per instance: -o/2 of dL/dq, o of the
+            // alpha-hat sums.
+            const float nh = -0.5f * o;
+            const float Sdx = fold(sdx) * nh, Sdy = fold(sdy) * nh, Sdz = fold(sdz) * nh;
+            const float Sxx = fold(sxx) * nh, Sxy = fold(sxy) * nh, Sxz = fold(sxz) * nh;
+            const float Syy = fold(syy) * nh, Syz = fold(syz) * nh, Szz = fold(szz) * nh;
+            const float Ac = fold(acc_c) * o, Ao = fold(acc_o), Ae = fold(acc_e) * o;
+            const float vx = q1.x * Sdx + q1.y * Sdy + q1.z * Sdz;
+            const float vy = q1.y * Sdx + q1.w * Sdy + s12 * Sdz;
+            const float vz = q1.z * Sdx + s12 * Sdy + s22 * Sdz;
+            const float l11 = b.x * b.x + beta, l12 = b.y, l13 = b.z;
+            const float l22 = b.w * b.w + beta, l23 = c.x, l33 = c.y * c.y + beta;
+            const float dl11 = 2.0f * (Sxx * l11 + Sxy * l12 + Sxz * l13);
+            const float dl12 = 2.0f * (Sxy * l11 + Syy * l12 + Syz * l13);
+            const float dl13 = 2.0f * (Sxz * l11 + Syz * l12 + Szz * l13);
+            const float dl22 = 2.0f * (Syy * l22 + Syz * l23);
+            const float dl23 = 2.0f * (Syz * l22 + Szz * l23);
+            const float dl33 = 2.0f * (Szz * l33);
+            float4* out = partial + 3 * (int64_t)inst;
+            out[0] = make_float4(-2.0f * vx + Ae * geo.ele.x, -2.0f * vy + Ae * geo.ele.y,
+                                 -2.0f * vz + Ae * geo.ele.z, Ao);
+            out[1] = make_float4(dl11 * (2.0f * b.x), dl12, dl13, dl22 * (2.0f * b.w));
+            out[2] = make_float4(dl23, dl33 * (2.0f * c.y), Ac, 0.f);
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(256)
 reduce_kernel(int64_t G, const int* __restrict__ inst_offset, const long long* __restrict__ header,
               const float4* __restrict__ partial, float* __restrict__ d_means, float* __restrict__ d_tril,
@@ -1169,6 +1411,8 @@ static bool g_sort_attr_done[128];
 // Launch shapes of the shading kernels (process-wide; read at every launch).
 static std::atomic<int> g_fwd_batch{FWD_BATCH};
 static std::atomic<int> g_bwd_threads{BWD_THREADS};
+// Backward kernel variant: 0 scalar FP32, 1 packed FP32 pairs (backward_packed_kernel).
+static std::atomic<int> g_bwd_variant{0};
 
 extern "C" int us3d_ug_set_launch_config(int32_t forward_batch, int32_t backward_threads) {
     US3D_CHECK_ARG(forward_batch == 128 || forward_batch == 256 || forward_batch == 512,
@@ -1183,6 +1427,19 @@ extern "C" int us3d_ug_set_launch_config(int32_t forward_batch, int32_t backward
 extern "C" int us3d_ug_get_launch_config(int32_t* forward_batch, int32_t* backward_threads) {
     if (forward_batch) *forward_batch = g_fwd_batch.load();
     if (backward_threads) *backward_threads = g_bwd_threads.load();
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_set_backward_variant(int32_t variant) {
+    US3D_CHECK_ARG(variant == 0 || variant == 1, "backward variant must be 0 (scalar) or 1 (packed pairs), got %d",
+                   variant);
+    g_bwd_variant.store(variant);
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_get_backward_variant(int32_t* variant) {
+    US3D_CHECK_ARG(variant != nullptr, "variant is NULL");
+    *variant = g_bwd_variant.load();
     return US3D_OK;
 }
 
@@ -1418,8 +1675,15 @@ static int ug_backward_impl(void* workspace, const us3d_slice_frame* frames, int
                 w.header, w.pack, pixels, d_image, d_alpha, d_depth, saved_alpha, w.pixel_aux, chi2, beta, bg_alpha,
                 bg_intensity, loss_image, loss_target, loss_coef, partial);
         };
+        const bool packed = g_bwd_variant.load() == 1;
         if (!window_implied(beta))
             fused ? launch(backward_kernel<true, 256, true>, 256) : launch(backward_kernel<false, 256, true>, 256);
+        else if (packed && fused)
+            threads == 128 ? launch(backward_packed_kernel<true, 128>, 128)
+                           : launch(backward_packed_kernel<true, 256>, 256);
+        else if (packed)
+            threads == 128 ? launch(backward_packed_kernel<false, 128>, 128)
+                           : launch(backward_packed_kernel<false, 256>, 256);
         else if (fused)
             threads == 128 ? launch(backward_kernel<true, 128, false>, 128)
                            : launch(backward_kernel<true, 256, false>, 256);
