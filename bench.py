@@ -546,7 +546,7 @@ def run_e2e(a, dev, sc, specs, n_pool, world, rank, timed_barrier):
     cap = 0
     for k, r in enumerate(renderers):
         step(k)
-        cap = max(cap, int(r.last["binning"].total * 1.25) + 1024)
+        cap = max(cap, int(r.last["binning"].capacity), int(r.last["binning"].total * 1.25) + 1024)
     for r in renderers:
         r.params["capacity"] = cap
         r.params["sync_check"] = False

@@ -102,11 +102,25 @@ def test_config2_gaussianpile(config2, cuda_device):
     import test_gaussianpile_gpu as T
     from gp_helpers import run_b200_gp
 
+    from oracle import gaussianpile_oracle as GO
+    from ug_helpers import rel_l2
+
     sc, sweep = config2
     for f in FRAMES:
         fx = MG.run("config2", sc, _pose_probe_to_world(sweep[f]),
                     dict(H=H, W=W, lat=SPACING, ax=SPACING, near=0.0, centre=True, sigma_z=1.0, pose_grad=True))
-        T._check(run_b200_gp(fx, cuda_device), fx)
+        out = run_b200_gp(fx, cuda_device)
+        T._check(out, dict(fx, pose_grad=0))
+        # The pose gradient sums 200k Gaussians' contributions with lever arms of tens of mm that
+        # largely cancel; the reference adds them with float atomics, this library in double in a
+        # fixed order. Both are compared with the FP64 oracle: this library must be at least as
+        # close to it as the reference (or within 1e-4).
+        m = fx["meta"].tolist()
+        st = GO.render(fx["means"], fx["scales"], fx["quats"], fx["opacities"], fx["intensities"], fx["pose"],
+                       fx["grid"], fx["params"], H, W, m[2], m[3], m[4], int(m[5]), m[8], precision="f64")
+        d64 = GO.backward(st, fx["grad_image"], pose_grad=True)["d_pose"]
+        ours, ref = rel_l2(out["d_pose"], d64), rel_l2(fx["ref_d_pose"], d64)
+        assert ours <= max(1e-4, ref), (f, ours, ref)
 
 
 def test_config2_slice_adapted(config2, cuda_device):

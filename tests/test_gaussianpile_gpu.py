@@ -235,5 +235,6 @@ def test_gaussianpile_shape_gradients_reference_floor(cuda_device):
         report[k] = dict(floor=floor, ours_fd=ours, ref_vs_analytic=rel_l2(r1["ref_" + k], an))
     print("gaussianpile shape-gradient floor:", report)
     for k, r in report.items():
-        assert r["ours_fd"] <= max(1e-4, 2.0 * r["floor"]) or r["ours_fd"] <= 1e-3, (k, r)
+        # the finite-difference mode here is one more "run" of the same noisy difference quotient
+        assert r["ours_fd"] <= max(1e-4, 4.0 * r["floor"]), (k, r)
         assert r["ref_vs_analytic"] <= 1e-2, (k, r)

@@ -116,7 +116,7 @@ def _fd_check(loss, base, analytic, names, h=1e-4, picks=24, seed=0, tol=1e-4):
                 plus[which].reshape(-1)[fi] += step
                 minus[which].reshape(-1)[fi] -= step
                 d.append((loss(*plus) - loss(*minus)) / (2 * step))
-            if abs(d[0] - d[1]) > 1e-3 * max(abs(d[0]), 1e-8):
+            if not all(np.isfinite(d)) or abs(d[0] - d[1]) > 1e-3 * max(abs(d[0]), 1e-8):
                 continue
             fd.append(d[0])
             an.append(analytic[which].reshape(-1)[fi])
@@ -169,7 +169,7 @@ def test_slice_projection_gradients_fd64(cuda_device):
 
     g = torch.Generator().manual_seed(23)
     G = 80
-    means = (torch.rand(G, 3, generator=g) - 0.5) * torch.tensor([20.0, 16.0, 1.0])
+    means = (torch.rand(G, 3, generator=g) - 0.5) * torch.tensor([20.0, 16.0, 8.0])
     scales = torch.exp(torch.randn(G, 3, generator=g) * 0.3) * 0.8
     quats = torch.randn(G, 4, generator=g)
     opac = torch.rand(G, 1, generator=g) * 0.8 + 0.1
@@ -192,7 +192,8 @@ def test_slice_projection_gradients_fd64(cuda_device):
 
     def loss(mm, ss, qq, oo, cc):
         pr = PO.project(mm, ss, qq, oo, cc, V.numpy(), 0.0, 0.3, 3.0, 1.0, 1e-4, True)
-        assert np.array_equal(np.nonzero(pr["keep"])[0], kept)
+        if not np.array_equal(np.nonzero(pr["keep"])[0], kept):
+            return float("nan")  # the step moved a Gaussian across the cull: no derivative there
         return float((pr["means2d"] * wm.double().numpy()).sum() + (pr["inv2d"] * wi.double().numpy()).sum()
                      + (pr["weights"] * ww.double().numpy()).sum() + (pr["colors"] * wc.double().numpy()).sum())
 

@@ -152,9 +152,12 @@ def test_ultrags_gradients_fd64(cuda_device):
     """The surfel rasteriser's GPU backward against central differences (step 1e-4) of the
     FP64 oracle's colour image, for the parameters whose reference gradient is the derivative
     of its forward (3D means, scales, rotations, opacities, degree-0 SH; the screen-space
-    means2D gradient is the reference's densification statistic, not a derivative). A pick
-    whose differences at h and h/8 disagree crossed one of the forward's cuts (the alpha
-    threshold 1/255, the bounding box, the 0.99 clamp) and is left out."""
+    means2D gradient is the reference's densification statistic, not a derivative). The
+    reference's rotation gradient is taken w.r.t. the normalised quaternion (its VJP stops at
+    q / |q|), so with unit quaternions it is compared after projection onto the tangent space
+    (I - q q^T), which is the derivative of the forward. A pick whose differences at h and h/8
+    disagree crossed one of the forward's cuts (the alpha threshold 1/255, the bounding box,
+    the 0.99 clamp) and is left out."""
     import math
 
     from oracle import surfel_oracle as SO
@@ -163,7 +166,12 @@ def test_ultrags_gradients_fd64(cuda_device):
     # focal length, int(focal * tan_fov * 2), is then exactly the forward's
     scene = make_scene(40, 48, 48, 31, sh_degree=0, scale_range=(0.08, 0.3), fovx_deg=math.degrees(2 * math.atan(0.5)))
     scene["grad_others"] = np.zeros_like(scene["grad_others"])
+    q = scene["quats"].astype(np.float64)
+    scene["quats"] = np.ascontiguousarray(q / np.linalg.norm(q, axis=1, keepdims=True), dtype=np.float32)
     out = run_b200_gs(scene, cuda_device)
+    qn = scene["quats"].astype(np.float64)
+    g = out["d_rot"].reshape(-1, 4).astype(np.float64)
+    out["d_rot"] = g - qn * (g * qn).sum(1, keepdims=True)
     wc = scene["grad_color"].astype(np.float64)
     keys = ("means", "scales", "quats", "opacities", "shs")
     s64 = {k: (v.astype(np.float64) if isinstance(v, np.ndarray) else v) for k, v in scene.items()}

@@ -682,11 +682,14 @@ __device__ float shape_fd(const float* m, const float* s, const float* q, bool i
 
 // Exact shape gradient (analytic mode; the reference has only the central differences
 // above): the adjoint of the probe-frame covariance, g_Sc (from the same chain through Se and
-// Lc that gives the mean and pose gradients), is carried back through
-// Sc = A^T Sigma_w A + 1e-6 I, Sigma_w = R diag(s^2) R^T and R = rot(q / |q|):
-//   dL/dSigma_w = sum_ij g_Sc[i][j] a_i a_j^T, dL/ds_k = 2 s_k (R^T G R)_kk (0 where the
-//   1e-6 floor of the scale is active), dL/dR = (G + G^T) R diag(s^2), and dL/dq through the
-//   rotation of the normalised quaternion and the normalisation.
+// Lc that gives the mean and pose gradients), is carried back through Sc = A^T Sigma_w A +
+// 1e-6 I (Sc_ij = a_i^T Sigma_w a_j), the world covariance exactly as sigma_world forms it,
+// Sigma_w = R D R with D = diag(s^2) (the reference's product, R from quat_rot), and
+// R = rot(q / |q|):
+//   G = dL/dSigma_w = sum_ij g_Sc[i][j] a_i a_j^T,
+//   dL/ds_k = 2 s_k sum_ij G_ij R_ik R_kj (0 where the 1e-6 floor of the scale is active),
+//   dL/dR = G R^T D + D R^T G, and dL/dq through the rotation of the normalised quaternion and
+//   the normalisation.
 __device__ void shape_analytic(const float* s, const float* q, const Axes& A, const float g_Sc[9], float d_s[3],
                                float d_q[4]) {
     const float3 ax[3] = {A.lat, A.ax, A.ele};
@@ -714,22 +717,25 @@ __device__ void shape_analytic(const float* s, const float* q, const Axes& A, co
     for (int k = 0; k < 3; ++k) {
         const float sk = fmaxf(sv[k], 1e-6f);
         D[k] = sk * sk;
-        float rgr = 0.f;  // (R^T G R)_kk
+        float acc = 0.f;  // sum_ij G_ij R_ik R_kj
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+        for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int b = 0; b < 3; ++b) rgr += R[a * 3 + k] * G[a * 3 + b] * R[b * 3 + k];
-        d_s[k] = sv[k] > 1e-6f ? 2.f * sk * rgr : 0.f;
+            for (int j = 0; j < 3; ++j) acc += G[i * 3 + j] * R[i * 3 + k] * R[k * 3 + j];
+        d_s[k] = sv[k] > 1e-6f ? 2.f * sk * acc : 0.f;
     }
-    float gR[9];  // dL/dR = (G + G^T) R D
+    float gR[9];  // dL/dR = G R^T D + D R^T G
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            float acc = 0.f;
+        for (int b = 0; b < 3; ++b) {
+            float u = 0.f, v = 0.f;
 #pragma unroll
-            for (int b = 0; b < 3; ++b) acc += (G[a * 3 + b] + G[b * 3 + a]) * R[b * 3 + k];
-            gR[a * 3 + k] = acc * D[k];
+            for (int c = 0; c < 3; ++c) {
+                u += G[a * 3 + c] * R[b * 3 + c];
+                v += R[c * 3 + a] * G[c * 3 + b];
+            }
+            gR[a * 3 + b] = u * D[b] + D[a] * v;
         }
     // R of the unit quaternion (w, x, y, z) as in quat_rot; derivative per component
     const float n2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
@@ -912,8 +918,12 @@ finalize_kernel(int64_t G, float k_sigma, const int* __restrict__ inst_offset, c
 // first slot of pose_partial; one block then adds the chunk sums in block order.
 constexpr int POSE_BLOCKS = 512;
 
-__device__ __forceinline__ void pose_block_sum(float a[12]) {
-    __shared__ float red[256][13];
+// The pose gradient is a sum over all Gaussians of terms with long lever arms that largely
+// cancel, so the sums run in double: per-Gaussian float contributions, chunk sums and the final
+// sum accumulate in double (fixed order), and the chunk sums stay in double (two float slots
+// each, in the chunk's own first Gaussians' slots; chunks hold at least two Gaussians).
+__device__ __forceinline__ void pose_block_sum(double a[12]) {
+    __shared__ double red[256][13];
 #pragma unroll
     for (int i = 0; i < 12; ++i) red[threadIdx.x][i] = a[i];
     __syncthreads();
@@ -932,30 +942,33 @@ pose_chunk_kernel(int64_t G, int64_t chunk, float* __restrict__ pose_partial) {
     const int64_t g0 = (int64_t)blockIdx.x * chunk;
     if (g0 >= G) return;
     const int64_t g1 = g0 + chunk < G ? g0 + chunk : G;
-    float a[12];
+    double a[12];
 #pragma unroll
-    for (int i = 0; i < 12; ++i) a[i] = 0.f;
+    for (int i = 0; i < 12; ++i) a[i] = 0.0;
     for (int64_t g = g0 + threadIdx.x; g < g1; g += blockDim.x)
 #pragma unroll
-        for (int i = 0; i < 12; ++i) a[i] += pose_partial[12 * g + i];
+        for (int i = 0; i < 12; ++i) a[i] += (double)pose_partial[12 * g + i];
     pose_block_sum(a);  // ends with every read of the chunk done
-    if (threadIdx.x < 12) pose_partial[12 * g0 + threadIdx.x] = a[threadIdx.x];
+    double* out = reinterpret_cast<double*>(pose_partial + 12 * g0);
+    if (threadIdx.x < 12) out[threadIdx.x] = a[threadIdx.x];
 }
 
 __global__ void __launch_bounds__(256)
 pose_final_kernel(int64_t G, int64_t chunk, const float* __restrict__ pose_partial, float* __restrict__ d_pose) {
     const int nb = (int)((G + chunk - 1) / chunk);
-    float a[12];
+    double a[12];
 #pragma unroll
-    for (int i = 0; i < 12; ++i) a[i] = 0.f;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+    for (int i = 0; i < 12; ++i) a[i] = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        const double* in = reinterpret_cast<const double*>(pose_partial + 12 * (int64_t)b * chunk);
 #pragma unroll
-        for (int i = 0; i < 12; ++i) a[i] += pose_partial[12 * (int64_t)b * chunk + i];
+        for (int i = 0; i < 12; ++i) a[i] += in[i];
+    }
     pose_block_sum(a);
     if (threadIdx.x == 0) {
         const int idx[12] = {0, 4, 8, 1, 5, 9, 2, 6, 10, 3, 7, 11};
         for (int i = 0; i < 16; ++i) d_pose[i] = 0.f;
-        for (int i = 0; i < 12; ++i) d_pose[idx[i]] = a[i];
+        for (int i = 0; i < 12; ++i) d_pose[idx[i]] = (float)a[i];
     }
 }
 
@@ -995,7 +1008,8 @@ extern "C" size_t us3d_gp_workspace_bytes(int64_t n_gauss, int32_t H, int32_t W,
 
 extern "C" size_t us3d_gp_backward_scratch_bytes(int64_t n_gauss, int64_t cap) {
     if (n_gauss < 0 || cap < 0) return 0;
-    return (size_t)cap * PARTIAL_F4 * sizeof(float4) + (size_t)n_gauss * 12 * sizeof(float) + 256;
+    // + 2 Gaussians' pose slots: a chunk's double sums span two slots, also for a last chunk of one
+    return (size_t)cap * PARTIAL_F4 * sizeof(float4) + (size_t)(n_gauss + 2) * 12 * sizeof(float) + 256;
 }
 
 extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t n_gauss, const float* means,
@@ -1107,7 +1121,7 @@ extern "C" int us3d_gp_backward(void* workspace, int64_t n_gauss, const float* m
         ++launches;
     }
     if (pose_grad) {
-        const int64_t chunk = std::max<int64_t>(1, (n_gauss + POSE_BLOCKS - 1) / POSE_BLOCKS);
+        const int64_t chunk = std::max<int64_t>(2, (n_gauss + POSE_BLOCKS - 1) / POSE_BLOCKS);
         if (n_gauss > 0) {
             pose_chunk_kernel<<<(unsigned)((n_gauss + chunk - 1) / chunk), 256, 0, stream>>>(n_gauss, chunk,
                                                                                              pose_partial);

@@ -1044,8 +1044,10 @@ backward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frame
 // kept apart and added once per instance (deterministic; a different but fixed summation
 // order from backward_kernel's).
 
+// The compiled scalar a*b + c*d + e*f rounds as fma(e, f, fma(a, b, c*d)) (order 2; checked
+// on B200 against the scalar expression, zero differences in 6.7e7 random quadratic forms).
 #ifndef US3D_UG_QUAD_ORDER
-#define US3D_UG_QUAD_ORDER 1
+#define US3D_UG_QUAD_ORDER 2
 #endif
 
 typedef unsigned long long f32x2;

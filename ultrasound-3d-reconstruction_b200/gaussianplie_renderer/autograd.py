@@ -73,7 +73,6 @@ class _GaussianPileProjectedSliceCudaFunction(torch.autograd.Function):
     def forward(ctx, gauss_means, gauss_scales, gauss_quats, gauss_opacities, gauss_intensities,
                 pose_probe_to_world, slice_grid_geometry, meta, us_focus_params, shape_gradients=None):
         ctx.shape_gradients = shape_gradients or _default_shape_gradients
-        ctx.mode_given = shape_gradients is not None
         if not gauss_means.is_cuda:
             raise RuntimeError("gaussianplie_renderer requires CUDA tensors: the B200 kernels are the only compute path")
         dev = gauss_means.device
@@ -109,7 +108,8 @@ class _GaussianPileProjectedSliceCudaFunction(torch.autograd.Function):
         md, sd, qd, od, idt = ctx.dtypes
         grads = (dm.to(md), ds.to(sd), dq.to(qd), do.reshape(ctx.shapes[0]).to(od), di.reshape(ctx.shapes[1]).to(idt),
                  dp.to(ctx.pose_dtype), torch.zeros_like(grid), torch.zeros_like(meta), torch.zeros_like(params))
-        return grads + (None,) if ctx.mode_given else grads
+        # one gradient per input given to apply (nine, or ten with the mode)
+        return (grads + (None,))[:len(ctx.needs_input_grad)]
 
 
 def render_gaussianpile_projected_slice(config: GaussianPlieRenderConfig, gauss_means: torch.Tensor,

@@ -88,7 +88,9 @@ class GraphedTrainingStep:
             torch.empty((G, 3), device=device), torch.empty((G, 6), device=device), torch.empty((G,), device=device),
             torch.empty((G,), device=device))
         prime = UG.bin_gaussians(*self.params, self.frames, *self.cfg, slice_cull_pixels=pixels)
-        self.capacity = int(prime.total * margin) + 1024
+        # at least the capacity the priming binning succeeded with: with many small frames the
+        # (Gaussian, frame) pairs, which the capacity also bounds, can outnumber a quarter of it
+        self.capacity = max(int(prime.capacity), int(prime.total * margin) + 1024)
         self.binning = None
         self._run()  # uncaptured: sets kernel attributes and allocator state
         torch.cuda.synchronize(device)

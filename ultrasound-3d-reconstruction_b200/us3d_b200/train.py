@@ -157,7 +157,7 @@ class UltraGaussTrainer:
             frames = specs if isinstance(specs, UG.FrameTable) else UG.build_frame_table(list(specs), dev)
             prime = UG.bin_gaussians(*self._render_args(), frames, self.cfg.chi2_threshold, self.cfg.diag_beta,
                                      self.cfg.sort_by_depth, slice_cull_pixels=pixels, logit_attributes=True)
-            cap = int(prime.total * margin) + 1024
+            cap = max(int(prime.capacity), int(prime.total * margin) + 1024)
             self._batches.append(dict(frames=frames, pixels=pixels, targets=targets, capacity=cap, binning=None,
                                       stats=torch.zeros((frames.n_frames, 8), dtype=torch.float64, device=dev),
                                       coef=torch.zeros((frames.n_frames, 4), device=dev), graph=None))
@@ -190,7 +190,7 @@ class UltraGaussTrainer:
         targets = torch.empty((batch_size * hw,), device=dev)
         draw = torch.empty((batch_size,), dtype=torch.int64, device=dev)
         c = cfg or TrainConfig()
-        best = 0
+        best = worked = 0
         for _ in range(max(1, int(prime_batches))):
             torch.randint(0, pool.numel(), (batch_size,), generator=gen, device=dev, out=draw)
             source.fill(pool[draw], table, pixels, targets)
@@ -198,8 +198,9 @@ class UltraGaussTrainer:
                                  params.raw_intensities.reshape(-1), table, c.chi2_threshold, c.diag_beta,
                                  c.sort_by_depth, slice_cull_pixels=pixels, logit_attributes=True)
             best = max(best, b.total)
+            worked = max(worked, int(b.capacity))
         self = cls(params, [(table, pixels, targets)], c, margin=1.0, graph=graph, refine=refine)
-        self._batches[0]["capacity"] = int(best * margin) + 1024
+        self._batches[0]["capacity"] = max(worked, int(best * margin) + 1024)
         self.source = dict(source=source, pool=pool, gen=gen, draw=draw, prime_batches=max(1, int(prime_batches)),
                            margin=float(margin))
         return self
@@ -265,17 +266,18 @@ class UltraGaussTrainer:
             if self.source is None:
                 prime = UG.bin_gaussians(*self._render_args(), bt["frames"], c.chi2_threshold, c.diag_beta,
                                          c.sort_by_depth, slice_cull_pixels=bt["pixels"], logit_attributes=True)
-                bt["capacity"] = int(prime.total * self.margin) + 1024
+                bt["capacity"] = max(int(prime.capacity), int(prime.total * self.margin) + 1024)
         if self.source is not None:
             sc, bt = self.source, self._batches[0]
-            best = 0
+            best = worked = 0
             for _ in range(sc["prime_batches"]):
                 torch.randint(0, sc["pool"].numel(), sc["draw"].shape, generator=sc["gen"], device=dev, out=sc["draw"])
                 sc["source"].fill(sc["pool"][sc["draw"]], bt["frames"], bt["pixels"], bt["targets"])
                 prime = UG.bin_gaussians(*self._render_args(), bt["frames"], c.chi2_threshold, c.diag_beta,
                                          c.sort_by_depth, slice_cull_pixels=bt["pixels"], logit_attributes=True)
                 best = max(best, prime.total)
-            bt["capacity"] = int(best * sc["margin"]) + 1024
+                worked = max(worked, int(prime.capacity))
+            bt["capacity"] = max(worked, int(best * sc["margin"]) + 1024)
 
     def losses(self, batch_index: int = 0) -> torch.Tensor:
         return self._batches[batch_index]["stats"].cpu()
