@@ -74,6 +74,9 @@ def test_ultragray_bmode_scale_against_reference(cuda_device):
 
     from us3d_b200 import scenes
 
+    from ugr_helpers import SCENE_ARRAYS, params
+    from us3d_b200 import ultragray as U
+
     sc = scenes.make_bmode_scene(1_000_000, seed=0)
     fr = scenes.bmode_sweep(64)[32]
     scene = _scene_dict(sc, fr, 512, 1024, 5)
@@ -82,6 +85,19 @@ def test_ultragray_bmode_scale_against_reference(cuda_device):
     t0 = time.perf_counter()
     run_b200_ugr(scene, cuda_device)
     t_ours = time.perf_counter() - t0
+    # device time of the forward (binning included) and of the backward
+    t = {k: torch.as_tensor(scene[k]).to(cuda_device).contiguous() for k in SCENE_ARRAYS}
+    p = params(scene)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record()
+    _, b = U.forward(t["means"], t["scales"], t["quats"], t["attenuations"], t["sh"], t["pixels"], t["ray_o"],
+                     t["ray_d"], t["origin"], t["lat"], t["ele"], t["ax"], t["pert"], p, capacity=out["total"] + 1024)
+    ev[1].record()
+    U.backward(b, t["quats"], t["pixels"], t["ray_o"], t["ray_d"], t["ele"], t["pert"], t["grad_image"], p)
+    ev[2].record()
+    ev[2].synchronize()
+    print(f"ultragray B-mode device time: forward {ev[0].elapsed_time(ev[1]):.2f} ms, "
+          f"backward {ev[1].elapsed_time(ev[2]):.2f} ms")
     t0 = time.perf_counter()
     ref = run_reference_ugr(REF, scene, cuda_device)
     t_ref = time.perf_counter() - t0

@@ -83,7 +83,7 @@ def make_sweep_batch(n_sweeps: int = 64, g_min: int = 10_000, g_max: int = 1_000
         specs += ss
         pix += [f.pixels for f in sw]
         off += G
-    dev = device or torch.device("cuda")
+    dev = device or torch.device("cuda", torch.cuda.current_device())
     params = [torch.cat(p).to(dev).contiguous() for p in parts]
     pixels = torch.cat(pix).to(dev).contiguous()
     gd = torch.Generator().manual_seed(seed + 99)
@@ -261,7 +261,7 @@ def run_training(n_init: int = 2_000_000, n_gt: int = 4_000_000, n_frames: int =
     from .refine import RefineConfig
     from .train import TrainConfig, UltraGaussParameters, UltraGaussTrainer
 
-    dev = device or torch.device("cuda")
+    dev = device or torch.device("cuda", torch.cuda.current_device())
     t0 = time.perf_counter()
     gt_pts, gt_int = layered_point_cloud(n_gt, seed=seed + 1)
     gt = scenes.make_scene(n_gt, seed=seed + 2, log_scale_mean=math.log(0.35), log_scale_std=0.3)
