@@ -37,23 +37,26 @@ UNIT = "frames/s"
 BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (params, grads, outputs, upstream)
 
 # DRAM bytes (read + write) per frame of each stage's dominant kernel, from one ncu capture
-# of a 4-frame launch of the same scene, scaled linearly to the frames of a launch.
-# dram__bytes_read.sum + dram__bytes_write.sum of one 4-frame launch of the headline scene
-# (ncu --set full), per frame; the backward stage is backward_kernel + reduce_kernel.
+# of a 4-frame launch of the same scene (ncu --set full), scaled linearly to the frames of a
+# launch; the backward stage is the shading adjoint + the per-Gaussian reduce_kernel. Keyed by
+# backward variant (0 scalar FP32, 1 packed FP32x2); the forward is the same kernel for both.
 NCU_TRAFFIC_PER_FRAME = {
-    "ug_backward": (100.252416e6 + 114.988544e6 + 156.020480e6 + 28.401920e6) / 4,
-    "ug_forward": (52.274432e6 + 5.454592e6) / 4,
+    0: {"ug_backward": (100.252416e6 + 114.988544e6 + 156.020480e6 + 28.401920e6) / 4,
+        "ug_forward": (52.274432e6 + 5.454592e6) / 4},
+    1: {"ug_backward": (99.148032e6 + 114.697984e6 + 156.020480e6 + 28.401920e6) / 4,
+        "ug_forward": (52.270336e6 + 5.618176e6) / 4},
 }
 # Warp instructions executed per frame by each stage's kernels (smsp__inst_executed.sum of the
-# same 4-frame capture, per frame): the shading kernels are bound by instruction issue, whose
-# ceiling is 148 SMs x 4 schedulers x one warp instruction per clock.
+# same 4-frame captures, per frame): the shading kernels are bound by instruction issue or by
+# the FMA pipe, whose ceilings are 148 SMs x 4 schedulers x one warp instruction per clock.
 # (per frame, per launch): the per-Gaussian gradient reduction runs once per launch.
 NCU_WARP_INST_PER_FRAME = {
-    "ug_forward": (547342384 / 4, 0.0),
-    "ug_backward": (594881545 / 4, 21e6),
+    0: {"ug_forward": (547342384 / 4, 0.0), "ug_backward": (594881545 / 4, 21e6)},
+    1: {"ug_forward": (547342384 / 4, 0.0), "ug_backward": (377437123 / 4, 21e6)},
 }
-# Share of cycles the FMA pipe was busy in that capture (sm__pipe_fma_cycles_active).
-NCU_FMA_PIPE = {"ug_forward": 0.5172, "ug_backward": 0.6857}
+# Share of cycles the FMA pipe was busy in those captures (sm__pipe_fma_cycles_active).
+NCU_FMA_PIPE = {0: {"ug_forward": 0.5172, "ug_backward": 0.6857},
+                1: {"ug_forward": 0.5178, "ug_backward": 0.7181}}
 SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 
@@ -328,7 +331,7 @@ def run_b200(a):
     peaks = json.load(open(ROOT / "MEASURED_PEAKS.json")) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg / (stage_avg_ms / 1e3) / 1e9
-    traffic = NCU_TRAFFIC_PER_FRAME.get(dominant)
+    traffic = NCU_TRAFFIC_PER_FRAME[launch_shape[2]].get(dominant)
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": int(traffic * F) if traffic else None,
                 "traffic_source": "ncu dram bytes of a 4-frame launch scaled to the launch's frames" if traffic else None,
@@ -342,7 +345,7 @@ def run_b200(a):
     step_gbs = b_frame * frames_total / (ms_batched / 1e3) / 1e9
     roofline["step"] = {"bytes_per_frame": int(b_frame), "achieved": round(step_gbs, 2),
                         "frac": round(step_gbs / peak, 4)}
-    roofline["issue"] = issue_roofline(stage_ms, F, clocks)
+    roofline["issue"] = issue_roofline(stage_ms, F, clocks, launch_shape[2])
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -383,7 +386,7 @@ def run_b200(a):
         print(json.dumps(out), flush=True)
 
 
-def issue_roofline(stage_ms, frames_per_launch, clocks):
+def issue_roofline(stage_ms, frames_per_launch, clocks, variant=1):
     """The bound the shading kernels actually meet: warp instructions issued per second
     against the GPU's issue ceiling (148 SMs x 4 schedulers x 1 warp instruction per clock at
     the median SM clock sampled during the timed region), per stage, from the instruction
@@ -394,7 +397,7 @@ def issue_roofline(stage_ms, frames_per_launch, clocks):
     out = {"bound": "instruction issue", "unit": "warp inst/s", "sm_mhz": mhz, "peak": ceiling,
            "source": "smsp__inst_executed.sum per frame of a 4-frame ncu capture (profiles/) x frames per launch "
                      "/ CUDA-event stage time; peak = 148 SMs x 4 schedulers x median SM clock"}
-    for stage, (per_frame, per_launch) in NCU_WARP_INST_PER_FRAME.items():
+    for stage, (per_frame, per_launch) in NCU_WARP_INST_PER_FRAME[variant].items():
         ms = stage_ms.get(stage)
         if not ms:
             continue
@@ -402,7 +405,7 @@ def issue_roofline(stage_ms, frames_per_launch, clocks):
         achieved = inst / (ms / 1e3)
         out[stage] = {"achieved": round(achieved, 1), "frac": round(achieved / ceiling, 4),
                       "warp_inst_per_launch": int(inst), "stage_ms": round(ms, 4),
-                      "fma_pipe_busy": NCU_FMA_PIPE.get(stage)}
+                      "fma_pipe_busy": NCU_FMA_PIPE[variant].get(stage)}
     return out
 
 

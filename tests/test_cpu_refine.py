@@ -77,3 +77,24 @@ def test_refine_schedule():
 
     c = RefineConfig(every=2500, start=1000, stop=20000)
     assert [s for s in range(1, 25001) if c.due(s)] == list(range(2500, 20001, 2500))
+
+
+def test_principal_scales_chunked_and_non_finite(monkeypatch):
+    """Eigenvalues are taken in chunks (the batched solver refuses millions of matrices in
+    one call): chunked and whole results agree; a Gaussian with a non-finite factor gets NaN
+    scales (and is pruned by refine) without disturbing the others."""
+    from us3d_b200 import refine as R
+
+    g = torch.Generator().manual_seed(3)
+    tril = torch.randn((1000, 6), generator=g)
+    whole = R.principal_scales(tril, 1e-4)
+    monkeypatch.setattr(R, "EIG_CHUNK", 37)
+    chunked = R.principal_scales(tril, 1e-4)
+    assert torch.equal(whole, chunked)
+    assert (whole[:, 0] <= whole[:, 1]).all() and (whole[:, 1] <= whole[:, 2]).all()
+    bad = tril.clone()
+    bad[5, 2] = float("nan")
+    s = R.principal_scales(bad, 1e-4)
+    assert torch.isnan(s[5]).all()
+    keep = torch.arange(1000) != 5
+    assert torch.equal(s[keep], whole[keep])

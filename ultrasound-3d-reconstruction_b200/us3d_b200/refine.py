@@ -14,7 +14,7 @@ device with PyTorch tensor operations (it runs once every few thousand steps):
 
 * scale: the principal standard deviations of Sigma = (L L^T)^-1, L the lower-triangular factor
   with diagonal raw^2 + beta (the renderer's precision parameterisation);
-* prune: largest scale > ``prune_max_scale_mm``, smallest scale < ``prune_min_scale_mm`` or
+* prune: non-finite parameters, largest scale > ``prune_max_scale_mm``, smallest scale < ``prune_min_scale_mm`` or
   opacity sigmoid(raw) < ``min_opacity``;
 * densify (not pruned, mean importance per visited step > ``grad_threshold``): largest scale
   <= ``split_scale_mm`` -> clone (an exact copy is added); larger -> split (replaced by two
@@ -86,11 +86,21 @@ def factor_from_raw(raw_tril: torch.Tensor, beta: float) -> torch.Tensor:
     return L
 
 
+EIG_CHUNK = 1 << 17  # matrices per batched eigenvalue call (the solver's batched form refuses millions)
+
+
 def principal_scales(raw_tril: torch.Tensor, beta: float) -> torch.Tensor:
-    """(G,3) standard deviations along the principal axes, ascending."""
+    """(G,3) standard deviations along the principal axes, ascending (NaN where the
+    parameters are not finite)."""
     L = factor_from_raw(raw_tril.double(), beta)
-    lam = torch.linalg.eigvalsh(L @ L.transpose(-1, -2)).clamp_min(1e-300)
-    return (1.0 / lam.sqrt()).flip(-1).float()
+    M = L @ L.transpose(-1, -2)
+    bad = ~torch.isfinite(M).flatten(1).all(1)
+    M[bad] = torch.eye(3, dtype=M.dtype, device=M.device)
+    lam = torch.cat([torch.linalg.eigvalsh(M[i:i + EIG_CHUNK]) for i in range(0, M.shape[0], EIG_CHUNK)]) \
+        if M.shape[0] else M.new_zeros((0, 3))
+    scales = (1.0 / lam.clamp_min(1e-300).sqrt()).flip(-1).float()
+    scales[bad] = float("nan")
+    return scales
 
 
 def _raw_from_factor(L: torch.Tensor, beta: float) -> torch.Tensor:
@@ -113,6 +123,7 @@ def refine(params, optimizer, stats: RefineStats, cfg: RefineConfig,
     s_min, s_max = scales[:, 0], scales[:, 2]
     opac = torch.sigmoid(raw_o.reshape(-1))
     prune = (s_max > cfg.prune_max_scale_mm) | (s_min < cfg.prune_min_scale_mm) | (opac < cfg.min_opacity)
+    prune |= ~(torch.isfinite(scales).all(1) & torch.isfinite(means).all(1) & torch.isfinite(opac))
     score = stats.score()
     cand = (~prune) & (score > cfg.grad_threshold)
     budget = max(0, int(cfg.max_gaussians) - int((~prune).sum()))
