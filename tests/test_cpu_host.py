@@ -147,3 +147,25 @@ def test_frame_table_gaussian_sets_validation():
     for sets in bad:
         with pytest.raises(ValueError):
             UG.build_frame_table([dataclasses.replace(s, gaussian_set=x) for s, x in zip(base, sets)], cpu)
+
+
+def test_ultragray_profile_schedule_and_ray_stats(monkeypatch):
+    """The UltraGray profiling hook's schedule (every n-th call after the warm-up) and its
+    per-ray statistics (quantiles over rays with hits, linear interpolation)."""
+    import numpy as np
+    import torch
+
+    from ultragray_renderer import autograd as A
+
+    monkeypatch.setenv("ULTRAGRAY_PROFILE_EVERY", "3")
+    monkeypatch.setenv("ULTRAGRAY_PROFILE_WARMUP", "4")
+    assert [s for s in range(1, 16) if A._should_profile(s)] == [6, 9, 12, 15]
+    monkeypatch.setenv("ULTRAGRAY_PROFILE_EVERY", "x")
+    assert not any(A._should_profile(s) for s in range(1, 16))
+    counts = torch.tensor([0, 3, 7, 0, 1, 12, 5], dtype=torch.int32)
+    s = A.ray_stats(counts, 28)
+    act = np.array([3, 7, 1, 12, 5], np.float64)
+    p50, p90, p99 = np.quantile(act, [0.5, 0.9, 0.99])
+    assert s == (f"total_hits=28 active_rays=5/7 hits_mean_all={28 / 7:.1f} hits_mean_active={act.mean():.1f} "
+                 f"hits_p50={p50:.1f} hits_p90={p90:.1f} hits_p99={p99:.1f} hits_max=12")
+    assert "active_rays=0/3" in A.ray_stats(torch.zeros(3, dtype=torch.int32), 0)

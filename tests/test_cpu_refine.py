@@ -79,22 +79,32 @@ def test_refine_schedule():
     assert [s for s in range(1, 25001) if c.due(s)] == list(range(2500, 20001, 2500))
 
 
-def test_principal_scales_chunked_and_non_finite(monkeypatch):
-    """Eigenvalues are taken in chunks (the batched solver refuses millions of matrices in
-    one call): chunked and whole results agree; a Gaussian with a non-finite factor gets NaN
-    scales (and is pruned by refine) without disturbing the others."""
+def test_principal_scales_closed_form_and_non_finite():
+    """Scales in closed form (no batched solver: the library one refuses millions of matrices
+    in one call): against LAPACK on random factors including Gaussians elongated 10^5 : 1,
+    each scale to 1e-9 relative; a Gaussian with a non-finite factor gets NaN scales (and is
+    pruned by refine) without disturbing the others."""
     from us3d_b200 import refine as R
 
     g = torch.Generator().manual_seed(3)
-    tril = torch.randn((1000, 6), generator=g)
-    whole = R.principal_scales(tril, 1e-4)
-    monkeypatch.setattr(R, "EIG_CHUNK", 37)
-    chunked = R.principal_scales(tril, 1e-4)
-    assert torch.equal(whole, chunked)
-    assert (whole[:, 0] <= whole[:, 1]).all() and (whole[:, 1] <= whole[:, 2]).all()
-    bad = tril.clone()
+    tril = torch.randn((5000, 6), generator=g, dtype=torch.float64) * torch.tensor([3.0, 1, 1, 0.2, 1, 0.05])
+    L = R.factor_from_raw(tril, 1e-4)
+    ref = (1.0 / torch.linalg.eigvalsh(L @ L.transpose(-1, -2)).sqrt()).flip(-1)
+    well = torch.nan_to_num(ref[:, 2] / ref[:, 0], nan=1e30) < 1e4  # LAPACK loses the small eigenvalue beyond
+    scales = R.principal_scales(tril.float(), 1e-4)
+    assert torch.allclose(scales.double()[well], ref[well], rtol=1e-6)
+    s64 = R.principal_scales(tril, 1e-4).double()
+    L = R.factor_from_raw(tril, 1e-4)
+    # elongated ones against the exact relation s_min s_mid s_max = 1 / det L and the
+    # singular values of L^-1 (the covariance's square roots) from an SVD
+    sv = torch.linalg.svdvals(torch.linalg.inv(L)).flip(-1)
+    assert torch.allclose(s64[:, 2], sv[:, 2], rtol=1e-6)
+    assert torch.allclose(s64[:, 0], sv[:, 0], rtol=1e-6)
+    assert (scales[:, 0] <= scales[:, 1]).all() and (scales[:, 1] <= scales[:, 2]).all()
+    assert (s64[:, 2] / s64[:, 0]).max() > 1e5
+    bad = tril.float().clone()
     bad[5, 2] = float("nan")
     s = R.principal_scales(bad, 1e-4)
     assert torch.isnan(s[5]).all()
-    keep = torch.arange(1000) != 5
-    assert torch.equal(s[keep], whole[keep])
+    keep = torch.arange(5000) != 5
+    assert torch.equal(s[keep], scales[keep])

@@ -162,3 +162,37 @@ def test_dropin_renderer_autograd_matches_low_level(cuda_device):
         pass
     if REF is not None:
         _check(out, run_reference_ugr(REF, sc, dev))
+
+
+def test_dropin_profiling_lines(cuda_device, monkeypatch, capsys):
+    """ULTRAGRAY_PROFILE_EVERY / _WARMUP: calls after the warm-up whose counter is a multiple
+    of EVERY print a forward line (times and the per-ray hit statistics of the call's own ray
+    lists) and a backward line; the image and gradients are those of an unprofiled call."""
+    from ultragray_renderer import ProbeGeometry, UltragrayRenderConfig, UltragrayRenderer
+    from ultragray_renderer import autograd as A
+
+    scene = make_scene(2500, 48, 64, 52)
+    W, H = 48, 64
+    cfg = UltragrayRenderConfig(image_width=W, image_height=H, width_mm=scene["width_mm"], near_mm=scene["near_mm"],
+                                ops_max_offset_mm=0.0, quadrature_window_radius_mm=scene["wr"])
+    t = {k: torch.as_tensor(v).to(cuda_device) for k, v in scene.items() if isinstance(v, np.ndarray)}
+    geo = ProbeGeometry(t["origin"], t["lat"], t["ele"], t["ax"])
+    monkeypatch.setenv("ULTRAGRAY_PROFILE_EVERY", "2")
+    monkeypatch.setenv("ULTRAGRAY_PROFILE_WARMUP", "1")
+    monkeypatch.setattr(A, "_PROFILE_STEP", 0)
+    outs = []
+    for _ in range(3):  # steps 1 (warm-up), 2 (profiled), 3 (not a multiple of 2)
+        params = [t[k].clone().requires_grad_(True) for k in ("means", "scales", "quats", "attenuations", "sh")]
+        img = UltragrayRenderer(cfg)(*params, t["pixels"], t["ray_o"], t["ray_d"], geo)
+        (img * t["grad_image"]).sum().backward()
+        outs.append([img.detach()] + [p.grad for p in params])
+    lines = [ln for ln in capsys.readouterr().out.splitlines() if ln.startswith("[ULTRAGRAY_PROFILE]")]
+    assert len(lines) == 2 and "step=2 phase=forward" in lines[0] and "step=2 phase=backward" in lines[1], lines
+    sc = dict(scene, pert=np.zeros(W, np.float32), col_off=float(cfg.lateral_col_offset))
+    out = run_b200_ugr(sc, cuda_device)
+    counts = torch.as_tensor(out["counts"])
+    assert f"total_hits={int(out['total'])} " in lines[0]
+    assert f"active_rays={int((counts > 0).sum())}/{W} " in lines[0]
+    assert f"hits_max={int(counts.max())}" in lines[0]
+    for a, b in zip(outs[1], outs[0]):
+        assert torch.equal(a, b)

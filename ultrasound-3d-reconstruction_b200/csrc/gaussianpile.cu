@@ -531,10 +531,15 @@ backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restric
         const float inv00 = f1.x, inv01 = f1.y, inv11 = f1.z, bno_const = f1.w;
         const float s2_00 = f2.x, s2_01 = f2.y, s2_11 = f2.z, inv_det_norm = f2.w;
         const float mu_ele = f3.x, inv_de = f3.y, dse_dax = f3.z, sigma_ele = f3.w;
-        // Every term of the per-instance partial is a fixed combination of six sums over the
-        // contributing pixels of up * bno (bno = the weight without the opacity) times 1, dlat,
-        // dax, dlat^2, dlat dax, dax^2: the lanes accumulate those and the terms are formed once.
-        float m0 = 0.f, mx = 0.f, my = 0.f, mxx = 0.f, mxy = 0.f, myy = 0.f;
+        // Every term of the per-instance partial is a fixed combination of nine sums over the
+        // contributing pixels of ub = up * bno (bno = the weight without the opacity) times 1,
+        // q_lat, q_ax, q_lat^2, q_lat q_ax, q_ax^2 (q = inv2 d) and dlat^2, dlat dax, dax^2: the
+        // lanes accumulate those and the terms are formed once. The q-weighted sums are taken
+        // per pixel, not expanded from moments of d: for an elongated footprint q nearly
+        // cancels along the long axis, and the expansion inv00^2 S(dlat^2) + 2 inv00 inv01
+        // S(dlat dax) + ... loses in fp32 the digits that the chain through Se and Lc (with
+        // entries in the hundreds for such footprints) then amplifies.
+        float m0 = 0.f, sl = 0.f, sa = 0.f, sll = 0.f, sla = 0.f, saa = 0.f, mxx = 0.f, mxy = 0.f, myy = 0.f;
         float o = 0.f, c = 0.f;
         if (r_lat >= 0.f) {
             const int cx0 = max(x0, (int)ceilf((mu2_lat - r_lat) / lat_delta + col_off));
@@ -569,10 +574,14 @@ backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restric
                 const float weight = o * bno;
                 if (!isfinite(weight) || weight < weight_min) continue;
                 const float ub = grad_image[y * W + x] * bno;
+                const float ul = ub * qlat, ua = ub * qax;
                 const float ux = ub * dlat, uy = ub * dax;
                 m0 += ub;
-                mx += ux;
-                my += uy;
+                sl += ul;
+                sa += ua;
+                sll += ul * qlat;
+                sla += ul * qax;
+                saa += ua * qax;
                 mxx += ux * dlat;
                 mxy += ux * dax;
                 myy += uy * dax;
@@ -582,8 +591,11 @@ backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restric
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             m0 += __shfl_xor_sync(0xffffffffu, m0, off);
-            mx += __shfl_xor_sync(0xffffffffu, mx, off);
-            my += __shfl_xor_sync(0xffffffffu, my, off);
+            sl += __shfl_xor_sync(0xffffffffu, sl, off);
+            sa += __shfl_xor_sync(0xffffffffu, sa, off);
+            sll += __shfl_xor_sync(0xffffffffu, sll, off);
+            sla += __shfl_xor_sync(0xffffffffu, sla, off);
+            saa += __shfl_xor_sync(0xffffffffu, saa, off);
             mxx += __shfl_xor_sync(0xffffffffu, mxx, off);
             mxy += __shfl_xor_sync(0xffffffffu, mxy, off);
             myy += __shfl_xor_sync(0xffffffffu, myy, off);
@@ -593,10 +605,7 @@ backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restric
         float acc[P_COUNT];
         {
             const float co = c * o;  // cm = co * up * bno
-            const float ql = inv00 * mx + inv01 * my, qa = inv01 * mx + inv11 * my;  // sum ub q
-            const float qll = inv00 * inv00 * mxx + 2.f * inv00 * inv01 * mxy + inv01 * inv01 * myy;
-            const float qla = inv00 * inv01 * mxx + (inv00 * inv11 + inv01 * inv01) * mxy + inv01 * inv11 * myy;
-            const float qaa = inv01 * inv01 * mxx + 2.f * inv01 * inv11 * mxy + inv11 * inv11 * myy;
+            const float ql = sl, qa = sa, qll = sll, qla = sla, qaa = saa;
             const float ele2 = mu_ele * mu_ele * inv_de * inv_de;
             acc[P_INTENSITY] = o * m0;
             acc[P_OPACITY] = c * m0;

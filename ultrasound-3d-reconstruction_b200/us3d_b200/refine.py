@@ -27,6 +27,7 @@ device with PyTorch tensor operations (it runs once every few thousand steps):
 
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass
 from typing import Optional
 
@@ -86,21 +87,44 @@ def factor_from_raw(raw_tril: torch.Tensor, beta: float) -> torch.Tensor:
     return L
 
 
-EIG_CHUNK = 1 << 17  # matrices per batched eigenvalue call (the solver's batched form refuses millions)
+def _sym3_largest(M: torch.Tensor) -> torch.Tensor:
+    """Largest eigenvalue of symmetric 3x3 matrices (..., 3, 3), closed form: the
+    trigonometric solution of the characteristic cubic (q = tr/3, p = sqrt(|M - qI|_F^2 / 6),
+    r = det((M - qI) / p) / 2, largest root q + 2p cos(acos(r)/3)); elementwise tensor
+    arithmetic, any number of matrices in one pass. The largest root carries no cancellation,
+    so its relative error is a few ulps."""
+    a, b, c = M[..., 0, 0], M[..., 1, 1], M[..., 2, 2]
+    d, e, f = M[..., 0, 1], M[..., 1, 2], M[..., 0, 2]
+    q = (a + b + c) / 3.0
+    aq, bq, cq = a - q, b - q, c - q
+    p = torch.sqrt((aq * aq + bq * bq + cq * cq + 2.0 * (d * d + e * e + f * f)) / 6.0)
+    safe = torch.where(p > 0, p, torch.ones_like(p))
+    ba, bb, bc, bd, be, bf = aq / safe, bq / safe, cq / safe, d / safe, e / safe, f / safe
+    det = ba * (bb * bc - be * be) - bd * (bd * bc - be * bf) + bf * (bd * be - bb * bf)
+    return q + 2.0 * p * torch.cos(torch.acos((det * 0.5).clamp(-1.0, 1.0)) / 3.0)
 
 
 def principal_scales(raw_tril: torch.Tensor, beta: float) -> torch.Tensor:
     """(G,3) standard deviations along the principal axes, ascending (NaN where the
-    parameters are not finite)."""
+    parameters are not finite). With the precision L L^T (L lower triangular, diagonal
+    raw^2 + beta): s_min = 1 / sqrt(largest eigenvalue of L L^T), s_max = sqrt(largest
+    eigenvalue of the covariance L^-T L^-1) and s_mid from s_min s_mid s_max = 1 / det L. Only
+    largest eigenvalues are taken, in closed form (no batched solver: the library one refuses
+    millions of matrices in one call), so each scale keeps its relative accuracy however
+    elongated the Gaussian is."""
     L = factor_from_raw(raw_tril.double(), beta)
-    M = L @ L.transpose(-1, -2)
-    bad = ~torch.isfinite(M).flatten(1).all(1)
-    M[bad] = torch.eye(3, dtype=M.dtype, device=M.device)
-    lam = torch.cat([torch.linalg.eigvalsh(M[i:i + EIG_CHUNK]) for i in range(0, M.shape[0], EIG_CHUNK)]) \
-        if M.shape[0] else M.new_zeros((0, 3))
-    scales = (1.0 / lam.clamp_min(1e-300).sqrt()).flip(-1).float()
-    scales[bad] = float("nan")
-    return scales
+    l00, l10, l11, l20, l21, l22 = L[:, 0, 0], L[:, 1, 0], L[:, 1, 1], L[:, 2, 0], L[:, 2, 1], L[:, 2, 2]
+    Li = torch.zeros_like(L)  # L^-1, lower triangular
+    Li[:, 0, 0] = 1.0 / l00
+    Li[:, 1, 1] = 1.0 / l11
+    Li[:, 2, 2] = 1.0 / l22
+    Li[:, 1, 0] = -l10 / (l00 * l11)
+    Li[:, 2, 1] = -l21 / (l11 * l22)
+    Li[:, 2, 0] = (l10 * l21 - l11 * l20) / (l00 * l11 * l22)
+    s_min = 1.0 / torch.sqrt(_sym3_largest(L @ L.transpose(-1, -2)))
+    s_max = torch.sqrt(_sym3_largest(Li.transpose(-1, -2) @ Li))
+    s_mid = 1.0 / ((l00 * l11 * l22).abs() * s_min * s_max)
+    return torch.stack([s_min, s_mid, s_max], 1).float()
 
 
 def _raw_from_factor(L: torch.Tensor, beta: float) -> torch.Tensor:
