@@ -367,14 +367,16 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
 // Forward
 // ------------------------------------------------------------------------------------
 
-// One block per tile with PARTS threads per pixel (tile x tile pixels rounded up to whole
-// warps, times PARTS); candidates of the tile list are staged in shared memory. The sum over a
-// pixel's candidates is split by Gaussian index into four classes (g mod 4), each summed in
-// list order, and the class sums are added as ((c0 + c1) + c2) + c3; thread part p of a pixel
-// owns the classes congruent to p mod PARTS. The grouping depends on neither PARTS nor the
-// tile size, so the image does not either (the reference sums the whole list in order,
-// src/shader/forward.cu:88-210: the results agree up to rounding).
-template <int PARTS>
+// One block per tile, or per 1/SPLIT of a tile, with PARTS threads per pixel (the block's
+// pixels rounded up to whole warps, times PARTS); candidates of the tile list are staged in
+// shared memory. The sum over a pixel's candidates is split by Gaussian index into four classes
+// (g mod 4), each summed in list order, and the class sums are added as ((c0 + c1) + c2) + c3;
+// thread part p of a pixel owns the classes congruent to p mod PARTS. The grouping depends on
+// neither PARTS, SPLIT nor the tile size, so the image does not either (the reference sums the
+// whole list in order, src/shader/forward.cu:88-210: the results agree up to rounding). SPLIT
+// > 1 serves small frames: a 256x256 slice has 256 tiles, under two 1024-thread blocks per SM,
+// while quarter tiles give 1024 blocks of 256 threads that the SMs can balance.
+template <int PARTS, int SPLIT>
 __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float* __restrict__ grid,
                                const float* __restrict__ params, const int* __restrict__ tile_start,
                                const int* __restrict__ sorted_gid, const long long* __restrict__ header,
@@ -385,10 +387,12 @@ __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float*
     __shared__ unsigned char s_cls[FWD_BATCH];
     __shared__ float s_class_sum[4 * 1024 / PARTS];
     if (header[H_FLAGS] != 0) return;
-    const int t = blockIdx.x;
+    const int t = blockIdx.x / SPLIT, sub = blockIdx.x % SPLIT;
     const int tx = t % tiles_x, ty = t / tiles_x;
-    const int npix = (tile * tile + 31) / 32 * 32;  // pixel slots per part (whole warps)
-    const int slot = threadIdx.x % npix, part = threadIdx.x / npix;
+    // pixel slots per part (whole warps); with SPLIT > 1 the host guarantees tile^2 / SPLIT is
+    // a multiple of 32, so the sub-blocks partition the tile
+    const int npix = SPLIT == 1 ? (tile * tile + 31) / 32 * 32 : tile * tile / SPLIT;
+    const int slot = threadIdx.x % npix + sub * npix, part = threadIdx.x / npix;
     const int lx = slot % tile, ly = slot / tile;
     const int x = tx * tile + lx, y = ty * tile + ly;
     // the extra slots of the last warp own no pixel
@@ -470,13 +474,14 @@ __global__ void forward_kernel(int H, int W, int tile, int tiles_x, const float*
         }
     }
     // class c's sum sits in part c % PARTS, slot c / PARTS of its accumulators
+    const int ls = slot - sub * npix;  // the slot within this block
 #pragma unroll
-    for (int c = 0; c < PER; ++c) s_class_sum[(c * PARTS + part) * npix + slot] = acc[c];
+    for (int c = 0; c < PER; ++c) s_class_sum[(c * PARTS + part) * npix + ls] = acc[c];
     __syncthreads();
     if (part != 0 || !valid) return;
-    float total = s_class_sum[slot];
+    float total = s_class_sum[ls];
 #pragma unroll
-    for (int c = 1; c < 4; ++c) total += s_class_sum[c * npix + slot];
+    for (int c = 1; c < 4; ++c) total += s_class_sum[c * npix + ls];
     image[y * W + x] = total;
 }
 
@@ -1056,18 +1061,21 @@ extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t 
                                         w.tile_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(T, n_gauss, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_gp_sort_attr, stream));
-    // up to four threads per pixel (a whole-warp pixel block of at most 1024 threads)
+    // up to four threads per pixel (a whole-warp pixel block of at most 1024 threads); frames
+    // with fewer than four tiles per SM split each tile over four blocks when it divides into
+    // whole warps
     const int npix = (tile_size * tile_size + 31) / 32 * 32;
-    auto launch = [&](auto kernel, int parts) {
-        kernel<<<(unsigned)T, npix * parts, 0, stream>>>(H, W, tile_size, tx, grid_pack, focus_params, w.tile_start,
-                                                        w.sorted_gid, w.header, w.cand, out_image);
+    auto launch = [&](auto kernel, int parts, int split) {
+        kernel<<<(unsigned)(T * split), npix / split * parts, 0, stream>>>(
+            H, W, tile_size, tx, grid_pack, focus_params, w.tile_start, w.sorted_gid, w.header, w.cand, out_image);
     };
+    const bool split4 = T < 4 * 148 && (tile_size * tile_size) % 128 == 0;
     if (npix <= 256)
-        launch(forward_kernel<4>, 4);
+        split4 ? launch(forward_kernel<4, 4>, 4, 4) : launch(forward_kernel<4, 1>, 4, 1);
     else if (npix <= 512)
-        launch(forward_kernel<2>, 2);
+        split4 ? launch(forward_kernel<2, 4>, 2, 4) : launch(forward_kernel<2, 1>, 2, 1);
     else
-        launch(forward_kernel<1>, 1);
+        split4 ? launch(forward_kernel<1, 4>, 1, 4) : launch(forward_kernel<1, 1>, 1, 1);
     US3D_CHECK_LAUNCH("gp forward");
     prof_end(prof, stream);
     count_launches(1 + (n_gauss > 0) * 3 + 6 + 1 + TILE_SORT_LAUNCHES + 1);
