@@ -110,18 +110,21 @@ def test_config2_gaussianpile(config2, cuda_device):
         fx = MG.run("config2", sc, _pose_probe_to_world(sweep[f]),
                     dict(H=H, W=W, lat=SPACING, ax=SPACING, near=0.0, centre=True, sigma_z=1.0, pose_grad=True))
         out = run_b200_gp(fx, cuda_device)
-        T._check(out, dict(fx, pose_grad=0))
         # The pose gradient sums 200k Gaussians' contributions with lever arms of tens of mm that
         # largely cancel; the reference adds them with float atomics, this library in double in a
-        # fixed order. Both are compared with the FP64 oracle: both stand about 1e-4 from it (each
-        # Gaussian's contribution is evaluated in fast-math fp32 by both), and this library must
-        # be within 2e-4 of it or no farther than twice the reference's distance.
+        # fixed order. Gradients that differ from the reference by more than 1e-4 (the pose, and
+        # on some frames the means of a few very elongated footprints) are compared with the
+        # FP64 oracle instead: this library must stand within 1e-4 of it or no farther than twice
+        # the reference's own distance.
         m = fx["meta"].tolist()
         st = GO.render(fx["means"], fx["scales"], fx["quats"], fx["opacities"], fx["intensities"], fx["pose"],
                        fx["grid"], fx["params"], H, W, m[2], m[3], m[4], int(m[5]), m[8], precision="f64")
-        d64 = GO.backward(st, fx["grad_image"], pose_grad=True)["d_pose"]
-        ours, ref = rel_l2(out["d_pose"], d64), rel_l2(fx["ref_d_pose"], d64)
-        assert ours <= max(2e-4, 2.0 * ref), (f, ours, ref)
+        g64 = GO.backward(st, fx["grad_image"], pose_grad=True)
+        exact = {k: g64[k] for k in ("d_means", "d_opacity", "d_intensity", "d_pose")}
+        report = {k: (rel_l2(out[k], fx["ref_" + k]), rel_l2(out[k], exact[k]), rel_l2(fx["ref_" + k], exact[k]))
+                  for k in exact}
+        print(f"config-2 GaussianPile frame {f}: (ours vs ref, ours vs fp64, ref vs fp64) {report}")
+        T._check(out, fx, exact)
 
 
 def test_config2_slice_adapted(config2, cuda_device):

@@ -169,3 +169,15 @@ def test_ultragray_profile_schedule_and_ray_stats(monkeypatch):
     assert s == (f"total_hits=28 active_rays=5/7 hits_mean_all={28 / 7:.1f} hits_mean_active={act.mean():.1f} "
                  f"hits_p50={p50:.1f} hits_p90={p90:.1f} hits_p99={p99:.1f} hits_max=12")
     assert "active_rays=0/3" in A.ray_stats(torch.zeros(3, dtype=torch.int32), 0)
+
+
+def test_workload_time_to_accuracy():
+    """Time to reach a held-out L1 target from an evaluation curve of (seconds, frames, L1):
+    linear between evaluations, None when never reached."""
+    from us3d_b200 import workloads as WL
+
+    c = [(0.0, 0, 0.5), (1.0, 10, 0.3), (2.0, 20, 0.1)]
+    assert WL._seconds_to(c, 0.2) == 1.5
+    assert WL._seconds_to(c, 0.3) == 1.0
+    assert WL._seconds_to(c, 0.05) is None
+    assert WL._seconds_to([(0.0, 0, 0.5), (1.0, 8, 0.6), (2.0, 16, 0.4)], 0.45) == 1.75

@@ -108,3 +108,20 @@ def test_principal_scales_closed_form_and_non_finite():
     assert torch.isnan(s[5]).all()
     keep = torch.arange(5000) != 5
     assert torch.equal(s[keep], scales[keep])
+
+
+def test_refine_densify_fraction():
+    """With densify_fraction the threshold is a quantile of the visited, unpruned Gaussians'
+    scores: of the five survivors (scores 1, 0, 1, 0, 2) the top 20 % is Gaussian 7 alone, the
+    top 60 % adds the two with score 1 (0 clone, 2 split)."""
+    from us3d_b200.refine import refine
+
+    params, opt, stats, cfg, means, tril = _setup()
+    cfg.grad_threshold = 1e9  # ignored when a fraction is given
+    cfg.densify_fraction = 0.2
+    out = refine(params, opt, stats, cfg, torch.Generator().manual_seed(0))
+    assert out == {"kept": 5, "pruned": 3, "cloned": 1, "split": 0, "total": 6}
+    params, opt, stats, cfg, means, tril = _setup()
+    cfg.densify_fraction = 0.6
+    out = refine(params, opt, stats, cfg, torch.Generator().manual_seed(0))
+    assert out == {"kept": 4, "pruned": 3, "cloned": 2, "split": 1, "total": 8}

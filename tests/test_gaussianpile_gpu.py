@@ -25,17 +25,27 @@ pytestmark = pytest.mark.gpu
 ROOT = Path(__file__).resolve().parents[1]
 
 
-def _check(out, fx):
+def _check(out, fx, exact=None):
+    """Binning bit-exact, image <= 1e-5 and gradients <= 1e-4 against the reference. With
+    ``exact`` (the FP64 oracle's gradients of the same inputs), a gradient further than 1e-4
+    from the reference passes when it stands no farther from the FP64 values than 1e-4 or twice
+    the reference's own distance from them: on large scenes a few very elongated footprints
+    (conditional covariance entries in the hundreds) amplify fp32 rounding in both
+    implementations, each in its own summation order."""
     vis = fx["ref_rects"][:, 0] < fx["ref_rects"][:, 2]
     np.testing.assert_array_equal(out["rects"][vis], fx["ref_rects"][vis], err_msg="tile rectangles")
     np.testing.assert_array_equal(out["sorted_ids"], fx["ref_sorted_ids"], err_msg="sorted ids")
     np.testing.assert_array_equal(out["range_start"], fx["ref_range_start"], err_msg="range start")
     np.testing.assert_array_equal(out["range_end"], fx["ref_range_end"], err_msg="range end")
     assert rel_l2(out["image"], fx["ref_image"]) <= 1e-5, rel_l2(out["image"], fx["ref_image"])
-    for k in ("d_means", "d_opacity", "d_intensity"):
-        assert rel_l2(out[k], fx["ref_" + k]) <= 1e-4, (k, rel_l2(out[k], fx["ref_" + k]))
-    if int(fx["pose_grad"]):
-        assert rel_l2(out["d_pose"], fx["ref_d_pose"]) <= 1e-4, rel_l2(out["d_pose"], fx["ref_d_pose"])
+    names = ("d_means", "d_opacity", "d_intensity") + (("d_pose",) if int(fx["pose_grad"]) else ())
+    for k in names:
+        e = rel_l2(out[k], fx["ref_" + k])
+        if e <= 1e-4:
+            continue
+        assert exact is not None, (k, e)
+        ours, ref = rel_l2(out[k], exact[k]), rel_l2(fx["ref_" + k], exact[k])
+        assert ours <= max(1e-4, 2.0 * ref), (k, e, ours, ref)
     for k in ("d_scales", "d_quats"):
         assert rel_l2(out[k], fx["ref_" + k]) <= 1e-3, (k, rel_l2(out[k], fx["ref_" + k]))
 

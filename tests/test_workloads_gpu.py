@@ -26,9 +26,15 @@ def test_training_workload_small(cuda_device):
     from us3d_b200 import workloads as WL
 
     out = WL.run_training(n_init=20_000, n_gt=40_000, n_frames=48, size=128, spacing_mm=0.5, batch=8, steps=60,
-                          refine_every=20, plain_frames=64, max_gaussians=40_000, device=cuda_device)
-    b = out["batched"]
-    assert b["frames"] == 480 and b["frames_per_s"] > 0
-    assert len(b["refinements"]) == 3
-    assert b["held_out_l1"] < out["held_out_l1_at_start"], out
+                          refine_every=20, plain_frames=64, max_gaussians=40_000, evals=4, device=cuda_device)
+    for name in ("batched", "batched_lr_sqrt_batch"):
+        b = out[name]
+        assert b["frames"] == 480 and b["frames_per_s"] > 0
+        assert len(b["refinements"]) == 3
+        assert sum(r["cloned"] + r["split"] for r in b["refinements"]) > 0  # the top 1 % is densified
+        assert len(b["curve"]) == 5 and b["curve"][-1][1] == 480
+        assert b["held_out_l1"] < out["held_out_l1_at_start"], out
     assert 0.0 < out["plain"]["held_out_l1"] < 1.0
+    assert out["matched_accuracy"]["target_held_out_l1"] == out["plain"]["held_out_l1"]
+    assert WL._seconds_to([(0.0, 0, 0.5), (1.0, 10, 0.3), (2.0, 20, 0.1)], 0.2) == 1.5
+    assert WL._seconds_to([(0.0, 0, 0.5), (1.0, 10, 0.3)], 0.2) is None

@@ -16,7 +16,8 @@ device with PyTorch tensor operations (it runs once every few thousand steps):
   with diagonal raw^2 + beta (the renderer's precision parameterisation);
 * prune: non-finite parameters, largest scale > ``prune_max_scale_mm``, smallest scale < ``prune_min_scale_mm`` or
   opacity sigmoid(raw) < ``min_opacity``;
-* densify (not pruned, mean importance per visited step > ``grad_threshold``): largest scale
+* densify (not pruned, mean importance per visited step > ``grad_threshold``, or among the top
+  ``densify_fraction`` of the visited Gaussians when that is set): largest scale
   <= ``split_scale_mm`` -> clone (an exact copy is added); larger -> split (replaced by two
   children with means drawn from N(mean, Sigma) and Sigma shrunk by ``split_factor``^2, i.e.
   L scaled by ``split_factor``, other attributes copied);
@@ -50,6 +51,11 @@ class RefineConfig:
     min_opacity: float = 0.005
     max_gaussians: int = 500000
     diag_beta: float = 1.0e-4
+    # When set, the importance threshold of each refinement is the (1 - fraction) quantile of
+    # the scores of the visited, unpruned Gaussians (the top ``densify_fraction`` are densified)
+    # instead of ``grad_threshold``: |dL/dmean| scales with how the loss is normalised (pixels
+    # and frames per step), a quantile does not.
+    densify_fraction: Optional[float] = None
 
     def due(self, step: int) -> bool:
         """Whether a refinement follows training step ``step`` (counted from 1)."""
@@ -149,7 +155,13 @@ def refine(params, optimizer, stats: RefineStats, cfg: RefineConfig,
     prune = (s_max > cfg.prune_max_scale_mm) | (s_min < cfg.prune_min_scale_mm) | (opac < cfg.min_opacity)
     prune |= ~(torch.isfinite(scales).all(1) & torch.isfinite(means).all(1) & torch.isfinite(opac))
     score = stats.score()
-    cand = (~prune) & (score > cfg.grad_threshold)
+    threshold = cfg.grad_threshold
+    if cfg.densify_fraction is not None:
+        sv = torch.sort(score[(~prune) & (stats.visits > 0)]).values
+        n, m = sv.numel(), int(math.ceil(sv.numel() * float(cfg.densify_fraction)))
+        # the m highest scores lie strictly above sv[n - m - 1] (ties with it are left out)
+        threshold = float("inf") if m <= 0 else (float("-inf") if m >= n else float(sv[n - m - 1]))
+    cand = (~prune) & (score > threshold)
     budget = max(0, int(cfg.max_gaussians) - int((~prune).sum()))
     idx = cand.nonzero().flatten()
     if idx.numel() > budget:  # each candidate adds one Gaussian (a clone, or two children for one)

@@ -245,18 +245,60 @@ def speckle_targets(gt: scenes.GaussianScene, frames, device, seed: int = 0, sig
     return torch.cat(out)
 
 
+def _train_curve(make_trainer, params, steps: int, batch: int, evals: int, l1_on_held) -> dict:
+    """Trains ``steps`` steps, pausing ``evals`` times to take the held-out L1 (outside the
+    timed region); returns frames/s over the training time alone, the curve of (seconds,
+    frames, held-out L1) and the trainer's refinement log."""
+    trainer = make_trainer(params)
+    dev = params.means.device
+    curve = [(0.0, 0, round(l1_on_held(params), 6))]
+    every = max(1, steps // max(1, evals))
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms, done = 0.0, 0
+    while done < steps:
+        n = min(every, steps - done)
+        torch.cuda.synchronize(dev)
+        st.record()
+        for _ in range(n):
+            trainer.step(0)
+        en.record()
+        en.synchronize()
+        ms += st.elapsed_time(en)
+        done += n
+        curve.append((round(ms / 1e3, 3), done * batch, round(l1_on_held(params), 6)))
+    trainer.check()
+    out = dict(steps=steps, frames=steps * batch, seconds=round(ms / 1e3, 3),
+               frames_per_s=round(steps * batch / (ms / 1e3), 1), held_out_l1=curve[-1][2], curve=curve,
+               gaussians_final=int(params.means.shape[0]), refinements=list(getattr(trainer, "refine_log", [])))
+    del trainer
+    torch.cuda.empty_cache()
+    return out
+
+
+def _seconds_to(curve, target: float) -> Optional[float]:
+    """First time (linear between evaluations) at which the held-out L1 reaches target."""
+    for (t0, _, l0), (t1, _, l1) in zip(curve, curve[1:]):
+        if l1 <= target:
+            return round(t0 + (t1 - t0) * ((l0 - target) / (l0 - l1) if l0 > l1 else 1.0), 3)
+    return None
+
+
 def run_training(n_init: int = 2_000_000, n_gt: int = 4_000_000, n_frames: int = 1500, size: int = 512,
                  spacing_mm: float = 0.15, batch: int = 16, steps: int = 5000, refine_every: int = 500,
                  plain_frames: int = 16000, seed: int = 0, max_gaussians: int = 3_000_000,
-                 device: Optional[torch.device] = None) -> dict:
+                 densify_fraction: float = 0.01, evals: int = 20, device: Optional[torch.device] = None) -> dict:
     """The end-to-end training workload: initial Gaussians from the layered point cloud
     (n_init points), targets from an n_gt-Gaussian ground truth of the same structures with
     Rayleigh speckle, n_frames frames of size^2 px at spacing_mm from three crossing sweeps,
     batches of ``batch`` frames per step drawn on the device, forward + loss + backward +
-    Adam per step (graph-replayed), densify / prune every ``refine_every`` steps; then the
-    same initial state trained in the one-frame-per-step form (the reference's pattern) for
+    Adam per step (graph-replayed), densify (the top ``densify_fraction`` by importance) and
+    prune every ``refine_every`` steps. Three runs from the same initial state: the batched
+    form at the reference's learning rate (1e-3), the batched form at sqrt(batch) times it
+    (Adam's step does not grow with the batch, so a 16-frame step otherwise moves as far as a
+    1-frame step), and the one-frame-per-step form (the reference's pattern) for
     ``plain_frames`` frames. Reports frames/s, the step's HBM rate from its algorithmic bytes,
-    and the L1 both parameter sets reach on 64 held frames."""
+    held-out L1 curves on 64 frames, and the training time each batched run needs to reach the
+    plain form's final held-out L1 (matched accuracy)."""
     from .frames import DeviceFrameSource
     from .refine import RefineConfig
     from .train import TrainConfig, UltraGaussParameters, UltraGaussTrainer
@@ -292,54 +334,34 @@ def run_training(n_init: int = 2_000_000, n_gt: int = 4_000_000, n_frames: int =
         img, _, _, _ = UG.forward(b, pix, BG_A, BG_I, want_counts=False)
         return float((img - tgt).abs().mean())
 
-    cfg = TrainConfig()
-    rcfg = RefineConfig(every=refine_every, start=refine_every, stop=steps, max_gaussians=max_gaussians)
-    params = fresh()
-    l1_start = l1_on_held(params)
-    trainer = UltraGaussTrainer.from_source(params, source, batch, cfg, refine=rcfg, seed=seed)
-    l1 = []
-    torch.cuda.synchronize(dev)
-    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    st.record()
-    for i in range(steps):
-        trainer.step(0)
-        if (i + 1) % max(1, steps // 20) == 0:
-            l1.append((i + 1, float(trainer.losses(0)[:, 5].mean())))  # mean |x - y| of the batch
-    en.record()
-    en.synchronize()
-    trainer.check()
-    ms = st.elapsed_time(en)
-    G = int(params.means.shape[0])
-    batched = dict(steps=steps, frames=steps * batch, seconds=round(ms / 1e3, 3),
-                   frames_per_s=round(steps * batch / (ms / 1e3), 1), batch_l1_curve=l1,
-                   gaussians_final=G, refinements=trainer.refine_log)
+    rcfg = RefineConfig(every=refine_every, start=refine_every, stop=steps, max_gaussians=max_gaussians,
+                        densify_fraction=densify_fraction)
+    runs = {}
+    for name, lr in (("batched", 1.0e-3), ("batched_lr_sqrt_batch", 1.0e-3 * math.sqrt(batch))):
+        runs[name] = _train_curve(
+            lambda p, lr=lr: UltraGaussTrainer.from_source(p, source, batch, TrainConfig(lr=lr), refine=rcfg,
+                                                            seed=seed), fresh(), steps, batch, evals, l1_on_held)
+        runs[name]["lr"] = lr
     # algorithmic HBM bytes of a step at the final size: parameters read by binning, forward and
     # backward, gradients written, Adam's 28 bytes per parameter element, pixels and targets
     P = size * size
-    bytes_step = G * 44 * 3 + G * 44 + G * 11 * 28 + batch * P * (12 + 1 + 12 + 12)
-    batched["hbm_gbs_algorithmic"] = round(bytes_step * steps / (ms / 1e3) / 1e9, 1)
-    batched["held_out_l1"] = l1_on_held(params)
-    del trainer
-
-    params_p = fresh()
-    plain = UltraGaussTrainer.from_source(params_p, source, 1, cfg, seed=seed + 1)
-    n_plain = int(plain_frames)
-    torch.cuda.synchronize(dev)
-    st.record()
-    for _ in range(n_plain):
-        plain.step(0)
-    en.record()
-    en.synchronize()
-    plain.check()
-    ms_p = st.elapsed_time(en)
-    plain_res = dict(steps=n_plain, frames=n_plain, seconds=round(ms_p / 1e3, 3),
-                     frames_per_s=round(n_plain / (ms_p / 1e3), 1), held_out_l1=l1_on_held(params_p))
+    for r in runs.values():
+        G = r["gaussians_final"]
+        bytes_step = G * 44 * 3 + G * 44 + G * 11 * 28 + batch * P * (12 + 1 + 12 + 12)
+        r["hbm_gbs_algorithmic"] = round(bytes_step * r["steps"] / r["seconds"] / 1e9, 1)
+    plain = _train_curve(lambda p: UltraGaussTrainer.from_source(p, source, 1, TrainConfig(), seed=seed + 1), fresh(),
+                         int(plain_frames), 1, evals, l1_on_held)
+    plain["lr"] = 1.0e-3
+    target = plain["held_out_l1"]
+    matched = {name: dict(seconds_to_plain_final_l1=_seconds_to(r["curve"], target),
+                          plain_seconds=plain["seconds"]) for name, r in runs.items()}
     return dict(workload=f"UltraGauss training: {n_init} initial Gaussians (layered point cloud + inclusions), "
                          f"{n_frames} frames {size}^2 px @ {spacing_mm} mm from three crossing sweeps, targets from "
                          f"{n_gt} ground-truth Gaussians with Rayleigh speckle, {batch} frames/step, "
-                         f"densify/prune every {refine_every} steps",
-                preparation_s=round(prep_s, 2), held_out_l1_at_start=l1_start, batched=batched, plain=plain_res,
-                batched_over_plain_frames_per_s=round(batched["frames_per_s"] / plain_res["frames_per_s"], 3))
+                         f"densify (top {densify_fraction:.0%}) / prune every {refine_every} steps",
+                preparation_s=round(prep_s, 2), held_out_l1_at_start=runs["batched"]["curve"][0][2], **runs,
+                plain=plain, matched_accuracy=dict(target_held_out_l1=target, **matched),
+                batched_over_plain_frames_per_s=round(runs["batched"]["frames_per_s"] / plain["frames_per_s"], 3))
 
 
 def main():
