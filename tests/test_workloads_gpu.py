@@ -25,14 +25,14 @@ def test_sweeps_workload_small(cuda_device):
 def test_training_workload_small(cuda_device):
     from us3d_b200 import workloads as WL
 
-    out = WL.run_training(n_init=20_000, n_gt=40_000, n_frames=48, size=128, spacing_mm=0.5, batch=8, steps=60,
+    out = WL.run_training(n_init=20_000, n_gt=40_000, n_frames=48, size=128, spacing_mm=0.5, batch=8, steps=100,
                           refine_every=20, plain_frames=64, max_gaussians=40_000, evals=4, device=cuda_device)
     for name in ("batched", "batched_lr_sqrt_batch"):
         b = out[name]
-        assert b["frames"] == 480 and b["frames_per_s"] > 0
-        assert len(b["refinements"]) == 3
+        assert b["frames"] == 800 and b["frames_per_s"] > 0
+        assert [r["step"] for r in b["refinements"]] == [20, 40, 60]  # the first 60 % of the steps
         assert sum(r["cloned"] + r["split"] for r in b["refinements"]) > 0  # the top 1 % is densified
-        assert len(b["curve"]) == 5 and b["curve"][-1][1] == 480
+        assert len(b["curve"]) == 5 and b["curve"][-1][1] == 800
         assert b["held_out_l1"] < out["held_out_l1_at_start"], out
     assert 0.0 < out["plain"]["held_out_l1"] < 1.0
     assert out["matched_accuracy"]["target_held_out_l1"] == out["plain"]["held_out_l1"]

@@ -292,7 +292,7 @@ def run_training(n_init: int = 2_000_000, n_gt: int = 4_000_000, n_frames: int =
     Rayleigh speckle, n_frames frames of size^2 px at spacing_mm from three crossing sweeps,
     batches of ``batch`` frames per step drawn on the device, forward + loss + backward +
     Adam per step (graph-replayed), densify (the top ``densify_fraction`` by importance) and
-    prune every ``refine_every`` steps. Three runs from the same initial state: the batched
+    prune every ``refine_every`` steps during the first 60 % of the steps. Three runs from the same initial state: the batched
     form at the reference's learning rate (1e-3), the batched form at sqrt(batch) times it
     (Adam's step does not grow with the batch, so a 16-frame step otherwise moves as far as a
     1-frame step), and the one-frame-per-step form (the reference's pattern) for
@@ -334,7 +334,9 @@ def run_training(n_init: int = 2_000_000, n_gt: int = 4_000_000, n_frames: int =
         img, _, _, _ = UG.forward(b, pix, BG_A, BG_I, want_counts=False)
         return float((img - tgt).abs().mean())
 
-    rcfg = RefineConfig(every=refine_every, start=refine_every, stop=steps, max_gaussians=max_gaussians,
+    # refinement during the first 60 % of the steps, as the schedule it follows (every 2500 of
+    # 30k iterations, from 1k to 20k): the rest of the run settles the refined set
+    rcfg = RefineConfig(every=refine_every, start=refine_every, stop=int(steps * 0.6), max_gaussians=max_gaussians,
                         densify_fraction=densify_fraction)
     runs = {}
     for name, lr in (("batched", 1.0e-3), ("batched_lr_sqrt_batch", 1.0e-3 * math.sqrt(batch))):
