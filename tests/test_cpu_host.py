@@ -181,3 +181,70 @@ def test_workload_time_to_accuracy():
     assert WL._seconds_to(c, 0.3) == 1.0
     assert WL._seconds_to(c, 0.05) is None
     assert WL._seconds_to([(0.0, 0, 0.5), (1.0, 8, 0.6), (2.0, 16, 0.4)], 0.45) == 1.75
+
+
+def _ref_camera(raw, n, idx, origin):
+    """The reference loader's UltraGS camera fields for frame idx (pipeline_god_file.py:236-241,
+    269-290), restated: stored per-frame or shared values, else identity / probe origin / 0.5."""
+    import numpy as np
+
+    def mat(name):
+        if name not in raw:
+            return np.eye(4, dtype=np.float32)
+        a = raw[name].astype(np.float32)
+        return a[idx] if a.ndim == 3 and a.shape[0] == n else a
+
+    def arr(name, default):
+        if name not in raw:
+            return default.astype(np.float32)
+        a = raw[name].astype(np.float32)
+        return a[idx] if a.ndim >= 2 and a.shape[0] == n else a
+
+    def sca(name, default):
+        if name not in raw:
+            return np.float32(default)
+        a = raw[name].astype(np.float32)
+        return np.float32(a[idx] if a.ndim > 0 and a.shape[0] == n else a)
+
+    return mat("viewmatrix"), mat("projmatrix"), arr("camera_center", origin[idx]), sca("tanfovx", 0.5), \
+        sca("tanfovy", 0.5)
+
+
+def test_frame_source_camera_fields(tmp_path):
+    """UltraGS camera fields gathered per batch (device gathers; here on the CPU): per-frame,
+    shared and absent entries of the reference's NPZ layout, against the reference loader's
+    rules; an index outside the dataset is clamped and reported by check()."""
+    import numpy as np
+    import pytest
+    import torch
+
+    from us3d_b200.frames import DeviceFrameSource
+
+    n, h, w = 4, 8, 6
+    rng = np.random.default_rng(0)
+    base = dict(images=rng.integers(0, 255, (n, h, w), dtype=np.uint8),
+                probe_origin_world=rng.normal(size=(n, 3)).astype(np.float32),
+                axis_lateral_world=np.array([1, 0, 0], np.float32), axis_axial_world=np.array([0, 1, 0], np.float32),
+                axis_elevational_world=np.array([0, 0, 1], np.float32))
+    variants = [
+        {},
+        dict(viewmatrix=rng.normal(size=(n, 4, 4)).astype(np.float32), projmatrix=rng.normal(size=(4, 4)).astype(np.float32),
+             camera_center=rng.normal(size=(n, 3)).astype(np.float32), tanfovx=rng.uniform(0.1, 1, n).astype(np.float32),
+             tanfovy=np.float32(0.3)),
+        dict(camera_center=np.array([1.0, 2.0, 3.0], np.float32), tanfovx=np.float32(0.7)),
+    ]
+    for k, extra in enumerate(variants):
+        raw = dict(base, **extra)
+        path = tmp_path / f"c{k}.npz"
+        np.savez(path, **raw)
+        src = DeviceFrameSource.from_npz(path, 0.5, 0.5, device=torch.device("cpu"))
+        idx = torch.tensor([3, 0, 2], dtype=torch.int64)
+        got = src.camera(idx)
+        for j, i in enumerate(idx.tolist()):
+            want = _ref_camera(raw, n, i, base["probe_origin_world"])
+            for gv, wv in zip(got, want):
+                assert np.array_equal(gv[j].numpy(), np.asarray(wv, np.float32)), (k, i)
+        src.check()
+        src.camera(torch.tensor([1, 4], dtype=torch.int64))
+        with pytest.raises(IndexError):
+            src.check()

@@ -186,3 +186,23 @@ def test_stored_rays_and_poses_and_bad_index(cuda_device, tmp_path):
     src.geometry(torch.tensor([1, 7], dtype=torch.int64, device=dev))
     with pytest.raises(IndexError):
         src.check()
+
+
+def test_camera_fields_on_device(cuda_device):
+    """The UltraGS camera fields gathered on the GPU for a device index tensor equal the stored
+    per-frame values (shared / absent ones broadcast as the reference's loader does)."""
+    from us3d_b200.frames import DeviceFrameSource
+
+    images, g = _dataset(n=3, h=20, w=24)
+    rng = np.random.default_rng(5)
+    view = rng.normal(size=(3, 4, 4)).astype(np.float32)
+    proj = rng.normal(size=(4, 4)).astype(np.float32)
+    src = DeviceFrameSource(images, g["o"][:3], g["l"][:3], g["a"][:3], np.array([0, 0, 1], np.float32), 0.5, 0.5,
+                            device=cuda_device, viewmatrix=view, projmatrix=proj, tanfovx=np.float32(0.25))
+    idx = torch.tensor([2, 0], dtype=torch.int64, device=cuda_device)
+    v, p, c, tx, ty = src.camera(idx)
+    src.check()
+    assert torch.equal(v.cpu(), torch.from_numpy(view[[2, 0]]))
+    assert torch.equal(p.cpu(), torch.from_numpy(np.stack([proj, proj])))
+    assert torch.equal(c.cpu(), torch.from_numpy(g["o"][[2, 0]].astype(np.float32)))
+    assert torch.equal(tx.cpu(), torch.tensor([0.25, 0.25])) and torch.equal(ty.cpu(), torch.tensor([0.5, 0.5]))

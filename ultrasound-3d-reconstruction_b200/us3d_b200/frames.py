@@ -36,12 +36,17 @@ class DeviceFrameSource:
     normalised per frame); pixel_positions: optional (N,H*W,3) or (N,H,W,3) mm, otherwise
     generated from the geometry with ``delta_lateral_mm``, ``delta_axial_mm``, ``near_mm`` and
     the lateral centring of the reference's config; ray_origins / ray_dirs: optional (N,W,3) and
-    poses_world_to_probe optional (N,4,4), otherwise generated as the reference does."""
+    poses_world_to_probe optional (N,4,4), otherwise generated as the reference does. The UltraGS
+    camera fields (pipeline_god_file.py:236-241): viewmatrix / projmatrix optional (N,4,4) or one
+    (4,4) for all frames (identity when absent), camera_center optional (N,3) or (3,) (the frame's
+    probe origin when absent), tanfovx / tanfovy optional (N,) or scalars (``default_tanfov``,
+    the reference config's 0.5, when absent)."""
 
     def __init__(self, images, origin, axis_lat, axis_ax, axis_ele, delta_lateral_mm: float,
                  delta_axial_mm: float, near_mm: float = 0.0, center_lateral: bool = True,
                  pixel_positions=None, device: Optional[torch.device] = None, ray_origins=None, ray_dirs=None,
-                 poses_world_to_probe=None):
+                 poses_world_to_probe=None, viewmatrix=None, projmatrix=None, camera_center=None, tanfovx=None,
+                 tanfovy=None, default_tanfov=(0.5, 0.5)):
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         img = torch.as_tensor(np.asarray(images) if not torch.is_tensor(images) else images)
         if img.ndim == 4:
@@ -85,6 +90,25 @@ class DeviceFrameSource:
         self.ray_origins = stored(ray_origins, (self.width, 3))
         self.ray_dirs = stored(ray_dirs, (self.width, 3))
         self.poses = stored(poses_world_to_probe, (16,))
+
+        def matrices(a):
+            if a is None:
+                return torch.eye(4, dtype=torch.float32).expand(self.n, 4, 4).to(dev).contiguous()
+            m = torch.as_tensor(np.asarray(a, dtype=np.float32))
+            m = m if (m.ndim == 3 and m.shape[0] == self.n) else m.reshape(1, 4, 4).expand(self.n, 4, 4)
+            return m.to(dev).contiguous()
+
+        def scalars(a, default):
+            v = torch.as_tensor(np.asarray(a if a is not None else default, dtype=np.float32))
+            v = v.reshape(-1) if (v.ndim >= 1 and v.shape[0] == self.n) else v.reshape(1).expand(self.n)
+            return v.to(dev).contiguous()
+
+        self.viewmatrix = matrices(viewmatrix)
+        self.projmatrix = matrices(projmatrix)
+        # camera centre: stored values, else the probe origin as stored (not normalised)
+        self.camera_center = per_frame(camera_center, [0.0, 0.0, 0.0]) if camera_center is not None else o
+        self.tanfovx = scalars(tanfovx, default_tanfov[0])
+        self.tanfovy = scalars(tanfovy, default_tanfov[1])
         self.device = dev
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
@@ -101,7 +125,8 @@ class DeviceFrameSource:
             pose = np.tile(np.asarray(pose, np.float32).reshape(1, 4, 4), (n, 1, 1))  # one pose for all
         return cls(raw["images"], get("probe_origin_world"), get("axis_lateral_world"), get("axis_axial_world"),
                    get("axis_elevational_world"), delta_lateral_mm, delta_axial_mm, near_mm, center_lateral,
-                   get("pixel_positions_world"), device, get("ray_origins"), get("ray_dirs"), pose)
+                   get("pixel_positions_world"), device, get("ray_origins"), get("ray_dirs"), pose,
+                   get("viewmatrix"), get("projmatrix"), get("camera_center"), get("tanfovx"), get("tanfovy"))
 
     def frame_table(self, batch_size: int) -> UG.FrameTable:
         """An (unfilled) frame table for batches of ``batch_size`` frames."""
@@ -149,6 +174,18 @@ class DeviceFrameSource:
                              _ptr(origins), _ptr(dirs), _ptr(pose), _ptr(self.status), _stream()),
                    "us3d_frames_geometry")
         return origins, dirs, pose
+
+    def camera(self, indices: torch.Tensor):
+        """UltraGS camera fields of the dataset ``indices`` (device int64): (viewmatrix (F,4,4),
+        projmatrix (F,4,4), camera_center (F,3), tanfovx (F,), tanfovy (F,)); device gathers, no
+        synchronisation (an index outside the dataset is clamped and recorded for ``check``)."""
+        if indices.dtype != torch.int64 or indices.device != self.device:
+            raise ValueError("indices must be an int64 tensor on the dataset's device")
+        bad = ((indices < 0) | (indices >= self.n)).any().to(torch.int32)
+        torch.maximum(self.status, bad.reshape(1), out=self.status)
+        i = indices.clamp(0, self.n - 1)
+        return (self.viewmatrix.index_select(0, i), self.projmatrix.index_select(0, i),
+                self.camera_center.index_select(0, i), self.tanfovx.index_select(0, i), self.tanfovy.index_select(0, i))
 
     def check(self) -> None:
         """Raises if any index given to ``fill`` was out of range (synchronises)."""
