@@ -36,27 +36,25 @@ METRIC = "fwd+bwd frames/s @1M Gaussians 512² (batched vs plain, 1 B200); % HBM
 UNIT = "frames/s"
 BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (params, grads, outputs, upstream)
 
-# DRAM bytes (read + write) per frame of each stage's dominant kernel, from one ncu capture
-# of a 4-frame launch of the same scene (ncu --set full), scaled linearly to the frames of a
-# launch; the backward stage is the shading adjoint + the per-Gaussian reduce_kernel. Keyed by
-# backward variant (0 scalar FP32, 1 packed FP32x2); the forward is the same kernel for both.
-NCU_TRAFFIC_PER_FRAME = {
-    0: {"ug_backward": (100.252416e6 + 114.988544e6 + 156.020480e6 + 28.401920e6) / 4,
-        "ug_forward": (52.274432e6 + 5.454592e6) / 4},
-    1: {"ug_backward": (99.148032e6 + 114.697984e6 + 156.020480e6 + 28.401920e6) / 4,
-        "ug_forward": (52.270336e6 + 5.618176e6) / 4},
+# Per-frame ncu figures of each stage's kernels, from one capture of a 4-frame launch of the
+# same scene (ncu --set full; profiles/ultragauss_*_4frames.md), keyed by stage and by that
+# stage's kernel variant (0 one pixel per FP32 instruction, 1 packed FP32x2 pairs):
+#   traffic: dram__bytes_read.sum + dram__bytes_write.sum per frame (the backward stage is the
+#            shading adjoint + the per-Gaussian reduce_kernel), scaled to the launch's frames;
+#   inst:    (smsp__inst_executed.sum per frame, per launch) -- the reduction runs once per launch;
+#   fma:     sm__pipe_fma_cycles_active share of the shading kernel.
+# A variant without a capture has no entry and reports no issue figure.
+NCU_STAGE = {
+    "ug_forward": {
+        0: dict(traffic=(52.274432e6 + 5.454592e6) / 4, inst=(547342384 / 4, 0.0), fma=0.5172),
+    },
+    "ug_backward": {
+        0: dict(traffic=(100.252416e6 + 114.988544e6 + 156.020480e6 + 28.401920e6) / 4,
+                inst=(594881545 / 4, 21e6), fma=0.6857),
+        1: dict(traffic=(99.148032e6 + 114.697984e6 + 156.020480e6 + 28.401920e6) / 4,
+                inst=(377437123 / 4, 21e6), fma=0.7181),
+    },
 }
-# Warp instructions executed per frame by each stage's kernels (smsp__inst_executed.sum of the
-# same 4-frame captures, per frame): the shading kernels are bound by instruction issue or by
-# the FMA pipe, whose ceilings are 148 SMs x 4 schedulers x one warp instruction per clock.
-# (per frame, per launch): the per-Gaussian gradient reduction runs once per launch.
-NCU_WARP_INST_PER_FRAME = {
-    0: {"ug_forward": (547342384 / 4, 0.0), "ug_backward": (594881545 / 4, 21e6)},
-    1: {"ug_forward": (547342384 / 4, 0.0), "ug_backward": (377437123 / 4, 21e6)},
-}
-# Share of cycles the FMA pipe was busy in those captures (sm__pipe_fma_cycles_active).
-NCU_FMA_PIPE = {0: {"ug_forward": 0.5172, "ug_backward": 0.6857},
-                1: {"ug_forward": 0.5178, "ug_backward": 0.7181}}
 SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 
@@ -74,7 +72,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-train", action="store_true", help="skip the training-step measurement")
     ap.add_argument("--launch-shape", default=None,
-                    help="forward batch / backward threads [/ backward variant 0 scalar, 1 packed], e.g. "
+                    help="forward batch / backward threads [/ backward variant [/ forward variant]] (0 scalar, 1 packed), e.g. "
                          "512/256/1, instead of autotuning")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -253,14 +251,15 @@ def run_b200(a):
         return max_over_ranks(st.elapsed_time(en), device=dev)
 
     # -- launch-shape autotuning on the first batch (untimed; changes no result) --
-    from us3d_b200.batch import autotune_launch, set_backward_variant, set_launch_config
+    from us3d_b200.batch import autotune_launch, set_backward_variant, set_forward_variant, set_launch_config
 
     if a.launch_shape:
         launch_shape = tuple(int(x) for x in a.launch_shape.split("/"))
-        if len(launch_shape) == 2:
-            launch_shape = (*launch_shape, 1)
+        launch_shape = (*launch_shape, 1, 0)[:4] if len(launch_shape) == 2 else \
+            ((*launch_shape, 0) if len(launch_shape) == 3 else launch_shape)
         set_launch_config(launch_shape[0], launch_shape[1])
         set_backward_variant(launch_shape[2])
+        set_forward_variant(launch_shape[3])
         tuned = {}
     else:
         tuned = autotune_launch(batches[0][0], params, batches[0][1])
@@ -331,7 +330,8 @@ def run_b200(a):
     peaks = json.load(open(ROOT / "MEASURED_PEAKS.json")) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg / (stage_avg_ms / 1e3) / 1e9
-    traffic = NCU_TRAFFIC_PER_FRAME[launch_shape[2]].get(dominant)
+    variants = {"ug_forward": launch_shape[3], "ug_backward": launch_shape[2]}
+    traffic = NCU_STAGE.get(dominant, {}).get(variants.get(dominant), {}).get("traffic")
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": int(traffic * F) if traffic else None,
                 "traffic_source": "ncu dram bytes of a 4-frame launch scaled to the launch's frames" if traffic else None,
@@ -345,7 +345,7 @@ def run_b200(a):
     step_gbs = b_frame * frames_total / (ms_batched / 1e3) / 1e9
     roofline["step"] = {"bytes_per_frame": int(b_frame), "achieved": round(step_gbs, 2),
                         "frac": round(step_gbs / peak, 4)}
-    roofline["issue"] = issue_roofline(stage_ms, F, clocks, launch_shape[2])
+    roofline["issue"] = issue_roofline(stage_ms, F, clocks, variants)
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -357,7 +357,8 @@ def run_b200(a):
         "batched_form": "CUDA-graph replay of bin + forward + L1 gradient + backward per 16-frame batch",
         "launch_config": {"forward_batch": launch_shape[0], "backward_threads": launch_shape[1],
                           "backward_variant": ["scalar fp32", "packed fp32x2"][launch_shape[2]],
-                          "autotune_ms_per_step": {f"{k[0]}/{k[1]}/{k[2]}": round(v, 3) for k, v in tuned.items()}},
+                          "forward_variant": ["scalar fp32", "packed fp32x2"][launch_shape[3]],
+                          "autotune_ms_per_step": {"/".join(map(str, k)): round(v, 3) for k, v in tuned.items()}},
         "uncaptured": {"value": round(uncaptured_value, 3), "unit": UNIT,
                        "note": "same step launched from Python with one instance-total readback; "
                                "the roofline stage times come from this run's CUDA events"},
@@ -386,26 +387,28 @@ def run_b200(a):
         print(json.dumps(out), flush=True)
 
 
-def issue_roofline(stage_ms, frames_per_launch, clocks, variant=1):
+def issue_roofline(stage_ms, frames_per_launch, clocks, variants):
     """The bound the shading kernels actually meet: warp instructions issued per second
     against the GPU's issue ceiling (148 SMs x 4 schedulers x 1 warp instruction per clock at
     the median SM clock sampled during the timed region), per stage, from the instruction
-    counts of the committed ncu capture scaled to the launch's frames and this run's
-    CUDA-event stage times."""
+    counts of the committed ncu capture of the stage's kernel variant scaled to the launch's
+    frames and this run's CUDA-event stage times."""
     mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
     ceiling = SM_COUNT * SCHEDULERS_PER_SM * mhz * 1e6  # warp instructions / s
     out = {"bound": "instruction issue", "unit": "warp inst/s", "sm_mhz": mhz, "peak": ceiling,
            "source": "smsp__inst_executed.sum per frame of a 4-frame ncu capture (profiles/) x frames per launch "
                      "/ CUDA-event stage time; peak = 148 SMs x 4 schedulers x median SM clock"}
-    for stage, (per_frame, per_launch) in NCU_WARP_INST_PER_FRAME[variant].items():
+    for stage, by_variant in NCU_STAGE.items():
         ms = stage_ms.get(stage)
-        if not ms:
+        fig = by_variant.get(variants.get(stage))
+        if not ms or fig is None:
             continue
+        per_frame, per_launch = fig["inst"]
         inst = per_frame * frames_per_launch + per_launch
         achieved = inst / (ms / 1e3)
         out[stage] = {"achieved": round(achieved, 1), "frac": round(achieved / ceiling, 4),
-                      "warp_inst_per_launch": int(inst), "stage_ms": round(ms, 4),
-                      "fma_pipe_busy": NCU_FMA_PIPE[variant].get(stage)}
+                      "warp_inst_per_launch": int(inst), "stage_ms": round(ms, 4), "variant": variants.get(stage),
+                      "fma_pipe_busy": fig["fma"]}
     return out
 
 

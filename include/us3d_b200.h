@@ -221,6 +221,16 @@ US3D_API int us3d_ug_get_launch_config(int32_t* forward_batch, int32_t* backward
 US3D_API int us3d_ug_set_backward_variant(int32_t variant);
 US3D_API int us3d_ug_get_backward_variant(int32_t* variant);
 
+/* Forward kernel variant of the UltraGauss shading (process-wide, read at every launch): 0 =
+ * one pixel per thread and FP32 instruction, 1 = two pixels per thread and packed FP32
+ * instruction (sm_100 f32x2; 128-thread blocks whose warps own 8x8 quadrants, at most 256
+ * staged Gaussians per batch (a forward batch of 512 runs as 256); each lane
+ * rounds as the scalar kernel, so images, alpha, depth and the saved sums are bit-identical).
+ * The windowed case (diag_beta < 1e-10) always uses variant 0. Default 0. No counterpart in
+ * the reference. */
+US3D_API int us3d_ug_set_forward_variant(int32_t variant);
+US3D_API int us3d_ug_get_forward_variant(int32_t* variant);
+
 /*
  * Per-frame image loss of the reference's training step (image_loss in
  * pipeline_god_file.py:606-617 with simple_ssim at :627-637): for each frame f of the table,

@@ -499,9 +499,11 @@ def test_graphed_training_step_matches_eager(cuda_device):
 
 def test_launch_shapes_same_results_and_autotune(cuda_device):
     """Every launch shape of the shading kernels (forward batch 128/256/512, backward CTA
-    128/256 threads) gives bit-identical images and gradients for each backward variant; the
-    two variants (scalar FP32, packed f32x2 pairs) give the same images and gradients within
-    summation-order rounding; the autotuner times every (shape, variant) and keeps the fastest."""
+    128/256 threads) and both forward variants (one pixel per thread, two pixels per thread in
+    packed f32x2) give bit-identical images and gradients for each backward variant; the two
+    backward variants (scalar FP32, packed f32x2 pairs) give the same images and gradients
+    within summation-order rounding; the autotuner times every (shape, variant pair) and keeps
+    the fastest."""
     from ug_helpers import rel_l2
     from us3d_b200 import batch as B
     from us3d_b200 import ultragauss as UG
@@ -509,30 +511,37 @@ def test_launch_shapes_same_results_and_autotune(cuda_device):
     args, ft, pix, grads = _cull_case(cuda_device, G=60000)
     default = B.get_launch_config()
     default_variant = B.get_backward_variant()
+    default_fvariant = B.get_forward_variant()
     outs = {}
     try:
+        for fvariant in B.FORWARD_VARIANTS:
+            B.set_forward_variant(fvariant)
+            for variant in B.BACKWARD_VARIANTS:
+                B.set_backward_variant(variant)
+                for shape in B.LAUNCH_SHAPES:
+                    B.set_launch_config(*shape)
+                    b = UG.bin_gaussians(*args, ft, 7.815, 1e-4, True, slice_cull_pixels=pix)
+                    img, alpha, depth, _ = UG.forward(b, pix, 1e-6, 0.0, want_counts=False)
+                    g = UG.backward(b, pix, grads[0], grads[1], grads[2], alpha, 1e-6, 0.0)
+                    outs[(*shape, variant, fvariant)] = [x.cpu().numpy() for x in (img, alpha, depth, *g)]
         for variant in B.BACKWARD_VARIANTS:
-            B.set_backward_variant(variant)
-            for shape in B.LAUNCH_SHAPES:
-                B.set_launch_config(*shape)
-                b = UG.bin_gaussians(*args, ft, 7.815, 1e-4, True, slice_cull_pixels=pix)
-                img, alpha, depth, _ = UG.forward(b, pix, 1e-6, 0.0, want_counts=False)
-                g = UG.backward(b, pix, grads[0], grads[1], grads[2], alpha, 1e-6, 0.0)
-                outs[(*shape, variant)] = [x.cpu().numpy() for x in (img, alpha, depth, *g)]
-        for variant in B.BACKWARD_VARIANTS:
-            ref = outs[(*default, variant)]
-            for shape in B.LAUNCH_SHAPES:
-                for x, y in zip(outs[(*shape, variant)], ref):
-                    assert np.array_equal(x, y), (shape, variant)
-        scalar, packed = outs[(*default, 0)], outs[(*default, 1)]
+            ref = outs[(*default, variant, 0)]
+            for fvariant in B.FORWARD_VARIANTS:
+                for shape in B.LAUNCH_SHAPES:
+                    for x, y in zip(outs[(*shape, variant, fvariant)], ref):
+                        assert np.array_equal(x, y), (shape, variant, fvariant)
+        scalar, packed = outs[(*default, 0, 0)], outs[(*default, 1, 0)]
         for x, y in zip(scalar[:3], packed[:3]):
             assert np.array_equal(x, y)  # the forward is the same kernel
         for x, y in zip(scalar[3:], packed[3:]):
             assert rel_l2(y, x) <= 1e-5
         timings = B.autotune_launch(ft, list(args), pix, reps=1)
-        assert set(timings) == {(*s, v) for s in B.LAUNCH_SHAPES for v in B.BACKWARD_VARIANTS}
+        assert set(timings) == {(*s, v, f) for s in B.LAUNCH_SHAPES for v in B.BACKWARD_VARIANTS
+                                for f in B.FORWARD_VARIANTS if not (f == 1 and s[0] == 512)}
         best = min(timings, key=timings.get)
         assert B.get_launch_config() == best[:2] and B.get_backward_variant() == best[2]
+        assert B.get_forward_variant() == best[3]
     finally:
         B.set_launch_config(*default)
         B.set_backward_variant(default_variant)
+        B.set_forward_variant(default_fvariant)

@@ -152,3 +152,29 @@ def test_headline_workload_graph_replay_bit_identical(headline, cuda_device):
         step.check()
         for got, ref in zip(out, grads):
             assert torch.equal(got, ref)
+
+
+def test_headline_packed_forward_bit_identical(headline, cuda_device):
+    """The packed forward (two pixels per thread, f32x2) on the benchmarked workload: images,
+    alpha, depth and the gradients that depend on its saved sums are bit-identical to the
+    scalar forward's, in the batched slice-culled form and in the per-frame full binning."""
+    from us3d_b200 import batch as B
+    from us3d_b200 import ultragauss as UG
+
+    h = headline
+    P1 = h["P1"]
+    default = B.get_forward_variant()
+    try:
+        res = {}
+        for v in (0, 1):
+            B.set_forward_variant(v)
+            _, outs, grads = _batched(h)
+            single = UG.build_frame_table([h["specs"][3]], cuda_device)
+            b1 = UG.bin_gaussians(*h["params"], single, CHI2, BETA, True)
+            img1, a1, d1, _ = UG.forward(b1, h["pixels"][3 * P1:4 * P1], BG_A, BG_I, want_counts=False)
+            res[v] = [x.clone() for x in (*outs, *grads, img1, a1, d1)]
+            del b1
+        for x, y in zip(res[0], res[1]):
+            assert torch.equal(x, y)
+    finally:
+        B.set_forward_variant(default)

@@ -1089,6 +1089,139 @@ __device__ __forceinline__ f32x2 tri2(f32x2 a, f32x2 b, f32x2 c, f32x2 d, f32x2 
 #endif
 }
 
+// Forward with two pixels per thread in FP32x2 arithmetic. One 128-thread block per tile; warp
+// W (0..3) owns the 8x8 quadrant (column 8 (W & 1), row 8 (W >> 1)), i.e. 4x4 sub-blocks of
+// bands 2 (W >> 1) and 2 (W >> 1) + 1 and quarters 2 (W & 1) and 2 (W & 1) + 1, and visits a
+// staged Gaussian when its mask marks any of those four. Lane l shades pixels (x, y) and
+// (x, y + 4) of the quadrant, x = l & 7, y = l >> 3. Staged values are stored twice, {v, v},
+// so that one float4 load gives two operand pairs. Every lane rounds as forward_kernel does:
+// d, the quadratic form (the reference's term order with the contractions of the compiled
+// scalar expression, tri2), q * (-log2(e)/2), the exponential (scalar ex2), ah = o * e and the
+// sums, where a pair that does not contribute adds an exact zero (fma(0, v, s) = s); a Gaussian
+// visited because it marks another sub-block of the quadrant fails the chi-square test on
+// every pixel of this one and adds zeros too. Images, alpha, depth and the no-skip sums are
+// therefore bit-identical to forward_kernel's. (Not for the windowed case, beta < 1e-10.)
+template <int BATCH>
+__global__ void __launch_bounds__(128, 8)
+forward_packed_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames,
+                      const int* __restrict__ tile_frame, const int* __restrict__ tile_start,
+                      const int* __restrict__ sorted_gid, const blockmask_t* __restrict__ sorted_mask,
+                      const long long* __restrict__ header, const float4* __restrict__ pack,
+                      const float* __restrict__ pixels, float chi2, float beta, float bg_alpha, float bg_intensity,
+                      float* __restrict__ out_image, float* __restrict__ out_alpha, float* __restrict__ out_depth,
+                      float2* __restrict__ pixel_aux) {
+    constexpr int REC = 6;  // float4 per staged Gaussian: {mx,mx,my,my} {mz,mz,o,o} {q0,q0,q1,q1}
+                            // {q2,q2,q3,q3} {s12,s12,s22,s22} {c,c,dt,dt}
+    __shared__ float4 s_st[REC * BATCH];
+    __shared__ blockmask_t s_blocks[BATCH];
+    __shared__ unsigned short s_list[4][BATCH];
+    static_assert((BATCH - 1) * REC * 16 <= 0xffff, "staged offsets must fit 16 bits");
+    const int64_t t = blockIdx.x;
+    if (t >= T || header[H_FLAGS] != 0 || tile_frame[t] < 0) return;
+    const Geo geo = load_geo(frames + tile_frame[t]);
+    int tx, ty;
+    find_tile_coords(geo, t, tx, ty);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qc = warp & 1, qr = warp >> 1;
+    const int px = tx * TILE + 8 * qc + (lane & 7);
+    const int py0 = ty * TILE + 8 * qr + (lane >> 3), py1 = py0 + 4;
+    const int64_t p0 = (int64_t)geo.pix_off + (int64_t)py0 * geo.W + px;
+    const int64_t p1 = (int64_t)geo.pix_off + (int64_t)py1 * geo.W + px;
+    const bool valid0 = px < geo.W && py0 < geo.H && p0 < P;
+    const bool valid1 = px < geo.W && py1 < geo.H && p1 < P;
+    float3 pa = make_float3(0.f, 0.f, 0.f), pb = make_float3(0.f, 0.f, 0.f);
+    if (valid0) pa = make_float3(pixels[3 * p0], pixels[3 * p0 + 1], pixels[3 * p0 + 2]);
+    if (valid1) pb = make_float3(pixels[3 * p1], pixels[3 * p1 + 1], pixels[3 * p1 + 2]);
+    const f32x2 PX = pk2(pa.x, pb.x), PY = pk2(pa.y, pb.y), PZ = pk2(pa.z, pb.z);
+    const f32x2 CE = pk2(kNegHalfLog2e, kNegHalfLog2e);
+    const int s0 = tile_start[t];
+    const int n = tile_start[t + 1] - s0;
+    const bool culled = header[H_MODE] != 0;
+    const unsigned qmask = 0x33u << (8 * qr + 2 * qc);  // the quadrant's four sub-blocks
+
+    f32x2 sa = pk2(0.f, 0.f), sc = sa, sd = sa, kc = sa, kd = sa;
+    auto shade = [&](int off) {  // off: byte offset of the staged Gaussian in s_st
+        const float4* f = reinterpret_cast<const float4*>(reinterpret_cast<const char*>(s_st) + off);
+        const float4 f0 = f[0], f1 = f[1], f2 = f[2], f3 = f[3], f4 = f[4], f5 = f[5];
+        const f32x2 dx = sub2(PX, pk2(f0.x, f0.y)), dy = sub2(PY, pk2(f0.z, f0.w)), dz = sub2(PZ, pk2(f1.x, f1.y));
+        const f32x2 Q0 = pk2(f2.x, f2.y), Q1 = pk2(f2.z, f2.w), Q2 = pk2(f3.x, f3.y), Q3 = pk2(f3.z, f3.w);
+        const f32x2 S12 = pk2(f4.x, f4.y), S22 = pk2(f4.z, f4.w);
+        const f32x2 t0 = tri2(Q0, dx, Q1, dy, Q2, dz);
+        const f32x2 t1 = tri2(Q1, dx, Q3, dy, S12, dz);
+        const f32x2 t2 = tri2(Q2, dx, S12, dy, S22, dz);
+        const f32x2 q = tri2(t0, dx, t1, dy, t2, dz);
+        float q0, q1, e0, e1;
+        up2(q, q0, q1);
+        up2(mul2(q, CE), e0, e1);
+        float ah0, ah1;
+        up2(mul2(pk2(f1.z, f1.w), pk2(exp2f(e0), exp2f(e1))), ah0, ah1);  // o * exp(-q/2)
+        const bool pass0 = q0 <= chi2, pass1 = q1 <= chi2;
+        const bool keep0 = pass0 && ah0 > 1e-8f, keep1 = pass1 && ah1 > 1e-8f;
+        const f32x2 ak = pk2(keep0 ? ah0 : 0.f, keep1 ? ah1 : 0.f);
+        const f32x2 C = pk2(f5.x, f5.y), D = pk2(f5.z, f5.w);
+        sa = add2(sa, ak);
+        sc = fma2(ak, C, sc);
+        sd = fma2(ak, D, sd);
+        if (pass0 != keep0 || pass1 != keep1) {  // the reference's alpha-hat <= 1e-8 pairs (rare)
+            const f32x2 ap = pk2(pass0 && !keep0 ? ah0 : 0.f, pass1 && !keep1 ? ah1 : 0.f);
+            kc = fma2(ap, C, kc);
+            kd = fma2(ap, D, kd);
+        }
+    };
+    for (int b0 = 0; b0 < n; b0 += BATCH) {
+        const int nb = min(BATCH, n - b0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+            const int g = sorted_gid[s0 + b0 + j];
+            const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+            const float dterm = f3_dot(f3_sub(make_float3(a.x, a.y, a.z), geo.o), geo.ele);
+            float4 q1;
+            float s12, s22;
+            precision_from_raw(b.x, b.y, b.z, b.w, c.x, c.y, beta, q1, s12, s22);
+            float4* d = s_st + REC * j;
+            d[0] = make_float4(a.x, a.x, a.y, a.y);
+            d[1] = make_float4(a.z, a.z, a.w, a.w);
+            d[2] = make_float4(q1.x, q1.x, q1.y, q1.y);
+            d[3] = make_float4(q1.z, q1.z, q1.w, q1.w);
+            d[4] = make_float4(s12, s12, s22, s22);
+            d[5] = make_float4(c.z, c.z, dterm, dterm);
+            s_blocks[j] = sorted_mask[s0 + b0 + j];
+        }
+        __syncthreads();
+        if (!culled) {
+            for (int j = 0; j < nb; ++j) shade(j * (REC * 16));
+            continue;
+        }
+        int n_w = 0;
+        for (int jc = 0; jc < nb; jc += 32) {
+            const int jl = jc + lane;
+            const bool mine = jl < nb && (s_blocks[jl] & qmask);
+            const unsigned bits = __ballot_sync(0xffffffffu, mine);
+            if (mine) s_list[warp][n_w + __popc(bits & ((1u << lane) - 1u))] = (unsigned short)(jl * (REC * 16));
+            n_w += __popc(bits);
+        }
+        __syncwarp();
+        for (int k = 0; k < n_w; ++k) shade(s_list[warp][k]);
+    }
+    float a0, a1, c0, c1, d0, d1, kc0, kc1, kd0, kd1;
+    up2(sa, a0, a1);
+    up2(sc, c0, c1);
+    up2(sd, d0, d1);
+    up2(kc, kc0, kc1);
+    up2(kd, kd0, kd1);
+    auto store = [&](int64_t p, float s_a, float s_c, float s_d, float k_c, float k_d) {
+        const float alpha_total = s_a + bg_alpha;
+        const float num = s_c + bg_alpha * bg_intensity;
+        const float img = num / fmaxf(alpha_total, 1e-8f);
+        out_alpha[p] = alpha_total;
+        out_image[p] = fmaxf(0.0f, fminf(1.0f, img));
+        out_depth[p] = s_d / fmaxf(s_a, 1e-8f);
+        pixel_aux[p] = make_float2(s_c + k_c, s_d + k_d);
+    };
+    if (valid0) store(p0, a0, c0, d0, kc0, kd0);
+    if (valid1) store(p1, a1, c1, d1, kc1, kd1);
+}
+
 template <bool LOSS, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 backward_packed_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames,
@@ -1415,6 +1548,7 @@ static std::atomic<int> g_fwd_batch{FWD_BATCH};
 static std::atomic<int> g_bwd_threads{BWD_THREADS};
 // Backward kernel variant: 0 scalar FP32, 1 packed FP32 pairs (backward_packed_kernel).
 static std::atomic<int> g_bwd_variant{0};
+static std::atomic<int> g_fwd_variant{0};
 
 extern "C" int us3d_ug_set_launch_config(int32_t forward_batch, int32_t backward_threads) {
     US3D_CHECK_ARG(forward_batch == 128 || forward_batch == 256 || forward_batch == 512,
@@ -1442,6 +1576,19 @@ extern "C" int us3d_ug_set_backward_variant(int32_t variant) {
 extern "C" int us3d_ug_get_backward_variant(int32_t* variant) {
     US3D_CHECK_ARG(variant != nullptr, "variant is NULL");
     *variant = g_bwd_variant.load();
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_set_forward_variant(int32_t variant) {
+    US3D_CHECK_ARG(variant == 0 || variant == 1, "forward variant must be 0 (scalar) or 1 (packed pairs), got %d",
+                   variant);
+    g_fwd_variant.store(variant);
+    return US3D_OK;
+}
+
+extern "C" int us3d_ug_get_forward_variant(int32_t* variant) {
+    US3D_CHECK_ARG(variant != nullptr, "variant is NULL");
+    *variant = g_fwd_variant.load();
     return US3D_OK;
 }
 
@@ -1624,8 +1771,19 @@ extern "C" int us3d_ug_forward(void* workspace, const us3d_slice_frame* frames, 
             n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_mask, w.header, w.pack,
             pixels, chi2, beta, bg_alpha, bg_intensity, out_image, out_alpha, out_depth, w.pixel_aux);
     };
+    auto launch_packed = [&](auto kernel) {
+        kernel<<<(unsigned)n_tiles, 128, 0, stream>>>(
+            n_tiles, n_pixels, frames, w.tile_frame, w.tile_start, w.sorted_gid, w.sorted_mask, w.header, w.pack,
+            pixels, chi2, beta, bg_alpha, bg_intensity, out_image, out_alpha, out_depth, w.pixel_aux);
+    };
     if (!window_implied(beta)) {
         launch(forward_kernel<256, true>);
+    } else if (g_fwd_variant.load() == 1) {
+        // at most 256 staged Gaussians (96 bytes each) fit the static shared memory
+        if (g_fwd_batch.load() == 128)
+            launch_packed(forward_packed_kernel<128>);
+        else
+            launch_packed(forward_packed_kernel<256>);
     } else {
         switch (g_fwd_batch.load()) {
             case 128: launch(forward_kernel<128, false>); break;

@@ -112,6 +112,8 @@ _SIGNATURES = {
     "us3d_ug_get_launch_config": (c_int32, [POINTER(c_int32), POINTER(c_int32)]),
     "us3d_ug_set_backward_variant": (c_int32, [c_int32]),
     "us3d_ug_get_backward_variant": (c_int32, [POINTER(c_int32)]),
+    "us3d_ug_set_forward_variant": (c_int32, [c_int32]),
+    "us3d_ug_get_forward_variant": (c_int32, [POINTER(c_int32)]),
     "us3d_ug_refine_stats": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
     "us3d_ug_loss_scratch_bytes": (c_size_t, [c_int32]),
     "us3d_ug_loss": (

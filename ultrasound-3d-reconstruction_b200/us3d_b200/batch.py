@@ -121,6 +121,23 @@ class GraphedTrainingStep:
 
 LAUNCH_SHAPES = [(b, t) for b in (128, 256, 512) for t in (128, 256)]
 BACKWARD_VARIANTS = (0, 1)  # one pixel per FP32 instruction / two pixels per packed FP32 pair
+FORWARD_VARIANTS = (0, 1)   # one pixel per thread / two pixels per thread in packed FP32 pairs
+
+
+def get_forward_variant() -> int:
+    import ctypes
+
+    from . import _lib
+
+    v = ctypes.c_int32(0)
+    _lib.check(_lib.call("us3d_ug_get_forward_variant", ctypes.byref(v)), "us3d_ug_get_forward_variant")
+    return int(v.value)
+
+
+def set_forward_variant(variant: int) -> None:
+    from . import _lib
+
+    _lib.check(_lib.call("us3d_ug_set_forward_variant", int(variant)), "us3d_ug_set_forward_variant")
 
 
 def get_backward_variant() -> int:
@@ -160,11 +177,12 @@ def set_launch_config(forward_batch: int, backward_threads: int) -> None:
 def autotune_launch(frames: UG.FrameTable, params, pixels: torch.Tensor, reps: int = 3,
                     chi2_threshold: float = 7.815, diag_beta: float = 1e-4, bg_alpha: float = 1e-6):
     """Times the batched step (slice-culled bin, forward, backward with a seeded upstream
-    gradient) on the caller's frames for every launch shape the library is built for and both
-    backward variants, keeps the fastest (set_launch_config, set_backward_variant) and returns
-    {(forward_batch, backward_threads, backward_variant): ms per step}. The shapes change no
-    result; the variants differ in the backward's summation order only. Synchronises; run it
-    before capturing graphs."""
+    gradient) on the caller's frames for every launch shape the library is built for and every
+    forward and backward variant, keeps the fastest (set_launch_config, set_backward_variant,
+    set_forward_variant) and returns {(forward_batch, backward_threads, backward_variant,
+    forward_variant): ms per step}. Neither the shapes nor the forward variants change any
+    result; the backward variants differ in summation order only. Synchronises; run it before
+    capturing graphs."""
     means, tril, opac, inten = params[0], params[1].contiguous(), params[2].reshape(-1), params[3].reshape(-1)
     g = torch.Generator(device=pixels.device)
     g.manual_seed(0)
@@ -181,20 +199,25 @@ def autotune_launch(frames: UG.FrameTable, params, pixels: torch.Tensor, reps: i
         UG.backward(bb, pixels, d_image, zeros, zeros, alpha, bg_alpha, 0.0)
 
     timings = {}
-    for variant in BACKWARD_VARIANTS:
-        set_backward_variant(variant)
-        for shape in LAUNCH_SHAPES:
-            set_launch_config(*shape)
-            step()
-            torch.cuda.synchronize(pixels.device)
-            st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            st.record()
-            for _ in range(reps):
+    for fvariant in FORWARD_VARIANTS:
+        set_forward_variant(fvariant)
+        for variant in BACKWARD_VARIANTS:
+            set_backward_variant(variant)
+            for shape in LAUNCH_SHAPES:
+                if fvariant == 1 and shape[0] == 512:
+                    continue  # the packed forward stages at most 256 Gaussians (same as 256)
+                set_launch_config(*shape)
                 step()
-            en.record()
-            en.synchronize()
-            timings[(*shape, variant)] = st.elapsed_time(en) / reps
+                torch.cuda.synchronize(pixels.device)
+                st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                st.record()
+                for _ in range(reps):
+                    step()
+                en.record()
+                en.synchronize()
+                timings[(*shape, variant, fvariant)] = st.elapsed_time(en) / reps
     best = min(timings, key=timings.get)
     set_launch_config(best[0], best[1])
     set_backward_variant(best[2])
+    set_forward_variant(best[3])
     return timings
