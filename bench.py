@@ -47,6 +47,7 @@ BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (param
 NCU_STAGE = {
     "ug_forward": {
         0: dict(traffic=(52.274432e6 + 5.454592e6) / 4, inst=(547342384 / 4, 0.0), fma=0.5172),
+        1: dict(traffic=(52.252416e6 + 4.260352e6) / 4, inst=(487111780 / 4, 0.0), fma=0.5661),
     },
     "ug_backward": {
         0: dict(traffic=(100.252416e6 + 114.988544e6 + 156.020480e6 + 28.401920e6) / 4,
