@@ -25,6 +25,7 @@
 #include <algorithm>
 
 #include <atomic>
+#include <type_traits>
 
 #include "us3d_common.cuh"
 #include "scan.cuh"
@@ -766,9 +767,12 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
     const bool culled = header[H_MODE] != 0;
 
     // sums over the contributing pairs; kc, kd: the pairs the reference leaves out of the image
-    // (alpha-hat <= 1e-8) but keeps in the backward's numerator / depth sums
+    // (alpha-hat <= 1e-8) but keeps in the backward's numerator / depth sums. Such a pair needs
+    // a Gaussian whose alpha-hat can fall to 1e-8 inside the chi-square region; when no staged
+    // Gaussian of a batch can (TINY false), the batch runs without that test.
     float sa = 0.f, sc = 0.f, sd = 0.f, kc = 0.f, kd = 0.f;
-    auto shade = [&](int off) {  // off: byte offset of the staged Gaussian in s_st
+    auto shade = [&](int off, auto tiny) {  // off: byte offset of the staged Gaussian in s_st
+        constexpr bool TINY = decltype(tiny)::value;
         const float4* f = reinterpret_cast<const float4*>(reinterpret_cast<const char*>(s_st) + off);
         const float4 f0 = f[0], f1 = f[1], f2 = f[2];
         const float3 d = make_float3(pv.x - f0.x, pv.y - f0.y, pv.z - f0.z);
@@ -781,23 +785,28 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
         const float q = quad_form(d, f1, f2.x, f2.y);
         const float ah = f0.w * exp2f(q * kNegHalfLog2e);  // exp(-q/2), as in the backward
         const bool pass = q <= chi2;
-        const bool keep = pass && ah > 1e-8f;
+        const bool keep = pass && (!TINY || ah > 1e-8f);
         if (keep) {
             sa += ah;
             sc += ah * f2.z;
             sd += ah * f2.w;
         }
-        if (pass && !keep) {
+        if (TINY && pass && !keep) {
             kc += ah * f2.z;
             kd += ah * f2.w;
         }
     };
+    // alpha-hat of a passing pair is at least o * exp2(chi2 * (-log2(e)/2)) up to the rounding
+    // of the product and the exponential, which the factor 0.99999 covers
+    const float ah_floor = exp2f(chi2 * kNegHalfLog2e) * 0.99999f;
     for (int b0 = 0; b0 < n; b0 += BATCH) {
         const int nb = min(BATCH, n - b0);
         __syncthreads();
+        int tiny = 0;
         for (int j = threadIdx.x; j < nb; j += blockDim.x) {
             const int g = sorted_gid[s0 + b0 + j];
             const float4 a = pack[3 * g], b = pack[3 * g + 1], c = pack[3 * g + 2];
+            tiny |= !(a.w * ah_floor > 1e-8f);
             const float dterm = f3_dot(f3_sub(make_float3(a.x, a.y, a.z), geo.o), geo.ele);
             float4 q1;
             float s12, s22;
@@ -813,10 +822,13 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
             }
             s_blocks[j] = sorted_mask[s0 + b0 + j];
         }
-        __syncthreads();
+        const bool any_tiny = __syncthreads_or(tiny) != 0;
         // Lanes of an invalid pixel run along (their sums are never stored).
         if (!culled) {
-            for (int j = 0; j < nb; ++j) shade(j * (STRIDE * 16));
+            if (any_tiny)
+                for (int j = 0; j < nb; ++j) shade(j * (STRIDE * 16), std::true_type{});
+            else
+                for (int j = 0; j < nb; ++j) shade(j * (STRIDE * 16), std::false_type{});
             continue;
         }
         // Each warp lists, in staging order, the Gaussians whose mask marks one of its two
@@ -830,7 +842,10 @@ forward_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict__ frames
             n_w += __popc(bits);
         }
         __syncwarp();
-        for (int k = 0; k < n_w; ++k) shade(s_list[warp][k]);
+        if (any_tiny)
+            for (int k = 0; k < n_w; ++k) shade(s_list[warp][k], std::true_type{});
+        else
+            for (int k = 0; k < n_w; ++k) shade(s_list[warp][k], std::false_type{});
     }
     if (!valid) return;
     const float alpha_total = sa + bg_alpha;
