@@ -116,13 +116,17 @@ def test_live_reference_parity(G, H, W, spacing, seed, sort, cuda_device):
 
 def test_live_reference_parity_dense_tiles(cuda_device):
     """120000 Gaussians in a 16 mm cube under a 96x96 slice: tile buckets of every size class
-    of the tile sort (in-register segments, the 48 KB shared-memory pass, the 192 KB pass above
-    4096 keys, the global-memory network above 16384) against the reference's own binning."""
+    of the tile sort (in-register segments, the 48 KB shared-memory pass, the 64 KB packed pass
+    for 4097-8192 keys, the 192 KB pass up to 16384, the global-memory network above) against
+    the reference's own binning."""
     REF, REFK = _reference_modules()
     fx = _scene_case(120000, 96, 96, 0.25, 5, frame=1, cube_mm=16.0)
     fx.update(_reference_run(REF, REFK, fx, cuda_device))
     n = fx["ref_range_end"] - fx["ref_range_start"]
-    assert n.max() > 16384 and ((n > 4096) & (n <= 16384)).any() and ((n > 64) & (n <= 2048)).any()
+    print("bucket sizes: max", int(n.max()), "in (4096, 8192]:", int(((n > 4096) & (n <= 8192)).sum()),
+          "in (8192, 16384]:", int(((n > 8192) & (n <= 16384)).sum()))
+    assert n.max() > 16384 and ((n > 64) & (n <= 2048)).any()
+    assert ((n > 4096) & (n <= 8192)).any() and ((n > 8192) & (n <= 16384)).any()
     out = run_b200(fx, cuda_device)
     _assert_case(out, fx)
 

@@ -10,9 +10,10 @@ namespace us3d {
 
 constexpr int SORT_THREADS = 512;
 // Tiles of up to SORT_SMEM_CAP keys are ordered in shared memory by the first sort pass
-// (48 KB, four 512-thread blocks per SM); larger ones, up to SORT_BIG_CAP, by a second pass
-// with 192 KB (one block per SM); beyond that the network runs on global memory (one block
-// per tile).
+// (48 KB, four 512-thread blocks per SM); up to SORT_MID_CAP keys, when every element index of
+// the call fits a 13-bit slot packing, by a pass with 64 KB (three blocks per SM); larger ones,
+// up to SORT_BIG_CAP, by a pass with 192 KB (one block per SM); beyond that the network runs on
+// global memory (one block per tile).
 constexpr int SORT_SMEM_CAP = 4096;
 constexpr int SORT_BIG_CAP = 16384;
 constexpr int SORT_MIN_BLOCKS = 4;
@@ -340,6 +341,42 @@ static __device__ void block_sort_smem(unsigned long long* sk, int* sv, int npow
 // (hi << 32 | g << 12 | slot), which orders like the key itself (a bucket holds an element
 // once) and carries the bucket slot in its low 12 bits.
 constexpr int64_t SORT_PACK_G = (1 << 20) - 1;
+// Buckets of SORT_SMEM_CAP < n <= SORT_MID_CAP keys whose element indices are below
+// SORT_PACK_G_MID sort the same way with a 13-bit slot field, in 64 KB (three blocks per SM).
+constexpr int SORT_MID_CAP = 8192;
+constexpr int SORT_MID_SLOT_BITS = 13;
+constexpr int64_t SORT_PACK_G_MID = (1 << 19) - 1;
+
+// The packed sort of bucket t (n keys at s0, n <= 2^slot_bits, every element index below
+// 2^(32 - slot_bits)): the key (hi << 32 | g) is packed as (hi << 32 | g << slot_bits | slot),
+// which orders like the key itself (a bucket holds an element once) and carries the bucket
+// slot in its low slot_bits bits.
+static __device__ __forceinline__ void sort_bucket_packed(unsigned long long* s_keys, int s0, int n, int slot_bits,
+                                                          unsigned long long* __restrict__ keys,
+                                                          const int* __restrict__ slot_inst,
+                                                          int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
+                                                          const uint16_t* __restrict__ slot_mask,
+                                                          uint16_t* __restrict__ sorted_mask) {
+    int npow = 64;
+    while (npow < n) npow <<= 1;
+    const unsigned long long gmask = (1ull << (32 - slot_bits)) - 1ull, smask = (1ull << slot_bits) - 1ull;
+    for (int i = threadIdx.x; i < npow; i += blockDim.x) {
+        const unsigned long long k = i < n ? keys[s0 + i] : 0ull;
+        s_keys[i] = i < n ? ((k & 0xffffffff00000000ull) | ((k & gmask) << slot_bits) | (unsigned long long)i)
+                          : SORT_PAD_KEY;
+    }
+    __syncthreads();
+    block_sort_smem<false>(s_keys, nullptr, npow, n);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const unsigned long long k = s_keys[i];
+        const int slot = (int)(k & smask);
+        const uint32_t g = (uint32_t)((k >> slot_bits) & gmask);
+        sorted_gid[s0 + i] = (int)g;
+        sorted_inst[s0 + i] = slot_inst[s0 + slot];
+        if (sorted_mask) sorted_mask[s0 + i] = slot_mask[s0 + slot];
+        keys[s0 + i] = (k & 0xffffffff00000000ull) | g;
+    }
+}
 
 // Orders bucket t (n keys at s0) in shared memory of capacity `cap` (a power of two >= n)
 // and writes the sorted Gaussian indices, instance ids and keys; `packed`: every element index
@@ -351,27 +388,12 @@ static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_ke
                                                         int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
                                                         const uint16_t* __restrict__ slot_mask,
                                                         uint16_t* __restrict__ sorted_mask, bool packed) {
-    int npow = 64;
-    while (npow < n) npow <<= 1;
     if (packed && n <= SORT_SMEM_CAP) {
-        for (int i = threadIdx.x; i < npow; i += blockDim.x) {
-            const unsigned long long k = i < n ? keys[s0 + i] : 0ull;
-            s_keys[i] = i < n ? ((k & 0xffffffff00000000ull) | ((k & 0xfffffull) << 12) | (unsigned long long)i)
-                              : SORT_PAD_KEY;
-        }
-        __syncthreads();
-        block_sort_smem<false>(s_keys, nullptr, npow, n);
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const unsigned long long k = s_keys[i];
-            const int slot = (int)(k & 0xfffull);
-            const uint32_t g = (uint32_t)((k >> 12) & 0xfffffull);
-            sorted_gid[s0 + i] = (int)g;
-            sorted_inst[s0 + i] = slot_inst[s0 + slot];
-            if (sorted_mask) sorted_mask[s0 + i] = slot_mask[s0 + slot];
-            keys[s0 + i] = (k & 0xffffffff00000000ull) | g;
-        }
+        sort_bucket_packed(s_keys, s0, n, 12, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
         return;
     }
+    int npow = 64;
+    while (npow < n) npow <<= 1;
     for (int i = threadIdx.x; i < npow; i += blockDim.x) {
         s_keys[i] = i < n ? keys[s0 + i] : SORT_PAD_KEY;
         s_idx[i] = i;
@@ -430,11 +452,34 @@ tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long*
 constexpr int SORT_BIG_GRID = 148;      // one 192 KB block per SM
 constexpr int SORT_BIG_THREADS = 1024;  // the whole SM's threads on one large bucket
 
+// Buckets of SORT_SMEM_CAP < n <= SORT_MID_CAP keys of a call whose element indices fit the
+// 13-bit-slot packing: block b orders tiles b, b + grid, ... with 64 KB of shared memory
+// (three blocks per SM, so that a small image's few large buckets run side by side).
+constexpr int SORT_MID_GRID = 3 * 148;
+constexpr int SORT_MID_THREADS = 512;
+
+static __global__ void __launch_bounds__(SORT_MID_THREADS)
+tile_sort_mid_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
+                     unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
+                     int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
+                     const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask) {
+    extern __shared__ __align__(16) unsigned long long s_mid_keys[];
+    if (header[H_FLAGS] != 0) return;
+    for (int64_t t = blockIdx.x; t < T; t += gridDim.x) {
+        const int s0 = tile_start[t];
+        const int n = tile_start[t + 1] - s0;
+        if (n <= SORT_SMEM_CAP || n > SORT_MID_CAP) continue;  // the same for the whole block
+        sort_bucket_packed(s_mid_keys, s0, n, SORT_MID_SLOT_BITS, keys, slot_inst, sorted_gid, sorted_inst,
+                           slot_mask, sorted_mask);
+        __syncthreads();
+    }
+}
+
 static __global__ void __launch_bounds__(SORT_BIG_THREADS)
 tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
                      unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
                      int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
-                     const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask) {
+                     const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask, int mid) {
     extern __shared__ __align__(16) unsigned long long s_big_keys[];
     int* s_big_idx = reinterpret_cast<int*>(s_big_keys + SORT_BIG_CAP);
     __shared__ int s_list[SORT_BIG_THREADS];
@@ -447,7 +492,8 @@ tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long l
         const int64_t t = c0 + blockIdx.x + stride * threadIdx.x;
         if (t < T) {
             const int n = tile_start[t + 1] - tile_start[t];
-            if (n > SORT_SMEM_CAP && n <= SORT_BIG_CAP) s_list[atomicAdd(&s_n, 1)] = threadIdx.x;
+            if (n > SORT_SMEM_CAP && n <= SORT_BIG_CAP && !(mid && n <= SORT_MID_CAP))
+                s_list[atomicAdd(&s_n, 1)] = threadIdx.x;
         }
         __syncthreads();
         const int count = s_n;
@@ -463,6 +509,8 @@ tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long l
 }
 
 static inline size_t tile_sort_big_smem_bytes() { return SORT_BIG_CAP * (sizeof(unsigned long long) + sizeof(int)); }
+static inline size_t tile_sort_mid_smem_bytes() { return SORT_MID_CAP * sizeof(unsigned long long); }
+static inline bool tile_sort_mid(int64_t n_elems) { return n_elems < SORT_PACK_G_MID; }
 
 // Launches the tile sort on `stream` for keys whose low word indexes one of n_elems elements:
 // the shared-memory pass over all T tiles and, for large
@@ -487,15 +535,26 @@ static inline cudaError_t launch_tile_sort(int64_t T, int64_t n_elems, const int
         e = cudaFuncSetAttribute(tile_sort_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)tile_sort_big_smem_bytes());
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(tile_sort_mid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_sort_mid_smem_bytes());
+        if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 128) attr_done[dev] = true;
+    }
+    const bool mid = tile_sort_mid(n_elems);
+    if (mid) {
+        const unsigned mgrid = (unsigned)(T < SORT_MID_GRID ? T : SORT_MID_GRID);
+        tile_sort_mid_kernel<<<mgrid, SORT_MID_THREADS, tile_sort_mid_smem_bytes(), stream>>>(
+            T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
     }
     const unsigned grid = (unsigned)(T < SORT_BIG_GRID ? T : SORT_BIG_GRID);
     tile_sort_big_kernel<<<grid, SORT_BIG_THREADS, tile_sort_big_smem_bytes(), stream>>>(
-        T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
+        T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask, mid ? 1 : 0);
     return cudaGetLastError();
 }
 
-// Kernel launches launch_tile_sort makes for T > 0 tiles.
-constexpr int TILE_SORT_LAUNCHES = 2;
+// Kernel launches launch_tile_sort makes for T > 0 tiles over n_elems elements.
+static inline int tile_sort_launches(int64_t n_elems) { return 2 + (tile_sort_mid(n_elems) ? 1 : 0); }
 
 }  // namespace us3d

@@ -1078,7 +1078,7 @@ extern "C" int us3d_gp_forward(void* workspace, size_t workspace_bytes, int64_t 
         split4 ? launch(forward_kernel<1, 4>, 1, 4) : launch(forward_kernel<1, 1>, 1, 1);
     US3D_CHECK_LAUNCH("gp forward");
     prof_end(prof, stream);
-    count_launches(1 + (n_gauss > 0) * 3 + 6 + 1 + TILE_SORT_LAUNCHES + 1);
+    count_launches(1 + (n_gauss > 0) * 3 + 6 + 1 + tile_sort_launches(n_gauss) + 1);
     return US3D_OK;
 }
 

@@ -459,7 +459,7 @@ extern "C" int us3d_sa_bounded_forward(void* workspace, size_t workspace_bytes, 
                                                             out_image, out_alpha);
     US3D_CHECK_LAUNCH("sa forward");
     prof_end(prof, stream);
-    count_launches(1 + 3 * (n > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
+    count_launches(1 + 3 * (n > 0) + 6 + 1 + tile_sort_launches(n) + 1);
     return US3D_OK;
 }
 

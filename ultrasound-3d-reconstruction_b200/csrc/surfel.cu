@@ -1072,7 +1072,7 @@ extern "C" int us3d_gs_forward(void* workspace, size_t workspace_bytes, int64_t 
                                                       background, out_color, out_others, w.accum, w.n_contrib);
     US3D_CHECK_LAUNCH("gs forward");
     prof_end(prof, stream);
-    count_launches(1 + 3 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1);
+    count_launches(1 + 3 * (n_gauss > 0) + 6 + 1 + tile_sort_launches(n_gauss) + 1);
     return US3D_OK;
 }
 

@@ -1747,7 +1747,7 @@ int us3d::ug::bin_with_task_capacity(void* workspace, size_t workspace_bytes, co
     }
     prof_end(prof, stream);
     count_launches(1 + (n_frames > 0) + (slice_cull && n_tiles > 0) + 4 * (n_gauss > 0) + 9 + 3 + (n_gauss > 0) +
-                   (1 + TILE_SORT_LAUNCHES) * (n_tiles > 0));
+                   (1 + tile_sort_launches(n_gauss)) * (n_tiles > 0));
     return US3D_OK;
 }
 

@@ -1137,7 +1137,7 @@ extern "C" int us3d_ugr_forward(void* workspace, size_t workspace_bytes, int64_t
                                      g_ugr_sort_attr, stream));
     const unsigned tiles_y = (unsigned)((H + FWD_SAMPLES - 1) / FWD_SAMPLES);
     const int* ckpt_rays = nullptr;
-    int launches = 1 + 3 * (n_gauss > 0) + 6 + 1 + TILE_SORT_LAUNCHES + 1;
+    int launches = 1 + 3 * (n_gauss > 0) + 6 + 1 + tile_sort_launches(n_gauss) + 1;
     if (uses_checkpoints(H, quadrature_window_radius_mm, local_window_only)) {
         const unsigned by = per_ray_blocks(W);
         ray_depth_kernel<<<(unsigned)W, 256, 0, stream>>>(W, H, w.header, pixel_positions, ray_origins, ray_dirs,
