@@ -46,7 +46,7 @@ BP, BG, BO, BD = 44, 44, 12, 12  # algorithmic bytes per Gaussian / pixel (param
 # A variant without a capture has no entry and reports no issue figure.
 NCU_STAGE = {
     "ug_forward": {
-        0: dict(traffic=(52.274432e6 + 5.454592e6) / 4, inst=(547342384 / 4, 0.0), fma=0.5172),
+        0: dict(traffic=(52.290304e6 + 4.972288e6) / 4, inst=(466223281 / 4, 0.0), fma=0.5092),
         1: dict(traffic=(52.252416e6 + 4.260352e6) / 4, inst=(487111780 / 4, 0.0), fma=0.5661),
     },
     "ug_backward": {
