@@ -417,12 +417,25 @@ __device__ __forceinline__ bool intersect(float pxf, float pyf, const float4 r0,
     return !(h.depth < NEAR_N);
 }
 
+// Asynchronous global -> shared copies (cp.async, sm_80 and later): the next batch of render
+// records is gathered into the second staging buffer while the current one is shaded.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 __global__ void __launch_bounds__(BLOCK)
 forward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
                const long long* __restrict__ header, const float4* __restrict__ rec, const float* __restrict__ bg,
                float* __restrict__ out_color, float* __restrict__ out_others, float* __restrict__ accum,
                uint32_t* __restrict__ n_contrib) {
-    __shared__ float4 s_rec[REC_F4][BLOCK];
+    __shared__ float4 s_rec[2][REC_F4][BLOCK];  // double-buffered staging
     if (header[H_FLAGS] != 0) return;
     const int tile = blockIdx.x;
     const int tx = tile % gx, ty = tile / gx;
@@ -440,19 +453,28 @@ forward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const i
     float N[3] = {0.f, 0.f, 0.f};
     float D = 0.f, M1 = 0.f, M2 = 0.f, distortion = 0.f, median_depth = 0.f, median_contributor = -1.f;
     const float mscale = FAR_N / (FAR_N - NEAR_N);
-    for (int i = 0; i < rounds; ++i, todo -= BLOCK) {
-        if (__syncthreads_count(done) == BLOCK) break;
+    // round i's records go to buffer i & 1; the copies of round i + 1 are issued once every
+    // thread has passed round i's barrier (so nobody still reads that buffer from round i - 1)
+    // and run while round i is shaded
+    auto stage = [&](int i) {
         const int prog = i * BLOCK + threadIdx.x;
         if (prog < n) {
             const float4* r = rec + (int64_t)REC_F4 * sorted_gid[s0 + prog];
 #pragma unroll
-            for (int f = 0; f < REC_F4; ++f) s_rec[f][threadIdx.x] = r[f];
+            for (int f = 0; f < REC_F4; ++f) cp_async16(&s_rec[i & 1][f][threadIdx.x], r + f);
         }
-        __syncthreads();
+        cp_async_commit();
+    };
+    if (rounds > 0) stage(0);
+    for (int i = 0; i < rounds; ++i, todo -= BLOCK) {
+        cp_async_wait_all();  // this thread's copies of round i have landed
+        if (__syncthreads_count(done) == BLOCK) break;  // ... and everyone's; no copy is in flight
+        if (i + 1 < rounds) stage(i + 1);
+        const float4(*sr)[BLOCK] = s_rec[i & 1];
         const int nb = min(BLOCK, todo);
         for (int j = 0; !done && j < nb; ++j) {
             ++contributor;
-            const float4 r0 = s_rec[0][j], r1 = s_rec[1][j], r2 = s_rec[2][j];
+            const float4 r0 = sr[0][j], r1 = sr[1][j], r2 = sr[2][j];
             Hit h;
             if (!intersect(pxf, pyf, r0, r1, r2, h)) continue;
             const float rho = fminf(h.rho3d, h.rho2d);
@@ -476,7 +498,7 @@ forward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const i
                 median_depth = h.depth;
                 median_contributor = (float)contributor;
             }
-            const float4 r3 = s_rec[3][j], r4 = s_rec[4][j];
+            const float4 r3 = sr[3][j], r4 = sr[4][j];
             N[0] += r3.x * w;
             N[1] += r3.y * w;
             N[2] += r3.z * w;
@@ -556,8 +578,8 @@ backward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const 
                 const float4* __restrict__ rec, const float* __restrict__ bg, const float* __restrict__ accum,
                 const uint32_t* __restrict__ n_contrib, const float* __restrict__ dL_dpix,
                 const float* __restrict__ dL_dothers, float4* __restrict__ partial) {
-    __shared__ float4 s_rec[REC_F4][BWD_BATCH];
-    __shared__ int s_inst[BWD_BATCH];
+    __shared__ float4 s_rec[2][REC_F4][BWD_BATCH];  // double-buffered staging
+    __shared__ int s_inst[2][BWD_BATCH];
     __shared__ float s_red[BWD_BATCH][BLOCK / 32][NGRAD];
     __shared__ int s_last;
     if (header[H_FLAGS] != 0) return;
@@ -613,17 +635,27 @@ backward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const 
     const float bg_dot_dpixel = bg[0] * dpix[0] + bg[1] * dpix[1] + bg[2] * dpix[2];
     const float mscale = FAR_N / (FAR_N - NEAR_N);
 
-    for (int b0 = 0; b0 < n_live; b0 += BWD_BATCH) {
+    // batch k (staged from the back of the tile list's live part) goes to buffer k & 1; the
+    // copies of batch k + 1 are issued after batch k's first barrier (every thread is then done
+    // with that buffer's previous batch) and run while batch k is replayed
+    auto stage = [&](int b0, int buf) {
         const int nb = min(BWD_BATCH, n_live - b0);
-        __syncthreads();
-        // stage from the back of the tile list's live part
         for (int q = threadIdx.x; q < nb * REC_F4; q += BLOCK) {
             const int jj = q / REC_F4, f = q - jj * REC_F4;
             const int slot = s0 + n_live - 1 - (b0 + jj);
-            s_rec[f][jj] = rec[(int64_t)REC_F4 * sorted_gid[slot] + f];
-            if (f == 0) s_inst[jj] = sorted_inst[slot];
+            cp_async16(&s_rec[buf][f][jj], rec + (int64_t)REC_F4 * sorted_gid[slot] + f);
+            if (f == 0) cp_async4(&s_inst[buf][jj], sorted_inst + slot);
         }
-        __syncthreads();
+        cp_async_commit();
+    };
+    if (n_live > 0) stage(0, 0);
+    for (int b0 = 0, k = 0; b0 < n_live; b0 += BWD_BATCH, ++k) {
+        const int nb = min(BWD_BATCH, n_live - b0);
+        cp_async_wait_all();  // this thread's copies of batch k have landed
+        __syncthreads();      // ... and everyone's; the previous batch's partials are written
+        if (b0 + BWD_BATCH < n_live) stage(b0 + BWD_BATCH, (k + 1) & 1);
+        const float4(*sr)[BWD_BATCH] = s_rec[k & 1];
+        const int* si = s_inst[k & 1];
         for (int jj = 0; jj < nb; ++jj) {
             float v[24];
 #pragma unroll
@@ -632,7 +664,7 @@ backward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const 
             if (inside) {
                 --contributor;
                 if (contributor < (uint32_t)last_contributor) {
-                    const float4 r0 = s_rec[0][jj], r1 = s_rec[1][jj], r2 = s_rec[2][jj];
+                    const float4 r0 = sr[0][jj], r1 = sr[1][jj], r2 = sr[2][jj];
                     Hit h;
                     const bool hit = intersect(pxf, pyf, r0, r1, r2, h);
                     float G = 0.f, alpha = 0.f;
@@ -649,7 +681,7 @@ backward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const 
                     }
                     if (ok) {
                         contrib = true;
-                        const float4 r3 = s_rec[3][jj], r4 = s_rec[4][jj];
+                        const float4 r3 = sr[3][jj], r4 = sr[4][jj];
                         const float col[3] = {r3.w, r4.x, r4.y};
                         const float nrm[3] = {r3.x, r3.y, r3.z};
                         T = T / (1.f - alpha);
@@ -740,7 +772,7 @@ backward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const 
             }
             s[18] = 0.f;
             s[19] = 0.f;
-            float4* out = partial + (int64_t)PARTIAL_F4 * s_inst[jj];
+            float4* out = partial + (int64_t)PARTIAL_F4 * si[jj];
 #pragma unroll
             for (int f = 0; f < PARTIAL_F4; ++f) out[f] = make_float4(s[4 * f], s[4 * f + 1], s[4 * f + 2], s[4 * f + 3]);
         }
