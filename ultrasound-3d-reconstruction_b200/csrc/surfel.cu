@@ -635,25 +635,39 @@ backward_kernel(int W, int H, int gx, const int* __restrict__ tile_start, const 
     const float bg_dot_dpixel = bg[0] * dpix[0] + bg[1] * dpix[1] + bg[2] * dpix[2];
     const float mscale = FAR_N / (FAR_N - NEAR_N);
 
-    // batch k (staged from the back of the tile list's live part) goes to buffer k & 1; the
-    // copies of batch k + 1 are issued after batch k's first barrier (every thread is then done
-    // with that buffer's previous batch) and run while batch k is replayed
-    auto stage = [&](int b0, int buf) {
-        const int nb = min(BWD_BATCH, n_live - b0);
-        for (int q = threadIdx.x; q < nb * REC_F4; q += BLOCK) {
-            const int jj = q / REC_F4, f = q - jj * REC_F4;
-            const int slot = s0 + n_live - 1 - (b0 + jj);
-            cp_async16(&s_rec[buf][f][jj], rec + (int64_t)REC_F4 * sorted_gid[slot] + f);
-            if (f == 0) cp_async4(&s_inst[buf][jj], sorted_inst + slot);
+    // batch k (staged from the back of the tile list's live part) goes to buffer k & 1: thread
+    // jj < BWD_BATCH copies Gaussian jj's record and instance id. The copies of batch k + 1 are
+    // issued after batch k's first barrier (every thread is then done with that buffer's
+    // previous batch) and run while batch k is replayed; the Gaussian index each copy needs is
+    // read one batch earlier still, so no thread waits on it.
+    static_assert(BWD_BATCH <= BLOCK, "one staging thread per batch entry");
+    auto load_gid = [&](int b0) {
+        const int jj = threadIdx.x;
+        return (jj < BWD_BATCH && b0 + jj < n_live) ? sorted_gid[s0 + n_live - 1 - (b0 + jj)] : -1;
+    };
+    auto stage = [&](int b0, int buf, int gid) {
+        const int jj = threadIdx.x;
+        if (gid >= 0) {
+            const float4* r = rec + (int64_t)REC_F4 * gid;
+#pragma unroll
+            for (int f = 0; f < REC_F4; ++f) cp_async16(&s_rec[buf][f][jj], r + f);
+            cp_async4(&s_inst[buf][jj], sorted_inst + (s0 + n_live - 1 - (b0 + jj)));
         }
         cp_async_commit();
     };
-    if (n_live > 0) stage(0, 0);
+    int gid_next = 0;
+    if (n_live > 0) {
+        stage(0, 0, load_gid(0));
+        gid_next = load_gid(BWD_BATCH);
+    }
     for (int b0 = 0, k = 0; b0 < n_live; b0 += BWD_BATCH, ++k) {
         const int nb = min(BWD_BATCH, n_live - b0);
         cp_async_wait_all();  // this thread's copies of batch k have landed
         __syncthreads();      // ... and everyone's; the previous batch's partials are written
-        if (b0 + BWD_BATCH < n_live) stage(b0 + BWD_BATCH, (k + 1) & 1);
+        if (b0 + BWD_BATCH < n_live) {
+            stage(b0 + BWD_BATCH, (k + 1) & 1, gid_next);
+            gid_next = load_gid(b0 + 2 * BWD_BATCH);
+        }
         const float4(*sr)[BWD_BATCH] = s_rec[k & 1];
         const int* si = s_inst[k & 1];
         for (int jj = 0; jj < nb; ++jj) {
