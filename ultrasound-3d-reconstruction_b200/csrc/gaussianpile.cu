@@ -517,15 +517,24 @@ backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restric
     const float weight_min = params[UF_WEIGHT_MIN];
     const float lat_delta = grid[SG_DELTA_LAT_MM], ax_delta = grid[SG_DELTA_AX_MM];
     const float col_off = grid[SG_LAT_COL_OFFSET], near_mm = grid[SG_NEAR_MM];
-    for (int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < total;
-         k += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        // the instance's tile: the last t with tile_start[t] <= k (empty tiles share a start)
+    // Each warp owns a contiguous run of instances, so the instance's tile (the last t with
+    // tile_start[t] <= k; empty tiles share a start) is found by one binary search per warp and
+    // then followed forward as k advances.
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t chunk = (total + n_warps - 1) / n_warps;
+    const int64_t k_begin = wid * chunk, k_end = min(total, k_begin + chunk);
+    int t = 0;
+    if (k_begin < k_end) {
         int lo = 0, hi = T;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (tile_start[mid] <= k) lo = mid; else hi = mid;
+            if (tile_start[mid] <= k_begin) lo = mid; else hi = mid;
         }
-        const int t = lo;
+        t = lo;
+    }
+    for (int64_t k = k_begin; k < k_end; ++k) {
+        while (t + 1 < T && tile_start[t + 1] <= k) ++t;
         const int tx = t % tiles_x, ty = t / tiles_x;
         const int x0 = tx * tile, y0 = ty * tile;
         const int x1 = min(W, (tx + 1) * tile), y1 = min(H, (ty + 1) * tile);
