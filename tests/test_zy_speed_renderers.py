@@ -30,16 +30,23 @@ def _ref(name):
     return __import__(name)
 
 
-def _time(fn, reps):
-    fn()
+def _time(fn, reps, trials=5):
+    """Median over ``trials`` of the mean CUDA-event time of ``reps`` calls, after three
+    warm-up calls (the first calls size workspaces and caches; a trial that catches a clock
+    ramp or another process's burst does not decide the figure)."""
+    for _ in range(3):
+        fn()
     torch.cuda.synchronize()
     st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    st.record()
-    for _ in range(reps):
-        fn()
-    en.record()
-    torch.cuda.synchronize()
-    return st.elapsed_time(en) / reps
+    out = []
+    for _ in range(trials):
+        st.record()
+        for _ in range(reps):
+            fn()
+        en.record()
+        torch.cuda.synchronize()
+        out.append(st.elapsed_time(en) / reps)
+    return sorted(out)[len(out) // 2]
 
 
 def _report(name, what, ms_ref, ms_ours):
