@@ -12,8 +12,9 @@ constexpr int SORT_THREADS = 512;
 // Tiles of up to SORT_SMEM_CAP keys are ordered in shared memory by the first sort pass
 // (48 KB, four 512-thread blocks per SM); up to SORT_MID_CAP keys, when every element index of
 // the call fits a 13-bit slot packing, by a pass with 64 KB (three blocks per SM); larger ones,
-// up to SORT_BIG_CAP, by a pass with 192 KB (one block per SM); beyond that the network runs on
-// global memory (one block per tile).
+// up to SORT_BIG_CAP, by a pass with 192 KB (one block per SM); up to SORT_HUGE_CAP, when the
+// bucket's keys pack into 64-bit words, by a pass with 224 KB (one block per SM); beyond that
+// the network runs on global memory (one block per tile).
 constexpr int SORT_SMEM_CAP = 4096;
 constexpr int SORT_BIG_CAP = 16384;
 constexpr int SORT_MIN_BLOCKS = 4;
@@ -409,6 +410,80 @@ static __device__ __forceinline__ void sort_bucket_smem(unsigned long long* s_ke
     }
 }
 
+// A bucket too large for any shared-memory pass: the network directly on global memory (the
+// calling block owns the bucket), with the slot indices as payload in sorted_inst.
+static __device__ void sort_bucket_global(int s0, int n, unsigned long long* __restrict__ keys,
+                                          const int* __restrict__ slot_inst, int* __restrict__ sorted_gid,
+                                          int* __restrict__ sorted_inst, const uint16_t* __restrict__ slot_mask,
+                                          uint16_t* __restrict__ sorted_mask) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sorted_inst[s0 + i] = i;
+    __syncthreads();
+    bitonic_sort(keys + s0, sorted_inst + s0, n);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int slot = sorted_inst[s0 + i];
+        sorted_gid[s0 + i] = (int)(uint32_t)(keys[s0 + i] & 0xffffffffull);
+        sorted_inst[s0 + i] = slot_inst[s0 + slot];
+        if (sorted_mask) sorted_mask[s0 + i] = slot_mask[s0 + slot];
+    }
+}
+
+// Buckets of SORT_BIG_CAP < n <= SORT_HUGE_CAP keys: when the call's element indices need
+// gbits bits and every depth key of the bucket is below 2^(64 - gbits - 15), the key
+// (hi << 32 | g) is packed as (hi << (gbits + 15) | g << 15 | slot) -- same order, slot in the
+// low 15 bits -- and the bucket sorts in 224 KB of shared memory (the network touches only the
+// first ceil(n / 64) * 64 entries); otherwise the global-memory network orders it.
+constexpr int SORT_HUGE_CAP = 28672;
+constexpr int SORT_HUGE_SLOT_BITS = 15;
+constexpr int SORT_HUGE_GRID = 148;       // one 224 KB block per SM
+constexpr int SORT_HUGE_THREADS = 1024;
+
+static __global__ void __launch_bounds__(SORT_HUGE_THREADS)
+tile_sort_huge_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
+                      unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
+                      int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
+                      const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask, int gbits) {
+    extern __shared__ __align__(16) unsigned long long s_huge[];
+    __shared__ int s_fits;
+    if (header[H_FLAGS] != 0) return;
+    const int sb = SORT_HUGE_SLOT_BITS, hi_bits = 64 - gbits - SORT_HUGE_SLOT_BITS;
+    const unsigned long long gmask = (1ull << gbits) - 1ull, smask = (1ull << sb) - 1ull;
+    for (int64_t t = blockIdx.x; t < T; t += gridDim.x) {
+        const int s0 = tile_start[t];
+        const int n = tile_start[t + 1] - s0;
+        if (n <= SORT_BIG_CAP || n > SORT_HUGE_CAP) continue;  // the same for the whole block
+        if (threadIdx.x == 0) s_fits = 1;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            if ((keys[s0 + i] >> 32) >> hi_bits) s_fits = 0;
+        __syncthreads();
+        if (!s_fits) {
+            sort_bucket_global(s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
+            __syncthreads();
+            continue;
+        }
+        int npow = 64;
+        while (npow < n) npow <<= 1;
+        const int nfill = (n + 63) & ~63;
+        for (int i = threadIdx.x; i < nfill; i += blockDim.x) {
+            const unsigned long long k = i < n ? keys[s0 + i] : 0ull;
+            s_huge[i] = i < n ? (((k >> 32) << (gbits + sb)) | ((k & gmask) << sb) | (unsigned long long)i)
+                              : SORT_PAD_KEY;
+        }
+        __syncthreads();
+        block_sort_smem<false>(s_huge, nullptr, npow, n);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned long long k = s_huge[i];
+            const int slot = (int)(k & smask);
+            const uint32_t g = (uint32_t)((k >> sb) & gmask);
+            sorted_gid[s0 + i] = (int)g;
+            sorted_inst[s0 + i] = slot_inst[s0 + slot];
+            if (sorted_mask) sorted_mask[s0 + i] = slot_mask[s0 + slot];
+            keys[s0 + i] = ((k >> (gbits + sb)) << 32) | g;
+        }
+        __syncthreads();
+    }
+}
+
 // One block per tile: order the tile's bucket by (depth key, Gaussian index), which is the
 // order the reference's stable radix sort of (tile << 32 | depth key) over instances
 // enumerated Gaussian by Gaussian produces (src/mapper/wrapper_mapper.cu:134-146). Keys
@@ -430,18 +505,8 @@ tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long*
     if (n <= SORT_SMEM_CAP) {
         sort_bucket_smem(s_keys, s_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask,
                          packed != 0);
-    } else if (n > SORT_BIG_CAP) {
-        // Oversized bucket: the network directly on global memory (one block owns it), with
-        // the slot indices as payload in sorted_inst.
-        for (int i = threadIdx.x; i < n; i += blockDim.x) sorted_inst[s0 + i] = i;
-        __syncthreads();
-        bitonic_sort(keys + s0, sorted_inst + s0, n);
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int slot = sorted_inst[s0 + i];
-            sorted_gid[s0 + i] = (int)(uint32_t)(keys[s0 + i] & 0xffffffffull);
-            sorted_inst[s0 + i] = slot_inst[s0 + slot];
-            if (sorted_mask) sorted_mask[s0 + i] = slot_mask[s0 + slot];
-        }
+    } else if (n > SORT_HUGE_CAP) {
+        sort_bucket_global(s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
     }
 }
 
@@ -510,6 +575,13 @@ tile_sort_big_kernel(int64_t T, const int* __restrict__ tile_start, const long l
 
 static inline size_t tile_sort_big_smem_bytes() { return SORT_BIG_CAP * (sizeof(unsigned long long) + sizeof(int)); }
 static inline size_t tile_sort_mid_smem_bytes() { return SORT_MID_CAP * sizeof(unsigned long long); }
+static inline size_t tile_sort_huge_smem_bytes() { return SORT_HUGE_CAP * sizeof(unsigned long long); }
+// Bits of the largest element index of a call (at least 1).
+static inline int tile_sort_gbits(int64_t n_elems) {
+    int b = 1;
+    while (b < 31 && (int64_t(1) << b) < n_elems) ++b;
+    return b;
+}
 static inline bool tile_sort_mid(int64_t n_elems) { return n_elems < SORT_PACK_G_MID; }
 
 // Launches the tile sort on `stream` for keys whose low word indexes one of n_elems elements:
@@ -538,6 +610,9 @@ static inline cudaError_t launch_tile_sort(int64_t T, int64_t n_elems, const int
         e = cudaFuncSetAttribute(tile_sort_mid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)tile_sort_mid_smem_bytes());
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(tile_sort_huge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_sort_huge_smem_bytes());
+        if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 128) attr_done[dev] = true;
     }
     const bool mid = tile_sort_mid(n_elems);
@@ -551,10 +626,16 @@ static inline cudaError_t launch_tile_sort(int64_t T, int64_t n_elems, const int
     const unsigned grid = (unsigned)(T < SORT_BIG_GRID ? T : SORT_BIG_GRID);
     tile_sort_big_kernel<<<grid, SORT_BIG_THREADS, tile_sort_big_smem_bytes(), stream>>>(
         T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask, mid ? 1 : 0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const unsigned hgrid = (unsigned)(T < SORT_HUGE_GRID ? T : SORT_HUGE_GRID);
+    tile_sort_huge_kernel<<<hgrid, SORT_HUGE_THREADS, tile_sort_huge_smem_bytes(), stream>>>(
+        T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask,
+        tile_sort_gbits(n_elems));
     return cudaGetLastError();
 }
 
 // Kernel launches launch_tile_sort makes for T > 0 tiles over n_elems elements.
-static inline int tile_sort_launches(int64_t n_elems) { return 2 + (tile_sort_mid(n_elems) ? 1 : 0); }
+static inline int tile_sort_launches(int64_t n_elems) { return 3 + (tile_sort_mid(n_elems) ? 1 : 0); }
 
 }  // namespace us3d
