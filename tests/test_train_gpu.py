@@ -261,3 +261,50 @@ def test_trainer_with_refinement(cuda_device):
     for t in params.tensors():
         assert torch.isfinite(t).all()
     assert torch.isfinite(tr.losses(0)).all()
+
+
+def test_trainer_checkpoint_resume_bit_identical(cuda_device, tmp_path):
+    """A run saved after a refinement and resumed in a fresh trainer (from the initial
+    parameters, so the loaded state has another number of Gaussians) takes the same steps bit
+    for bit as the uninterrupted run: parameters, Adam moments, step count, refinement
+    statistics and log, and the generators of the batch draws and of the refinement."""
+    from us3d_b200 import scenes
+    from us3d_b200.frames import DeviceFrameSource
+    from us3d_b200.refine import RefineConfig
+    from us3d_b200.train import TrainConfig, UltraGaussParameters, UltraGaussTrainer
+
+    dev = cuda_device
+    rng = np.random.default_rng(3)
+    n, h, w = 6, 64, 80
+    images = rng.integers(0, 255, (n, h, w), dtype=np.uint8)
+    origin = np.stack([np.array([4.0 + 2.5 * k, 2.0, 16.0], np.float32) for k in range(n)])
+    src = DeviceFrameSource(images, origin, np.array([0, 0, 1], np.float32), np.array([0, 1, 0], np.float32),
+                            np.array([1, 0, 0], np.float32), 0.25, 0.25, device=dev)
+    sc = scenes.make_scene(12000, seed=7, cube_mm=32.0)
+    rc = RefineConfig(every=3, start=3, stop=9, grad_threshold=1e-7, split_scale_mm=0.9, max_gaussians=16000)
+
+    def fresh():
+        params = UltraGaussParameters.from_points(sc.means.to(dev), sc.intensities.to(dev), init_scale_mm=0.8)
+        return params, UltraGaussTrainer.from_source(params, src, 3, TrainConfig(lr=1e-2), refine=rc, seed=5)
+
+    pa, ta = fresh()
+    for _ in range(10):
+        ta.step(0)
+    pb, tb = fresh()
+    for _ in range(4):
+        tb.step(0)
+    tb.save(tmp_path / "ckpt.pt")
+    assert [r["step"] for r in tb.refine_log] == [3]
+    pc, tc = fresh()
+    tc.load(tmp_path / "ckpt.pt")
+    assert tc.steps_done == 4 and pc.means.shape[0] == pb.means.shape[0] != 12000
+    for _ in range(6):
+        tc.step(0)
+    ta.check()
+    tc.check()
+    assert [r["step"] for r in tc.refine_log] == [r["step"] for r in ta.refine_log] == [3, 6, 9]
+    assert tc.refine_log == ta.refine_log
+    for x, y in zip(pa.tensors(), pc.tensors()):
+        assert torch.equal(x, y)
+    for x, y in zip(ta.optimizer.exp_avg + ta.optimizer.exp_avg_sq, tc.optimizer.exp_avg + tc.optimizer.exp_avg_sq):
+        assert torch.equal(x, y)

@@ -255,6 +255,11 @@ class UltraGaussTrainer:
 
         self.refine_log.append(dict(step=self.steps_done, **refine(self.params, self.optimizer, self.refine_stats,
                                                                     self.refine_cfg, self.refine_gen)))
+        self._rebuffer()
+
+    def _rebuffer(self) -> None:
+        """New gradient buffers, graphs and instance capacities after the parameter tensors were
+        replaced (a refinement or a loaded checkpoint with another number of Gaussians)."""
         dev = self.params.means.device
         G = self.params.means.shape[0]
         self.grads = (torch.empty((G, 3), device=dev), torch.empty((G, 6), device=dev),
@@ -278,6 +283,80 @@ class UltraGaussTrainer:
                 best = max(best, prime.total)
                 worked = max(worked, int(prime.capacity))
             bt["capacity"] = max(worked, int(best * sc["margin"]) + 1024)
+
+    _PARAM_NAMES = ("means", "raw_precision_tril", "raw_opacities", "raw_intensities")
+
+    def state_dict(self) -> dict:
+        """Everything a resumed run needs, as the reference's checkpoint (config, iteration,
+        parameters, optimizer state; pipeline_god_file.py:701-724) plus the refinement
+        statistics and log and the generators of the batch draws and the refinement: a run
+        resumed from it takes the same steps, bit for bit, as the uninterrupted one."""
+        import dataclasses
+
+        opt = self.optimizer
+        sd = dict(config=dataclasses.asdict(self.cfg), iteration=self.steps_done,
+                  params={k: getattr(self.params, k).detach().clone() for k in self._PARAM_NAMES},
+                  optimizer=dict(exp_avg=[m.clone() for m in opt.exp_avg], exp_avg_sq=[v.clone() for v in opt.exp_avg_sq],
+                                 step=opt.step_count, lr=opt.lr, betas=opt.betas, eps=opt.eps),
+                  refine=None, source_generator=None)
+        if self.refine_stats is not None:
+            sd["refine"] = dict(importance=self.refine_stats.importance.clone(), visits=self.refine_stats.visits.clone(),
+                                log=[dict(r) for r in self.refine_log], generator=self.refine_gen.get_state())
+        if self.source is not None:
+            sd["source_generator"] = self.source["gen"].get_state()
+        return sd
+
+    def load_state_dict(self, sd: dict) -> None:
+        """Restores a state_dict() into this trainer (same batches / frame source and refinement
+        schedule). Parameters of the same size are copied in place (the captured graphs stay
+        valid); a different number of Gaussians replaces the buffers and captures again."""
+        dev = self.params.means.device
+        new = {k: sd["params"][k].to(dev, torch.float32) for k in self._PARAM_NAMES}
+        opt = self.optimizer
+        same = all(getattr(self.params, k).shape == new[k].shape for k in self._PARAM_NAMES)
+        if same:
+            for k in self._PARAM_NAMES:
+                getattr(self.params, k).copy_(new[k])
+            for dst, src in zip(opt.exp_avg + opt.exp_avg_sq, sd["optimizer"]["exp_avg"] + sd["optimizer"]["exp_avg_sq"]):
+                dst.copy_(src.to(dev))
+        else:
+            for k in self._PARAM_NAMES:
+                setattr(self.params, k, new[k].contiguous())
+            opt.params = self.params.tensors()
+            opt.exp_avg = [m.to(dev).contiguous() for m in sd["optimizer"]["exp_avg"]]
+            opt.exp_avg_sq = [v.to(dev).contiguous() for v in sd["optimizer"]["exp_avg_sq"]]
+        opt.step_count = int(sd["optimizer"]["step"])
+        self.steps_done = int(sd["iteration"])
+        if sd.get("refine") is not None and self.refine_stats is not None:
+            from .refine import RefineStats
+
+            r = sd["refine"]
+            if not same:
+                self.refine_stats = RefineStats(new["means"].shape[0], dev)
+            self.refine_stats.importance.copy_(r["importance"].to(dev))
+            self.refine_stats.visits.copy_(r["visits"].to(dev))
+            self.refine_log = [dict(x) for x in r["log"]]
+            self.refine_gen.set_state(r["generator"])
+        if not same:
+            self._rebuffer()  # primes the capacity with draws of its own: before the states below
+        if sd.get("source_generator") is not None and self.source is not None:
+            self.source["gen"].set_state(sd["source_generator"])
+
+    def save(self, path) -> None:
+        """torch.save of state_dict() (tensors moved to the host)."""
+        def host(x):
+            if torch.is_tensor(x):
+                return x.cpu()
+            if isinstance(x, dict):
+                return {k: host(v) for k, v in x.items()}
+            if isinstance(x, (list, tuple)):
+                return type(x)(host(v) for v in x)
+            return x
+
+        torch.save(host(self.state_dict()), path)
+
+    def load(self, path) -> None:
+        self.load_state_dict(torch.load(path, map_location="cpu", weights_only=False))
 
     def losses(self, batch_index: int = 0) -> torch.Tensor:
         return self._batches[batch_index]["stats"].cpu()
