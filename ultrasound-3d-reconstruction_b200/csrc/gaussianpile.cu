@@ -601,18 +601,36 @@ backward_inst_kernel(int T, int W, int tile, int tiles_x, const float* __restric
                 myy += uy * dax;
             }
         }
-        // butterfly reduction: every lane ends with the same sums
+        // Transposed warp reduction of the nine sums (padded to 16): each exchange halves the
+        // values a lane carries, so after four exchanges lanes 2j and 2j + 1 hold partial sums
+        // of value j over 16 lanes, the fifth completes them, and every lane then reads the
+        // nine totals from lanes 0, 2, ..., 16 (25 shuffles instead of 45; fixed order).
+        {
+            const unsigned FULL = 0xffffffffu;
+            const float v[16] = {m0, sl, sa, sll, sla, saa, mxx, mxy, myy, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float a8[8], b4[4], c2[2];
+            const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4, h2 = lane & 2;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            m0 += __shfl_xor_sync(0xffffffffu, m0, off);
-            sl += __shfl_xor_sync(0xffffffffu, sl, off);
-            sa += __shfl_xor_sync(0xffffffffu, sa, off);
-            sll += __shfl_xor_sync(0xffffffffu, sll, off);
-            sla += __shfl_xor_sync(0xffffffffu, sla, off);
-            saa += __shfl_xor_sync(0xffffffffu, saa, off);
-            mxx += __shfl_xor_sync(0xffffffffu, mxx, off);
-            mxy += __shfl_xor_sync(0xffffffffu, mxy, off);
-            myy += __shfl_xor_sync(0xffffffffu, myy, off);
+            for (int i = 0; i < 8; ++i)
+                a8[i] = (h16 ? v[8 + i] : v[i]) + __shfl_xor_sync(FULL, h16 ? v[i] : v[8 + i], 16);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                b4[i] = (h8 ? a8[4 + i] : a8[i]) + __shfl_xor_sync(FULL, h8 ? a8[i] : a8[4 + i], 8);
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+                c2[i] = (h4 ? b4[2 + i] : b4[i]) + __shfl_xor_sync(FULL, h4 ? b4[i] : b4[2 + i], 4);
+            float d = (h2 ? c2[1] : c2[0]) + __shfl_xor_sync(FULL, h2 ? c2[0] : c2[1], 2);
+            d += __shfl_xor_sync(FULL, d, 1);
+            // value j = bits 4..1 of the lane (bit 4 selected the upper eight, bit 3 the upper four, ...)
+            m0 = __shfl_sync(FULL, d, 0);
+            sl = __shfl_sync(FULL, d, 2);
+            sa = __shfl_sync(FULL, d, 4);
+            sll = __shfl_sync(FULL, d, 6);
+            sla = __shfl_sync(FULL, d, 8);
+            saa = __shfl_sync(FULL, d, 10);
+            mxx = __shfl_sync(FULL, d, 12);
+            mxy = __shfl_sync(FULL, d, 14);
+            myy = __shfl_sync(FULL, d, 16);
         }
         // The terms of reference us_focus.cu:398-477 (per pixel: up * weight, up c bno and
         // cm = up c weight times the footprint derivatives) from the six moments.
