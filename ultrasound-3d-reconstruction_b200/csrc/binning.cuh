@@ -13,7 +13,7 @@ constexpr int SORT_THREADS = 512;
 // (48 KB, four 512-thread blocks per SM); up to SORT_MID_CAP keys, when every element index of
 // the call fits a 13-bit slot packing, by a pass with 64 KB (three blocks per SM); larger ones,
 // up to SORT_BIG_CAP, by a pass with 192 KB (one block per SM); up to SORT_HUGE_CAP, when the
-// bucket's keys pack into 64-bit words, by a pass with 224 KB (one block per SM); beyond that
+// bucket's keys pack into 64-bit words, by a pass with 222 KB (one block per SM); beyond that
 // the network runs on global memory (one block per tile).
 constexpr int SORT_SMEM_CAP = 4096;
 constexpr int SORT_BIG_CAP = 16384;
@@ -430,11 +430,11 @@ static __device__ void sort_bucket_global(int s0, int n, unsigned long long* __r
 // Buckets of SORT_BIG_CAP < n <= SORT_HUGE_CAP keys: when the call's element indices need
 // gbits bits and every depth key of the bucket is below 2^(64 - gbits - 15), the key
 // (hi << 32 | g) is packed as (hi << (gbits + 15) | g << 15 | slot) -- same order, slot in the
-// low 15 bits -- and the bucket sorts in 224 KB of shared memory (the network touches only the
+// low 15 bits -- and the bucket sorts in 222 KB of shared memory (the network touches only the
 // first ceil(n / 64) * 64 entries); otherwise the global-memory network orders it.
-constexpr int SORT_HUGE_CAP = 28672;
+constexpr int SORT_HUGE_CAP = 28416;  // 222 KB of keys + the block's static shared memory
 constexpr int SORT_HUGE_SLOT_BITS = 15;
-constexpr int SORT_HUGE_GRID = 148;       // one 224 KB block per SM
+constexpr int SORT_HUGE_GRID = 148;       // one 222 KB block per SM
 constexpr int SORT_HUGE_THREADS = 1024;
 
 static __global__ void __launch_bounds__(SORT_HUGE_THREADS)
@@ -444,13 +444,30 @@ tile_sort_huge_kernel(int64_t T, const int* __restrict__ tile_start, const long 
                       const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask, int gbits) {
     extern __shared__ __align__(16) unsigned long long s_huge[];
     __shared__ int s_fits;
+    __shared__ int s_list[SORT_HUGE_THREADS];
+    __shared__ int s_n;
     if (header[H_FLAGS] != 0) return;
     const int sb = SORT_HUGE_SLOT_BITS, hi_bits = 64 - gbits - SORT_HUGE_SLOT_BITS;
     const unsigned long long gmask = (1ull << gbits) - 1ull, smask = (1ull << sb) - 1ull;
-    for (int64_t t = blockIdx.x; t < T; t += gridDim.x) {
+    // block b owns tiles b, b + grid, ...: its threads inspect SORT_HUGE_THREADS of them at a
+    // time and the block sorts the ones in this size class, one after another
+    const int64_t stride = gridDim.x;
+    for (int64_t c0 = 0; c0 < T; c0 += stride * SORT_HUGE_THREADS) {
+      if (threadIdx.x == 0) s_n = 0;
+      __syncthreads();
+      {
+        const int64_t t = c0 + blockIdx.x + stride * threadIdx.x;
+        if (t < T) {
+            const int n = tile_start[t + 1] - tile_start[t];
+            if (n > SORT_BIG_CAP && n <= SORT_HUGE_CAP) s_list[atomicAdd(&s_n, 1)] = threadIdx.x;
+        }
+      }
+      __syncthreads();
+      const int count = s_n;
+      for (int kk = 0; kk < count; ++kk) {
+        const int64_t t = c0 + blockIdx.x + stride * s_list[kk];
         const int s0 = tile_start[t];
         const int n = tile_start[t + 1] - s0;
-        if (n <= SORT_BIG_CAP || n > SORT_HUGE_CAP) continue;  // the same for the whole block
         if (threadIdx.x == 0) s_fits = 1;
         __syncthreads();
         for (int i = threadIdx.x; i < n; i += blockDim.x)
@@ -481,6 +498,7 @@ tile_sort_huge_kernel(int64_t T, const int* __restrict__ tile_start, const long 
             keys[s0 + i] = ((k >> (gbits + sb)) << 32) | g;
         }
         __syncthreads();
+      }
     }
 }
 
@@ -529,14 +547,29 @@ tile_sort_mid_kernel(int64_t T, const int* __restrict__ tile_start, const long l
                      int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
                      const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask) {
     extern __shared__ __align__(16) unsigned long long s_mid_keys[];
+    __shared__ int s_list[SORT_MID_THREADS];
+    __shared__ int s_n;
     if (header[H_FLAGS] != 0) return;
-    for (int64_t t = blockIdx.x; t < T; t += gridDim.x) {
-        const int s0 = tile_start[t];
-        const int n = tile_start[t + 1] - s0;
-        if (n <= SORT_SMEM_CAP || n > SORT_MID_CAP) continue;  // the same for the whole block
-        sort_bucket_packed(s_mid_keys, s0, n, SORT_MID_SLOT_BITS, keys, slot_inst, sorted_gid, sorted_inst,
-                           slot_mask, sorted_mask);
+    // block b owns tiles b, b + grid, ...: its threads inspect SORT_MID_THREADS of them at a
+    // time and the block sorts the ones in this size class, one after another
+    const int64_t stride = gridDim.x;
+    for (int64_t c0 = 0; c0 < T; c0 += stride * SORT_MID_THREADS) {
+        if (threadIdx.x == 0) s_n = 0;
         __syncthreads();
+        const int64_t t = c0 + blockIdx.x + stride * threadIdx.x;
+        if (t < T) {
+            const int n = tile_start[t + 1] - tile_start[t];
+            if (n > SORT_SMEM_CAP && n <= SORT_MID_CAP) s_list[atomicAdd(&s_n, 1)] = threadIdx.x;
+        }
+        __syncthreads();
+        const int count = s_n;
+        for (int k = 0; k < count; ++k) {
+            const int64_t tt = c0 + blockIdx.x + stride * s_list[k];
+            const int s0 = tile_start[tt];
+            sort_bucket_packed(s_mid_keys, s0, tile_start[tt + 1] - s0, SORT_MID_SLOT_BITS, keys, slot_inst,
+                               sorted_gid, sorted_inst, slot_mask, sorted_mask);
+            __syncthreads();
+        }
     }
 }
 
