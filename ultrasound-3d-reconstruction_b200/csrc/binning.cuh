@@ -508,21 +508,32 @@ tile_sort_huge_kernel(int64_t T, const int* __restrict__ tile_start, const long 
 // within a bucket are distinct (a Gaussian enters a tile's bucket at most once), so any
 // correct sorting network gives that order. The optional 16-bit per-slot mask (slot_mask) follows
 // its instance into sorted_mask.
-static __global__ void __launch_bounds__(SORT_THREADS, SORT_MIN_BLOCKS)
+// PACKED: every element index of the call is below SORT_PACK_G, so buckets of up to
+// SORT_SMEM_CAP keys sort without a payload; the block then needs only the 32 KB key array and
+// runs with 256 threads, seven blocks (tiles) per SM instead of four.
+constexpr int SORT_PACKED_THREADS = 256;
+constexpr int SORT_PACKED_MIN_BLOCKS = 7;
+
+template <bool PACKED>
+static __global__ void __launch_bounds__(PACKED ? SORT_PACKED_THREADS : SORT_THREADS,
+                                         PACKED ? SORT_PACKED_MIN_BLOCKS : SORT_MIN_BLOCKS)
 tile_sort_kernel(int64_t T, const int* __restrict__ tile_start, const long long* __restrict__ header,
                  unsigned long long* __restrict__ keys, const int* __restrict__ slot_inst,
                  int* __restrict__ sorted_gid, int* __restrict__ sorted_inst,
-                 const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask, int packed) {
+                 const uint16_t* __restrict__ slot_mask, uint16_t* __restrict__ sorted_mask) {
     __shared__ __align__(16) unsigned long long s_keys[SORT_SMEM_CAP];
-    __shared__ __align__(16) int s_idx[SORT_SMEM_CAP];
+    __shared__ __align__(16) int s_idx[PACKED ? 4 : SORT_SMEM_CAP];
     const int64_t t = blockIdx.x;
     if (t >= T || header[H_FLAGS] != 0) return;
     const int s0 = tile_start[t];
     const int n = tile_start[t + 1] - s0;
     if (n <= 0) return;
     if (n <= SORT_SMEM_CAP) {
-        sort_bucket_smem(s_keys, s_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask,
-                         packed != 0);
+        if constexpr (PACKED)
+            sort_bucket_packed(s_keys, s0, n, 12, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
+        else
+            sort_bucket_smem(s_keys, s_idx, s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask,
+                             false);
     } else if (n > SORT_HUGE_CAP) {
         sort_bucket_global(s0, n, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
     }
@@ -628,9 +639,12 @@ static inline cudaError_t launch_tile_sort(int64_t T, int64_t n_elems, const int
                                            const uint16_t* slot_mask = nullptr,
                                            uint16_t* sorted_mask = nullptr) {
     if (T <= 0) return cudaSuccess;
-    const int packed = n_elems < SORT_PACK_G ? 1 : 0;
-    tile_sort_kernel<<<(unsigned)T, SORT_THREADS, 0, stream>>>(T, tile_start, header, keys, slot_inst, sorted_gid,
-                                                                sorted_inst, slot_mask, sorted_mask, packed);
+    if (n_elems < SORT_PACK_G)
+        tile_sort_kernel<true><<<(unsigned)T, SORT_PACKED_THREADS, 0, stream>>>(
+            T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
+    else
+        tile_sort_kernel<false><<<(unsigned)T, SORT_THREADS, 0, stream>>>(
+            T, tile_start, header, keys, slot_inst, sorted_gid, sorted_inst, slot_mask, sorted_mask);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int dev = 0;
