@@ -193,10 +193,12 @@ forward_kernel(int H, int W, int gw, float hw, float hh, float rs, const float2*
     alpha[p] = ao;
 }
 
-// One block per tile; thread k owns instance k and sweeps the part of its pixel bounding
-// box inside the tile (reference render.cu:428-515 and :517-600 for the per-pair terms).
+// One block per tile, or `split` blocks per tile that share its instances (frames with few
+// tiles: a 256x256 slice has 256, under two blocks per SM); a thread owns one instance at a time
+// and sweeps the part of its pixel bounding box inside the tile (reference render.cu:428-515 and
+// :517-600 for the per-pair terms), so the partials do not depend on the split.
 __global__ void __launch_bounds__(256)
-backward_kernel(int H, int W, int gw, float hw, float hh, float rs, const float2* __restrict__ means,
+backward_kernel(int split, int H, int W, int gw, float hw, float hh, float rs, const float2* __restrict__ means,
                 const float4* __restrict__ invs, const float* __restrict__ weights, const float* __restrict__ colors,
                 const float* __restrict__ grad_image, const float* __restrict__ grad_alpha,
                 const int4* __restrict__ bbox, const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
@@ -204,9 +206,9 @@ backward_kernel(int H, int W, int gw, float hw, float hh, float rs, const float2
                 float4* __restrict__ partial) {
     __shared__ float4 s_go[TILE * TILE];  // grad_image rgb, grad_alpha
     if (header[H_FLAGS] != 0) return;
-    const int t = blockIdx.x;
+    const int t = blockIdx.x / split, part = blockIdx.x % split;
     const int s0 = tile_start[t], n = tile_start[t + 1] - s0;
-    if (n <= 0) return;
+    if (n <= part * (int)blockDim.x) return;
     const int tx0 = (t % gw) * TILE, ty0 = (t / gw) * TILE;
     {
         const int x = tx0 + (threadIdx.x % TILE), y = ty0 + (threadIdx.x / TILE);
@@ -219,7 +221,7 @@ backward_kernel(int H, int W, int gw, float hw, float hh, float rs, const float2
     }
     __syncthreads();
     const float r2 = rs * rs;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    for (int k = part * blockDim.x + threadIdx.x; k < n; k += split * blockDim.x) {
         const int g = sorted_gid[s0 + k];
         const int4 bb = bbox[g];
         const int x0 = max(bb.x, tx0), x1 = min(bb.z, min(tx0 + TILE - 1, W - 1));
@@ -491,7 +493,8 @@ extern "C" int us3d_sa_bounded_backward(void* workspace, int64_t n, int32_t H, i
     cudaStream_t stream = (cudaStream_t)stream_;
     float4* partial = reinterpret_cast<float4*>(scratch);
     const int prof = prof_begin("sa_backward", stream);
-    backward_kernel<<<(unsigned)T, 256, 0, stream>>>(H, W, gw, half_width, half_height, radius_sigma,
+    const int split = T < 4 * 148 ? 4 : 1;  // few tiles: four blocks share each tile's instances
+    backward_kernel<<<(unsigned)(T * split), 256, 0, stream>>>(split, H, W, gw, half_width, half_height, radius_sigma,
                                                      reinterpret_cast<const float2*>(means2d),
                                                      reinterpret_cast<const float4*>(inv2d), weights, colors,
                                                      grad_image, grad_alpha, w.bbox, w.tile_start, w.sorted_gid,
