@@ -166,7 +166,7 @@ def test_config2_slice_adapted(config2, cuda_device):
                   means2d=c(m2), inv2d=c(inv2), weights=c(w2), colors=c(c2), grad_image=c(gi), grad_alpha=c(ga),
                   ref_image=c(image), ref_alpha=c(alpha), ref_d_means=c(dm), ref_d_inv=c(di), ref_d_weights=c(dw),
                   ref_d_colors=c(dc), ref_sorted_ids=c(ids), ref_range_start=c(starts), ref_range_end=c(ends))
-        T._check(run_b200_sa(fx, dev), fx)
+        T._check(run_b200_sa(fx, dev), fx, fp64_gate=True)
 
 
 def test_config2_ultrags(config2, cuda_device):

@@ -19,14 +19,38 @@ pytestmark = pytest.mark.gpu
 ROOT = Path(__file__).resolve().parents[1]
 
 
-def _check(out, fx):
+def exact_gradients(fx):
+    """The FP64 C oracle's gradients of a fixture's inputs."""
+    from oracle import slice_adapted_oracle as SO
+
+    st = SO.render(int(fx["H"]), int(fx["W"]), float(fx["half_width"]), float(fx["half_height"]), fx["means2d"],
+                   fx["inv2d"], fx["weights"], fx["colors"], float(fx["radius_sigma"]), precision="f64")
+    return SO.backward(st, fx["grad_image"], fx["grad_alpha"])
+
+
+def _check(out, fx, fp64_gate=False):
+    """Tile binning bit-exact, images <= 1e-5 and gradients <= 1e-4 relative L2 from the reference.
+
+    With ``fp64_gate`` (large scenes), a gradient further than 1e-4 from the reference passes when
+    it stands no farther from the FP64 oracle's gradients than 1e-4 or twice the reference's own
+    distance from them: a Gaussian's mean gradient is a sum of pixel terms that largely cancel,
+    so fp32 rounding in either implementation's summation order shows up in the relative error."""
     np.testing.assert_array_equal(out["sorted_ids"], fx["ref_sorted_ids"], err_msg="sorted ids")
     np.testing.assert_array_equal(out["range_start"], fx["ref_range_start"], err_msg="range start")
     np.testing.assert_array_equal(out["range_end"], fx["ref_range_end"], err_msg="range end")
     for k in ("image", "alpha"):
         assert rel_l2(out[k], fx["ref_" + k]) <= 1e-5, (k, rel_l2(out[k], fx["ref_" + k]))
+    exact = None
     for k in ("d_means", "d_inv", "d_weights", "d_colors"):
-        assert rel_l2(out[k], fx["ref_" + k]) <= 1e-4, (k, rel_l2(out[k], fx["ref_" + k]))
+        e = rel_l2(out[k], fx["ref_" + k])
+        if e <= 1e-4:
+            continue
+        assert fp64_gate, (k, e)
+        exact = exact if exact is not None else exact_gradients(fx)
+        ex = exact[k].reshape(out[k].shape)
+        ours, ref = rel_l2(out[k], ex), rel_l2(fx["ref_" + k].reshape(out[k].shape), ex)
+        print(f"[fp64 gate] {k}: vs reference {e:.3e}, ours vs fp64 {ours:.3e}, reference vs fp64 {ref:.3e}")
+        assert ours <= max(1e-4, 2.0 * ref), (k, e, ours, ref)
 
 
 @pytest.mark.parametrize("name", sa_golden_names() or ["binned"])

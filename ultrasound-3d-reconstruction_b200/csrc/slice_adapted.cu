@@ -24,6 +24,8 @@ namespace sa {
 constexpr int TILE = 16;  // reference SLICE_3DGS_TILE_SIZE (render.cu:14)
 constexpr int FWD_BATCH = 256;
 constexpr int PARTIAL_F4 = 3;  // 12 floats per instance
+constexpr int BWD_CHUNK = 1024;  // instances a backward block orders by box area at a time
+constexpr int AREA_BINS = 32;    // area classes of 8 pixels (a box inside one tile covers 1..256)
 
 struct Workspace {
     long long* header;
@@ -205,10 +207,14 @@ backward_kernel(int split, int H, int W, int gw, float hw, float hh, float rs, c
                 const int* __restrict__ sorted_inst, const long long* __restrict__ header,
                 float4* __restrict__ partial) {
     __shared__ float4 s_go[TILE * TILE];  // grad_image rgb, grad_alpha
+    __shared__ int s_key[BWD_CHUNK];      // area class << 16 | rank within the class
+    __shared__ int s_ord[BWD_CHUNK];      // chunk positions ordered by area class
+    __shared__ int s_bin[AREA_BINS];
     if (header[H_FLAGS] != 0) return;
     const int t = blockIdx.x / split, part = blockIdx.x % split;
     const int s0 = tile_start[t], n = tile_start[t + 1] - s0;
-    if (n <= part * (int)blockDim.x) return;
+    const int cs = min(BWD_CHUNK, (n + split - 1) / split);  // chunk: the split shares a tile evenly
+    if (n <= part * cs) return;
     const int tx0 = (t % gw) * TILE, ty0 = (t / gw) * TILE;
     {
         const int x = tx0 + (threadIdx.x % TILE), y = ty0 + (threadIdx.x / TILE);
@@ -221,20 +227,60 @@ backward_kernel(int split, int H, int W, int gw, float hw, float hh, float rs, c
     }
     __syncthreads();
     const float r2 = rs * rs;
-    for (int k = part * blockDim.x + threadIdx.x; k < n; k += split * blockDim.x) {
-        const int g = sorted_gid[s0 + k];
-        const int4 bb = bbox[g];
-        const int x0 = max(bb.x, tx0), x1 = min(bb.z, min(tx0 + TILE - 1, W - 1));
-        const int y0 = max(bb.y, ty0), y1 = min(bb.w, min(ty0 + TILE - 1, H - 1));
-        const float2 m = means[g];
-        const float4 inv = invs[g];
-        const float weight = weights[g];
-        const float c0 = colors[3 * g], c1 = colors[3 * g + 1], c2 = colors[3 * g + 2];
-        float gm0 = 0.f, gm1 = 0.f, gi0 = 0.f, gi1 = 0.f, gi2 = 0.f, gi3 = 0.f, gwt = 0.f, gc0 = 0.f, gc1 = 0.f,
-              gc2 = 0.f;
-        for (int y = y0; y <= y1; ++y) {
-            const float py = plane_y(y, H, hh);
-            for (int x = x0; x <= x1; ++x) {
+    const int xe = min(tx0 + TILE - 1, W - 1), ye = min(ty0 + TILE - 1, H - 1);
+    // The tile's instances go out in chunks; inside a chunk, positions are handed to threads in
+    // order of the box-in-tile area (a counting sort on area classes), so that the 32 lanes of a
+    // warp sweep similar pixel counts. Which thread computes an instance does not change its sums.
+    for (int q0 = part * cs; q0 < n; q0 += split * cs) {
+        const int nc = min(cs, n - q0);
+        __syncthreads();  // the previous chunk's s_ord is read to the end
+        if (threadIdx.x < AREA_BINS) s_bin[threadIdx.x] = 0;
+        __syncthreads();
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            const int4 bb = bbox[sorted_gid[s0 + q0 + j]];
+            const int area = max(0, min(bb.z, xe) - max(bb.x, tx0) + 1) * max(0, min(bb.w, ye) - max(bb.y, ty0) + 1);
+            const int bin = min(AREA_BINS - 1, max(area - 1, 0) >> 3);
+            s_key[j] = (bin << 16) | atomicAdd(&s_bin[bin], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {  // exclusive scan of the class counts in one warp
+            const int v = s_bin[threadIdx.x];
+            int incl = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                if ((int)threadIdx.x >= o) incl += u;
+            }
+            s_bin[threadIdx.x] = incl - v;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            const int key = s_key[j];
+            s_ord[s_bin[key >> 16] + (key & 0xffff)] = j;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+            const int k = q0 + s_ord[i];
+            const int g = sorted_gid[s0 + k];
+            const int4 bb = bbox[g];
+            const int x0 = max(bb.x, tx0), x1 = min(bb.z, xe);
+            const int y0 = max(bb.y, ty0), y1 = min(bb.w, ye);
+            const float2 m = means[g];
+            const float4 inv = invs[g];
+            const float weight = weights[g];
+            const float c0 = colors[3 * g], c1 = colors[3 * g + 1], c2 = colors[3 * g + 2];
+            float gm0 = 0.f, gm1 = 0.f, gi0 = 0.f, gi1 = 0.f, gi2 = 0.f, gi3 = 0.f, gwt = 0.f, gc0 = 0.f, gc1 = 0.f,
+                  gc2 = 0.f;
+            // Row-major sweep of the box in one loop (the same pixel order as rows then columns), so
+            // that lanes with equal areas but different box shapes run in step.
+            const int bw = x1 - x0 + 1;
+            const int cnt = (x1 >= x0 && y1 >= y0) ? bw * (y1 - y0 + 1) : 0;
+            int x = x0 - 1, y = y0;
+            float py = plane_y(y0, H, hh);
+            for (int q = 0; q < cnt; ++q) {
+                if (++x > x1) {
+                    x = x0;
+                    py = plane_y(++y, H, hh);
+                }
                 const float px = plane_x(x, W, hw);
                 const float dx = px - m.x, dy = py - m.y;
                 const float qx = inv.x * dx + inv.y * dy;
@@ -261,11 +307,11 @@ backward_kernel(int split, int H, int W, int gw, float hw, float hh, float rs, c
                 gm0 += 0.5f * dpow * ((inv.x + inv.x) * dx + (inv.y + inv.z) * dy);
                 gm1 += 0.5f * dpow * ((inv.z + inv.y) * dx + (inv.w + inv.w) * dy);
             }
+            float4* out = partial + (int64_t)PARTIAL_F4 * sorted_inst[s0 + k];
+            out[0] = make_float4(gm0, gm1, gi0, gi1);
+            out[1] = make_float4(gi2, gi3, gwt, gc0);
+            out[2] = make_float4(gc1, gc2, 0.f, 0.f);
         }
-        float4* out = partial + (int64_t)PARTIAL_F4 * sorted_inst[s0 + k];
-        out[0] = make_float4(gm0, gm1, gi0, gi1);
-        out[1] = make_float4(gi2, gi3, gwt, gc0);
-        out[2] = make_float4(gc1, gc2, 0.f, 0.f);
     }
 }
 
