@@ -42,8 +42,13 @@ struct Workspace {
     int* slot_inst;
     int* sorted_gid;
     int* sorted_inst;
+    float4* fwd_part;  // list-range sums of the forward when it splits tiles (frame_split(T) x T x 256)
     size_t bytes;
 };
+
+// Blocks that share one tile in the splat kernels: frames with fewer tiles than four per SM split
+// each tile four ways (a 256x256 slice has 256 tiles, under two blocks per SM).
+static inline int frame_split(int64_t T) { return T < 4 * 148 ? 4 : 1; }
 
 static Workspace carve(void* base, int64_t N, int64_t T, int64_t cap) {
     Carver c(base);
@@ -62,6 +67,7 @@ static Workspace carve(void* base, int64_t N, int64_t T, int64_t cap) {
     w.slot_inst = c.take<int>((size_t)cap);
     w.sorted_gid = c.take<int>((size_t)cap);
     w.sorted_inst = c.take<int>((size_t)cap);
+    w.fwd_part = c.take<float4>(frame_split(T) > 1 ? (size_t)frame_split(T) * T * TILE * TILE : 0);
     w.bytes = align_up(c.off, 256);
     return w;
 }
@@ -136,24 +142,29 @@ __global__ void check_kernel(long long* __restrict__ header, int64_t cap) {
 }
 
 
-// One block of 16x16 threads per tile, staged Gaussians, per-pixel sums in tile-list order
-// (reference render.cu:354-426).
+// One block of 16x16 threads per tile and list range, staged Gaussians, per-pixel sums in
+// tile-list order (reference render.cu:354-426). With split > 1 the tile's list is cut into
+// `split` contiguous ranges, block (tile, part) sums range `part` into part_out, and
+// combine_kernel adds the ranges in order.
 __global__ void __launch_bounds__(TILE * TILE)
-forward_kernel(int H, int W, int gw, float hw, float hh, float rs, const float2* __restrict__ means,
+forward_kernel(int split, int H, int W, int gw, float hw, float hh, float rs, const float2* __restrict__ means,
                const float4* __restrict__ invs, const float* __restrict__ weights, const float* __restrict__ colors,
                const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
-               const long long* __restrict__ header, float* __restrict__ image, float* __restrict__ alpha) {
+               const long long* __restrict__ header, float* __restrict__ image, float* __restrict__ alpha,
+               float4* __restrict__ part_out) {
     __shared__ float4 s_inv[FWD_BATCH];
     __shared__ float4 s_mw[FWD_BATCH];   // mx, my, weight, c0
     __shared__ float2 s_c12[FWD_BATCH];  // c1, c2
     if (header[H_FLAGS] != 0) return;
-    const int t = blockIdx.x;
+    const int t = blockIdx.x / split, part = blockIdx.x % split;
     const int x = (t % gw) * TILE + (threadIdx.x % TILE);
     const int y = (t / gw) * TILE + (threadIdx.x / TILE);
     const bool valid = x < W && y < H;
     const float px = plane_x(x, W, hw), py = plane_y(y, H, hh);
     const float r2 = rs * rs;
-    const int s0 = tile_start[t], n = tile_start[t + 1] - s0;
+    const int l0 = tile_start[t], ln = tile_start[t + 1] - l0;
+    const int lo = (int)((int64_t)ln * part / split), hi = (int)((int64_t)ln * (part + 1) / split);
+    const int s0 = l0 + lo, n = hi - lo;
     float o0 = 0.f, o1 = 0.f, o2 = 0.f, ao = 0.f;
     for (int b0 = 0; b0 < n; b0 += FWD_BATCH) {
         const int nb = min(FWD_BATCH, n - b0);
@@ -187,12 +198,41 @@ forward_kernel(int H, int W, int gw, float hw, float hh, float rs, const float2*
             }
         }
     }
+    if (split > 1) {
+        part_out[((int64_t)part * (gridDim.x / split) + t) * (TILE * TILE) + threadIdx.x] = make_float4(o0, o1, o2, ao);
+        return;
+    }
     if (!valid) return;
     const int64_t p = (int64_t)y * W + x;
     image[3 * p + 0] = o0;
     image[3 * p + 1] = o1;
     image[3 * p + 2] = o2;
     alpha[p] = ao;
+}
+
+// Sum of a pixel's list-range sums, in range order (thread per pixel of the tile grid).
+__global__ void __launch_bounds__(256)
+combine_kernel(int split, int T, int H, int W, int gw, const long long* __restrict__ header,
+               const float4* __restrict__ part_in, float* __restrict__ image, float* __restrict__ alpha) {
+    if (header[H_FLAGS] != 0) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // tile * 256 + pixel in tile
+    if (i >= (int64_t)T * TILE * TILE) return;
+    const int t = (int)(i / (TILE * TILE)), l = (int)(i % (TILE * TILE));
+    const int x = (t % gw) * TILE + (l % TILE), y = (t / gw) * TILE + (l / TILE);
+    if (x >= W || y >= H) return;
+    float4 a = part_in[i];
+    for (int k = 1; k < split; ++k) {
+        const float4 b = part_in[(int64_t)k * T * TILE * TILE + i];
+        a.x += b.x;
+        a.y += b.y;
+        a.z += b.z;
+        a.w += b.w;
+    }
+    const int64_t p = (int64_t)y * W + x;
+    image[3 * p + 0] = a.x;
+    image[3 * p + 1] = a.y;
+    image[3 * p + 2] = a.z;
+    alpha[p] = a.w;
 }
 
 // One block per tile, or `split` blocks per tile that share its instances (frames with few
@@ -502,12 +542,18 @@ extern "C" int us3d_sa_bounded_forward(void* workspace, size_t workspace_bytes, 
                                         w.tile_cursor, w.header, w.keys, w.slot_inst, stream));
     US3D_CHECK_CUDA(launch_tile_sort(T, n, w.tile_start, w.header, w.keys, w.slot_inst, w.sorted_gid, w.sorted_inst,
                                      g_sa_sort_attr, stream));
-    forward_kernel<<<(unsigned)T, TILE * TILE, 0, stream>>>(H, W, gw, half_width, half_height, radius_sigma, m2, iv,
-                                                            weights, colors, w.tile_start, w.sorted_gid, w.header,
-                                                            out_image, out_alpha);
+    const int split = frame_split(T);
+    forward_kernel<<<(unsigned)(T * split), TILE * TILE, 0, stream>>>(
+        split, H, W, gw, half_width, half_height, radius_sigma, m2, iv, weights, colors, w.tile_start, w.sorted_gid,
+        w.header, out_image, out_alpha, w.fwd_part);
     US3D_CHECK_LAUNCH("sa forward");
+    if (split > 1) {
+        combine_kernel<<<(unsigned)((T * TILE * TILE + 255) / 256), 256, 0, stream>>>(split, (int)T, H, W, gw, w.header,
+                                                                                   w.fwd_part, out_image, out_alpha);
+        US3D_CHECK_LAUNCH("sa forward combine");
+    }
     prof_end(prof, stream);
-    count_launches(1 + 3 * (n > 0) + 6 + 1 + tile_sort_launches(n) + 1);
+    count_launches(1 + 3 * (n > 0) + 6 + 1 + tile_sort_launches(n) + 1 + (split > 1));
     return US3D_OK;
 }
 
@@ -539,7 +585,7 @@ extern "C" int us3d_sa_bounded_backward(void* workspace, int64_t n, int32_t H, i
     cudaStream_t stream = (cudaStream_t)stream_;
     float4* partial = reinterpret_cast<float4*>(scratch);
     const int prof = prof_begin("sa_backward", stream);
-    const int split = T < 4 * 148 ? 4 : 1;  // few tiles: four blocks share each tile's instances
+    const int split = frame_split(T);
     backward_kernel<<<(unsigned)(T * split), 256, 0, stream>>>(split, H, W, gw, half_width, half_height, radius_sigma,
                                                      reinterpret_cast<const float2*>(means2d),
                                                      reinterpret_cast<const float4*>(inv2d), weights, colors,
