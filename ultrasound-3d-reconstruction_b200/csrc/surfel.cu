@@ -805,6 +805,44 @@ __device__ __forceinline__ V3 dnormvdv(const V3 v, const V3 dv) {
 // One thread per Gaussian: sum its instance partials in order, then the preprocess backward
 // (backward.cu:406-602): mean2D -> homography, homography -> mean / scale / rotation, normal
 // -> rotation, SH -> colour and mean, and the reference's screen-space mean gradient.
+// Per-Gaussian sums of its instances' partials, in instance order, written over its first
+// instance's partial: PARTIAL_F4 threads per Gaussian, thread f summing float4 column f, so that
+// the threads of a Gaussian read each 80-byte partial together and many Gaussians' loads are in
+// flight (the sums are the ones a thread summing all columns would form).
+constexpr int REDUCE_THREADS = 32 * PARTIAL_F4;  // 32 Gaussians per block
+__global__ void __launch_bounds__(REDUCE_THREADS)
+reduce_partials_kernel(int64_t n_gauss, const int* __restrict__ radii, const int* __restrict__ inst_offset,
+                       const long long* __restrict__ header, float4* __restrict__ partial) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t g = t / PARTIAL_F4;
+    const int f = (int)(t % PARTIAL_F4);
+    if (g >= n_gauss || radii[g] <= 0 || header[H_FLAGS] != 0) return;
+    const int i0 = inst_offset[g], i1 = inst_offset[g + 1];
+    if (i1 <= i0) return;
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    int i = i0;
+    for (; i + 4 <= i1; i += 4) {  // four instances' loads in flight
+        float4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = partial[(int64_t)PARTIAL_F4 * (i + u) + f];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            s.x += v[u].x;
+            s.y += v[u].y;
+            s.z += v[u].z;
+            s.w += v[u].w;
+        }
+    }
+    for (; i < i1; ++i) {
+        const float4 v = partial[(int64_t)PARTIAL_F4 * i + f];
+        s.x += v.x;
+        s.y += v.y;
+        s.z += v.z;
+        s.w += v.w;
+    }
+    partial[(int64_t)PARTIAL_F4 * i0 + f] = s;
+}
+
 __global__ void __launch_bounds__(128)
 reduce_preprocess_kernel(Params p, float focal_x, float focal_y, float tan_fovx, float tan_fovy,
                          const int* __restrict__ radii, const int* __restrict__ inst_offset,
@@ -819,25 +857,18 @@ reduce_preprocess_kernel(Params p, float focal_x, float focal_y, float tan_fovx,
 #pragma unroll
     for (int q = 0; q < 20; ++q) s[q] = 0.f;
     const bool vis = radii[g] > 0 && header[H_FLAGS] == 0;
-    if (vis) {
-        auto add = [&](const float4& x, int f) {
-            s[4 * f] += x.x; s[4 * f + 1] += x.y; s[4 * f + 2] += x.z; s[4 * f + 3] += x.w;
-        };
-        const int i1 = inst_offset[g + 1];
-        int i = inst_offset[g];
-        // two instances' loads in flight at a time; the sums keep instance order
-        for (; i + 2 <= i1; i += 2) {
-            const float4* r = partial + (int64_t)PARTIAL_F4 * i;
-            float4 v[2 * PARTIAL_F4];
+    if (vis) {  // the instance sums reduce_partials_kernel left in the first instance's partial
+        const int i0 = inst_offset[g];
+        if (inst_offset[g + 1] > i0) {
+            const float4* r = partial + (int64_t)PARTIAL_F4 * i0;
 #pragma unroll
-            for (int f = 0; f < 2 * PARTIAL_F4; ++f) v[f] = r[f];
-#pragma unroll
-            for (int f = 0; f < 2 * PARTIAL_F4; ++f) add(v[f], f % PARTIAL_F4);
-        }
-        if (i < i1) {
-            const float4* r = partial + (int64_t)PARTIAL_F4 * i;
-#pragma unroll
-            for (int f = 0; f < PARTIAL_F4; ++f) add(r[f], f);
+            for (int f = 0; f < PARTIAL_F4; ++f) {
+                const float4 x = r[f];
+                s[4 * f] = x.x;
+                s[4 * f + 1] = x.y;
+                s[4 * f + 2] = x.z;
+                s[4 * f + 3] = x.w;
+            }
         }
     }
     // defaults: everything zero, render sums passed through
@@ -1164,13 +1195,16 @@ extern "C" int us3d_gs_backward(void* workspace, int64_t n_gauss, int32_t sh_deg
     backward_kernel<<<(unsigned)T, BLOCK, 0, stream>>>(width, height, p.gx, w.tile_start, w.sorted_gid,
                                                        w.sorted_inst, w.header, w.rec, background, w.accum,
                                                        w.n_contrib, dL_dcolor, dL_dothers, partial);
-    if (n_gauss > 0)
+    if (n_gauss > 0) {
+        reduce_partials_kernel<<<(unsigned)((n_gauss * PARTIAL_F4 + REDUCE_THREADS - 1) / REDUCE_THREADS),
+                                 REDUCE_THREADS, 0, stream>>>(n_gauss, radii, w.inst_offset, w.header, partial);
         reduce_preprocess_kernel<<<(unsigned)((n_gauss + 127) / 128), 128, 0, stream>>>(
             p, focal_x, focal_y, tan_fovx, tan_fovy, radii, w.inst_offset, w.header, partial, w.rec, w.clamped,
             d_means2D, d_colors, d_opacity, d_means3D, d_transmat, d_sh, d_scales, d_rotations);
+    }
     US3D_CHECK_LAUNCH("gs backward");
     prof_end(prof, stream);
-    count_launches(1 + (n_gauss > 0));
+    count_launches(1 + 2 * (n_gauss > 0));
     return US3D_OK;
 }
 
