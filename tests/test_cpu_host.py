@@ -248,3 +248,20 @@ def test_frame_source_camera_fields(tmp_path):
         src.camera(torch.tensor([1, 4], dtype=torch.int64))
         with pytest.raises(IndexError):
             src.check()
+
+
+def test_float_outputs_one_allocation():
+    """Gradient outputs carved from one buffer: shapes as asked, each view 16-byte aligned and
+    disjoint from the others, the listed ones zero-filled."""
+    from us3d_b200._alloc import float_outputs
+
+    shapes = [(5, 3), (5, 1), (5, 0, 3), (4, 4), (7,)]
+    out = float_outputs(torch.device("cpu"), shapes, zero=(3,))
+    assert [tuple(t.shape) for t in out] == shapes
+    assert all(t.dtype == torch.float32 and t.is_contiguous() for t in out)
+    assert all(t.data_ptr() % 16 == 0 for t in out if t.numel())
+    assert torch.equal(out[3], torch.zeros(4, 4))
+    for i, t in enumerate(out):
+        t.fill_(float(i + 1))
+    for i, t in enumerate(out):
+        assert bool((t == float(i + 1)).all())

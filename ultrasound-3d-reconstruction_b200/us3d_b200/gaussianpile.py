@@ -9,6 +9,7 @@ from typing import Optional
 import torch
 
 from . import _lib
+from ._alloc import float_outputs
 
 _capacity_hint: dict = {}
 
@@ -79,12 +80,9 @@ def backward(b: GPBinning, grad_image: torch.Tensor, pose_grad: bool = False,
     dev = means.device
     sbytes = int(_lib.call("us3d_gp_backward_scratch_bytes", G, b.capacity))
     scratch = torch.empty(max(sbytes, 16), dtype=torch.uint8, device=dev)
-    dm = torch.empty((G, 3), dtype=torch.float32, device=dev)
-    ds = torch.empty((G, 3), dtype=torch.float32, device=dev)
-    dq = torch.empty((G, 4), dtype=torch.float32, device=dev)
-    do = torch.empty((G,), dtype=torch.float32, device=dev)
-    di = torch.empty((G,), dtype=torch.float32, device=dev)
-    dp = torch.zeros((4, 4), dtype=torch.float32, device=dev)
+    # every gradient is written in full; the pose gradient only when it is asked for
+    dm, ds, dq, do, di, dp = float_outputs(dev, [(G, 3), (G, 3), (G, 4), (G,), (G,), (4, 4)],
+                                           zero=() if pose_grad else (5,))
     gi = grad_image.reshape(-1).contiguous().float()
     st = _lib.call("us3d_gp_backward", b.workspace.data_ptr(), G, *(t.data_ptr() for t in b.tensors), b.H, b.W, b.tile,
                    b.k_sigma, b.capacity, gi.data_ptr(), flags, scratch.data_ptr(), scratch.numel(),

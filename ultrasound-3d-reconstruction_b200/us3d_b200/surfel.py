@@ -14,6 +14,7 @@ from typing import Optional
 import torch
 
 from . import _lib
+from ._alloc import float_outputs
 
 _capacity_hint: dict = {}
 
@@ -97,11 +98,10 @@ def backward(state: Optional[GSState], background, means3D, radii, colors, scale
     if P == 0 or state is None:
         return z(P, 3), z(P, 3), z(P, 1), z(P, 3), z(P, 9), z(P, M, 3), z(P, 2), z(P, 4)
     # the backward writes every entry of each gradient it is given; the others stay zero
-    e = lambda *s: torch.empty(s, dtype=torch.float32, device=dev)  # noqa: E731
-    dmeans2D, dcolors, dopacity, dmeans3D, dtrans = e(P, 3), e(P, 3), e(P, 1), e(P, 3), e(P, 9)
-    dsh = e(P, M, 3) if M > 0 and _ptr(sh) else z(P, M, 3)
-    dscales = e(P, 2) if _ptr(scales) else z(P, 2)
-    drot = e(P, 4) if _ptr(rotations) else z(P, 4)
+    has_sh, has_sc, has_rot = M > 0 and _ptr(sh) is not None, _ptr(scales) is not None, _ptr(rotations) is not None
+    dmeans2D, dcolors, dopacity, dmeans3D, dtrans, dsh, dscales, drot = float_outputs(
+        dev, [(P, 3), (P, 3), (P, 1), (P, 3), (P, 9), (P, M, 3), (P, 2), (P, 4)],
+        zero=[i for i, given in ((5, has_sh), (6, has_sc), (7, has_rot)) if not given])
     H, W = int(dL_dout_color.shape[1]), int(dL_dout_color.shape[2])
     scratch = torch.empty(max(int(_lib.call("us3d_gs_backward_scratch_bytes", state.capacity)), 16),
                           dtype=torch.uint8, device=dev)
@@ -112,8 +112,8 @@ def backward(state: Optional[GSState], background, means3D, radii, colors, scale
                    _ptr(transmat_precomp), viewmatrix.data_ptr(), projmatrix.data_ptr(), _ptr(campos),
                    float(tan_fovx), float(tan_fovy), radii.data_ptr(), state.capacity, gc.data_ptr(), go.data_ptr(),
                    scratch.data_ptr(), scratch.numel(), dmeans2D.data_ptr(), dcolors.data_ptr(), dopacity.data_ptr(),
-                   dmeans3D.data_ptr(), dtrans.data_ptr(), dsh.data_ptr() if M > 0 and _ptr(sh) else None,
-                   dscales.data_ptr() if _ptr(scales) else None, drot.data_ptr() if _ptr(rotations) else None,
+                   dmeans3D.data_ptr(), dtrans.data_ptr(), dsh.data_ptr() if has_sh else None,
+                   dscales.data_ptr() if has_sc else None, drot.data_ptr() if has_rot else None,
                    _stream())
     _lib.check(st, "us3d_gs_backward")
     return dmeans2D, dcolors, dopacity, dmeans3D, dtrans, dsh, dscales, drot
