@@ -804,8 +804,46 @@ __device__ __forceinline__ float3 normalize3_bwd(const float3 raw, const float3 
     return make_float3((g.x - n.x * dn) * il, (g.y - n.y * dn) * il, (g.z - n.z * dn) * il);
 }
 
-// Per Gaussian: reduce its instance partials (fixed order), then the chain rule through
-// Se and Lc, finite-difference shape gradients, sanitising, and the pose contribution
+// Per-Gaussian sums of its instances' partial records, in instance order, written over its first
+// instance's record: PARTIAL_F4 threads per Gaussian, thread f summing float4 column f, so that
+// the threads of a Gaussian read each 80-byte record together and many Gaussians' loads are in
+// flight (the sums are the ones a thread summing all columns would form).
+constexpr int REDUCE_THREADS = 32 * PARTIAL_F4;  // 32 Gaussians per block
+__global__ void __launch_bounds__(REDUCE_THREADS)
+reduce_partials_kernel(int64_t G, const int* __restrict__ inst_offset, const long long* __restrict__ header,
+                       float4* __restrict__ partial) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t g = t / PARTIAL_F4;
+    const int f = (int)(t % PARTIAL_F4);
+    if (g >= G || header[H_FLAGS] != 0) return;
+    const int i0 = inst_offset[g], i1 = inst_offset[g + 1];
+    if (i1 <= i0) return;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    int i = i0;
+    for (; i + 4 <= i1; i += 4) {  // four instances' loads in flight
+        float4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = partial[(int64_t)PARTIAL_F4 * (i + u) + f];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            acc.x += v[u].x;
+            acc.y += v[u].y;
+            acc.z += v[u].z;
+            acc.w += v[u].w;
+        }
+    }
+    for (; i < i1; ++i) {
+        const float4 v = partial[(int64_t)PARTIAL_F4 * i + f];
+        acc.x += v.x;
+        acc.y += v.y;
+        acc.z += v.z;
+        acc.w += v.w;
+    }
+    partial[(int64_t)PARTIAL_F4 * i0 + f] = acc;
+}
+
+// Per Gaussian: its instance partials summed by reduce_partials_kernel, then the chain rule
+// through Se and Lc, finite-difference shape gradients, sanitising, and the pose contribution
 // (reference us_focus.cu:479-803).
 __global__ void __launch_bounds__(128)
 finalize_kernel(int64_t G, float k_sigma, const int* __restrict__ inst_offset, const int4* __restrict__ rects,
@@ -845,15 +883,14 @@ finalize_kernel(int64_t G, float k_sigma, const int* __restrict__ inst_offset, c
     float acc[P_COUNT];
 #pragma unroll
     for (int i = 0; i < P_COUNT; ++i) acc[i] = 0.f;
-    const float4* pr = reinterpret_cast<const float4*>(partial);
-    for (int i = inst_offset[g]; i < inst_offset[g + 1]; ++i) {
-        const float4* r = pr + (int64_t)PARTIAL_F4 * i;
+    if (inst_offset[g + 1] > inst_offset[g]) {  // the sums reduce_partials_kernel left in the first record
+        const float4* r = reinterpret_cast<const float4*>(partial) + (int64_t)PARTIAL_F4 * inst_offset[g];
         const float4 a = r[0], b = r[1], c = r[2], d = r[3], e = r[4];
-        acc[0] += a.x; acc[1] += a.y; acc[2] += a.z; acc[3] += a.w;
-        acc[4] += b.x; acc[5] += b.y; acc[6] += b.z; acc[7] += b.w;
-        acc[8] += c.x; acc[9] += c.y; acc[10] += c.z; acc[11] += c.w;
-        acc[12] += d.x; acc[13] += d.y; acc[14] += d.z; acc[15] += d.w;
-        acc[16] += e.x; acc[17] += e.y; acc[18] += e.z;
+        acc[0] = a.x; acc[1] = a.y; acc[2] = a.z; acc[3] = a.w;
+        acc[4] = b.x; acc[5] = b.y; acc[6] = b.z; acc[7] = b.w;
+        acc[8] = c.x; acc[9] = c.y; acc[10] = c.z; acc[11] = c.w;
+        acc[12] = d.x; acc[13] = d.y; acc[14] = d.z; acc[15] = d.w;
+        acc[16] = e.x; acc[17] = e.y; acc[18] = e.z;
     }
 
     const float depth = fmaxf(F.mu_ax - near_mm, 0.f);
@@ -1157,6 +1194,10 @@ extern "C" int us3d_gp_backward(void* workspace, int64_t n_gauss, const float* m
         launches = 1;
     }
     if (n_gauss > 0) {
+        reduce_partials_kernel<<<(unsigned)((n_gauss * PARTIAL_F4 + REDUCE_THREADS - 1) / REDUCE_THREADS),
+                                 REDUCE_THREADS, 0, stream>>>(n_gauss, w.inst_offset, w.header,
+                                                              reinterpret_cast<float4*>(partial));
+        ++launches;
         finalize_kernel<<<(unsigned)((n_gauss + 127) / 128), 128, 0, stream>>>(
             n_gauss, k_sigma, w.inst_offset, w.rects, means, scales, quats, pose, grid_pack, focus_params, w.header,
             partial, pose_grad, shape_analytic_mode, d_means, d_scales, d_quats, d_opacities, d_intensities,
