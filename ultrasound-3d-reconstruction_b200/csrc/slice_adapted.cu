@@ -355,31 +355,52 @@ backward_kernel(int split, int H, int W, int gw, float hw, float hh, float rs, c
     }
 }
 
-__global__ void __launch_bounds__(256)
+// Per-Gaussian gradient: the sum of its instances' 48-byte partials in instance order.
+// REDUCE_COLS threads per Gaussian, thread f summing float4 column f, so that a Gaussian's
+// threads read each partial together; the sums are the ones a thread summing all columns would
+// form.
+constexpr int REDUCE_COLS = 3;
+constexpr int REDUCE_THREADS = 64 * REDUCE_COLS;  // 64 Gaussians per block
+__global__ void __launch_bounds__(REDUCE_THREADS)
 reduce_kernel(int64_t N, const int* __restrict__ inst_offset, const long long* __restrict__ header,
               const float4* __restrict__ partial, float* __restrict__ d_means, float* __restrict__ d_inv,
               float* __restrict__ d_w, float* __restrict__ d_c) {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t g = t / REDUCE_COLS;
+    const int f = (int)(t % REDUCE_COLS);
     if (g >= N) return;
-    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, c = a;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
     if (header[H_FLAGS] == 0) {
-        for (int i = inst_offset[g]; i < inst_offset[g + 1]; ++i) {
-            const float4 x = partial[3 * (int64_t)i], y = partial[3 * (int64_t)i + 1], z = partial[3 * (int64_t)i + 2];
-            a.x += x.x; a.y += x.y; a.z += x.z; a.w += x.w;
-            b.x += y.x; b.y += y.y; b.z += y.z; b.w += y.w;
-            c.x += z.x; c.y += z.y;
+        const int i1 = inst_offset[g + 1];
+        int i = inst_offset[g];
+        for (; i + 4 <= i1; i += 4) {  // four instances' loads in flight, summed in order
+            float4 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = partial[(int64_t)PARTIAL_F4 * (i + u) + f];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a.x += v[u].x; a.y += v[u].y; a.z += v[u].z; a.w += v[u].w;
+            }
+        }
+        for (; i < i1; ++i) {
+            const float4 v = partial[(int64_t)PARTIAL_F4 * i + f];
+            a.x += v.x; a.y += v.y; a.z += v.z; a.w += v.w;
         }
     }
-    d_means[2 * g] = a.x;
-    d_means[2 * g + 1] = a.y;
-    d_inv[4 * g] = a.z;
-    d_inv[4 * g + 1] = a.w;
-    d_inv[4 * g + 2] = b.x;
-    d_inv[4 * g + 3] = b.y;
-    d_w[g] = b.z;
-    d_c[3 * g] = b.w;
-    d_c[3 * g + 1] = c.x;
-    d_c[3 * g + 2] = c.y;
+    if (f == 0) {
+        d_means[2 * g] = a.x;
+        d_means[2 * g + 1] = a.y;
+        d_inv[4 * g] = a.z;
+        d_inv[4 * g + 1] = a.w;
+    } else if (f == 1) {
+        d_inv[4 * g + 2] = a.x;
+        d_inv[4 * g + 3] = a.y;
+        d_w[g] = a.z;
+        d_c[3 * g] = a.w;
+    } else {
+        d_c[3 * g + 1] = a.x;
+        d_c[3 * g + 2] = a.y;
+    }
 }
 
 __global__ void export_kernel(int T, const int* __restrict__ tile_start, const int* __restrict__ sorted_gid,
@@ -592,8 +613,8 @@ extern "C" int us3d_sa_bounded_backward(void* workspace, int64_t n, int32_t H, i
                                                      grad_image, grad_alpha, w.bbox, w.tile_start, w.sorted_gid,
                                                      w.sorted_inst, w.header, partial);
     if (n > 0)
-        reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(n, w.inst_offset, w.header, partial, d_means,
-                                                                        d_inv, d_weights, d_colors);
+        reduce_kernel<<<(unsigned)((n * REDUCE_COLS + REDUCE_THREADS - 1) / REDUCE_THREADS), REDUCE_THREADS, 0,
+                        stream>>>(n, w.inst_offset, w.header, partial, d_means, d_inv, d_weights, d_colors);
     US3D_CHECK_LAUNCH("sa backward");
     prof_end(prof, stream);
     count_launches(1 + (n > 0));

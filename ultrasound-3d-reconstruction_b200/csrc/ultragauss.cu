@@ -1421,56 +1421,60 @@ backward_packed_kernel(int64_t T, int64_t P, const us3d_slice_frame* __restrict_
     }
 }
 
-__global__ void __launch_bounds__(256)
+// Per-Gaussian gradient: the sum of its instances' 48-byte partials in instance order.
+// REDUCE_COLS threads per Gaussian, thread f summing float4 column f, so that a Gaussian's
+// threads read each partial together and many Gaussians' loads are in flight; the sums are the
+// ones a thread summing all columns would form.
+constexpr int REDUCE_COLS = 3;                      // float4 columns of a partial record
+constexpr int REDUCE_THREADS = 64 * REDUCE_COLS;     // 64 Gaussians per block
+__global__ void __launch_bounds__(REDUCE_THREADS)
 reduce_kernel(int64_t G, const int* __restrict__ inst_offset, const long long* __restrict__ header,
               const float4* __restrict__ partial, float* __restrict__ d_means, float* __restrict__ d_tril,
               float* __restrict__ d_opac, float* __restrict__ d_inten) {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t g = t / REDUCE_COLS;
+    const int f = (int)(t % REDUCE_COLS);
     if (g >= G) return;
-    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, c = a;
-    auto add = [&](const float4 x, const float4 y, const float4 z) {
-        a.x += x.x; a.y += x.y; a.z += x.z; a.w += x.w;
-        b.x += y.x; b.y += y.y; b.z += y.z; b.w += y.w;
-        c.x += z.x; c.y += z.y; c.z += z.z;
-    };
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
     if (header[H_FLAGS] == 0) {
-        const int i0 = inst_offset[g], i1 = inst_offset[g + 1];
-        const float4* src = partial + 3 * (int64_t)i0;
-        int i = i0;
+        const int i1 = inst_offset[g + 1];
+        int i = inst_offset[g];
         // four instances' loads in flight at a time; the sums keep instance order
-        for (; i + 4 <= i1; i += 4, src += 12) {
-            float4 v[12];
+        for (; i + 4 <= i1; i += 4) {
+            float4 v[4];
 #pragma unroll
-            for (int u = 0; u < 12; ++u) v[u] = src[u];
+            for (int u = 0; u < 4; ++u) v[u] = partial[3 * (int64_t)(i + u) + f];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) add(v[3 * u], v[3 * u + 1], v[3 * u + 2]);
+            for (int u = 0; u < 4; ++u) {
+                a.x += v[u].x;
+                a.y += v[u].y;
+                a.z += v[u].z;
+                a.w += v[u].w;
+            }
         }
-        if (i < i1) {  // the last one to three instances: their loads first, then the sums in order
-            const int rest = i1 - i;
-            float4 v[9];
-#pragma unroll
-            for (int u = 0; u < 3; ++u)
-                if (u < rest) {
-                    v[3 * u] = src[3 * u];
-                    v[3 * u + 1] = src[3 * u + 1];
-                    v[3 * u + 2] = src[3 * u + 2];
-                }
-#pragma unroll
-            for (int u = 0; u < 3; ++u)
-                if (u < rest) add(v[3 * u], v[3 * u + 1], v[3 * u + 2]);
+        for (; i < i1; ++i) {
+            const float4 v = partial[3 * (int64_t)i + f];
+            a.x += v.x;
+            a.y += v.y;
+            a.z += v.z;
+            a.w += v.w;
         }
     }
-    d_means[3 * g + 0] = a.x;
-    d_means[3 * g + 1] = a.y;
-    d_means[3 * g + 2] = a.z;
-    d_opac[g] = a.w;
-    d_tril[6 * g + 0] = b.x;
-    d_tril[6 * g + 1] = b.y;
-    d_tril[6 * g + 2] = b.z;
-    d_tril[6 * g + 3] = b.w;
-    d_tril[6 * g + 4] = c.x;
-    d_tril[6 * g + 5] = c.y;
-    d_inten[g] = c.z;
+    if (f == 0) {
+        d_means[3 * g + 0] = a.x;
+        d_means[3 * g + 1] = a.y;
+        d_means[3 * g + 2] = a.z;
+        d_opac[g] = a.w;
+    } else if (f == 1) {
+        d_tril[6 * g + 0] = a.x;
+        d_tril[6 * g + 1] = a.y;
+        d_tril[6 * g + 2] = a.z;
+        d_tril[6 * g + 3] = a.w;
+    } else {
+        d_tril[6 * g + 4] = a.x;
+        d_tril[6 * g + 5] = a.y;
+        d_inten[g] = a.z;
+    }
 }
 
 // Per-pixel candidates of a full (reference) binning in tile-list order: the pixels' window
@@ -1868,9 +1872,8 @@ static int ug_backward_impl(void* workspace, const us3d_slice_frame* frames, int
         US3D_CHECK_LAUNCH("ug backward");
     }
     if (n_gauss > 0) {
-        reduce_kernel<<<(unsigned)((n_gauss + 255) / 256), 256, 0, stream>>>(n_gauss, w.inst_offset, w.header,
-                                                                               partial, d_means, d_tril, d_opac,
-                                                                               d_inten);
+        reduce_kernel<<<(unsigned)((n_gauss * REDUCE_COLS + REDUCE_THREADS - 1) / REDUCE_THREADS), REDUCE_THREADS, 0,
+                        stream>>>(n_gauss, w.inst_offset, w.header, partial, d_means, d_tril, d_opac, d_inten);
         US3D_CHECK_LAUNCH("ug reduce");
     }
     prof_end(prof, stream);

@@ -1029,28 +1029,49 @@ backward_kernel(int W, int H, const int* __restrict__ ray_start, const int* __re
     }
 }
 
-__global__ void __launch_bounds__(256)
+// Per-Gaussian gradient: the sum of its instances' partial records in instance order.
+// REDUCE_COLS threads per Gaussian, thread f summing float4 column f, so that a Gaussian's
+// threads read each record together and many Gaussians' loads are in flight; the sums are the
+// ones a thread summing all columns would form.
+constexpr int REDUCE_COLS = 4;
+constexpr int REDUCE_THREADS = 64 * REDUCE_COLS;  // 64 Gaussians per block
+__global__ void __launch_bounds__(REDUCE_THREADS)
 reduce_kernel(int64_t G, const int* __restrict__ inst_offset, const long long* __restrict__ header,
               const float4* __restrict__ partial, float* __restrict__ d_means, float* __restrict__ d_scales,
               float* __restrict__ d_quats, float* __restrict__ d_attens, float* __restrict__ d_sh) {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t g = t / REDUCE_COLS;
+    const int f = (int)(t % REDUCE_COLS);
     if (g >= G) return;
-    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, c = a, d = a;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
     if (header[H_FLAGS] == 0) {
-        for (int i = inst_offset[g]; i < inst_offset[g + 1]; ++i) {
-            const float4* r = partial + (int64_t)PARTIAL_F4 * i;
-            const float4 x = r[0], y = r[1], z = r[2], w = r[3];
-            a.x += x.x; a.y += x.y; a.z += x.z; a.w += x.w;
-            b.x += y.x; b.y += y.y; b.z += y.z; b.w += y.w;
-            c.x += z.x; c.y += z.y; c.z += z.z;
-            d.x += w.x; d.y += w.y; d.z += w.z; d.w += w.w;
+        const int i1 = inst_offset[g + 1];
+        int i = inst_offset[g];
+        for (; i + 4 <= i1; i += 4) {  // four instances' loads in flight, summed in order
+            float4 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = partial[(int64_t)PARTIAL_F4 * (i + u) + f];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a.x += v[u].x; a.y += v[u].y; a.z += v[u].z; a.w += v[u].w;
+            }
+        }
+        for (; i < i1; ++i) {
+            const float4 v = partial[(int64_t)PARTIAL_F4 * i + f];
+            a.x += v.x; a.y += v.y; a.z += v.z; a.w += v.w;
         }
     }
-    d_means[3 * g] = a.x; d_means[3 * g + 1] = a.y; d_means[3 * g + 2] = a.z;
-    d_attens[g] = a.w;
-    d_scales[3 * g] = b.x; d_scales[3 * g + 1] = b.y; d_scales[3 * g + 2] = b.z;
-    d_sh[4 * g] = b.w; d_sh[4 * g + 1] = c.x; d_sh[4 * g + 2] = c.y; d_sh[4 * g + 3] = c.z;
-    d_quats[4 * g] = d.x; d_quats[4 * g + 1] = d.y; d_quats[4 * g + 2] = d.z; d_quats[4 * g + 3] = d.w;
+    if (f == 0) {
+        d_means[3 * g] = a.x; d_means[3 * g + 1] = a.y; d_means[3 * g + 2] = a.z;
+        d_attens[g] = a.w;
+    } else if (f == 1) {
+        d_scales[3 * g] = a.x; d_scales[3 * g + 1] = a.y; d_scales[3 * g + 2] = a.z;
+        d_sh[4 * g] = a.w;
+    } else if (f == 2) {
+        d_sh[4 * g + 1] = a.x; d_sh[4 * g + 2] = a.y; d_sh[4 * g + 3] = a.z;
+    } else {
+        d_quats[4 * g] = a.x; d_quats[4 * g + 1] = a.y; d_quats[4 * g + 2] = a.z; d_quats[4 * g + 3] = a.w;
+    }
 }
 
 // Reference-format CSR of the ray binning (MapperForwardCUDA outputs, wrapper_mapper.cu:119-127).
@@ -1215,9 +1236,9 @@ extern "C" int us3d_ugr_backward(void* workspace, int64_t n_gauss, const float* 
                                                      quadrature_window_radius_mm, local_window_only ? 1 : 0,
                                                      local_max_window_mm, ckpt_rays, partial);
     if (n_gauss > 0)
-        reduce_kernel<<<(unsigned)((n_gauss + 255) / 256), 256, 0, stream>>>(n_gauss, w.inst_offset, w.header, partial,
-                                                                              d_means, d_scales, d_quats,
-                                                                              d_attenuations, d_sh);
+        reduce_kernel<<<(unsigned)((n_gauss * REDUCE_COLS + REDUCE_THREADS - 1) / REDUCE_THREADS), REDUCE_THREADS, 0,
+                        stream>>>(n_gauss, w.inst_offset, w.header, partial, d_means, d_scales, d_quats,
+                                  d_attenuations, d_sh);
     US3D_CHECK_LAUNCH("ugr backward");
     prof_end(prof, stream);
     count_launches(launches);
