@@ -34,7 +34,9 @@
 namespace us3d {
 namespace ug {
 
-// Resident CTAs per SM the forward is compiled for (register budget 65536 / (256 x n)).
+// Resident CTAs per SM the forward is compiled for (register budget 65536 / (256 x n)). Five
+// measured fastest on the 1M-Gaussian 512x512 scene: 2.25 ms per 16 frames, against 2.39 ms with
+// six (40 registers) and 2.50 ms with seven (32 registers).
 #ifndef US3D_UG_FWD_MIN_CTAS
 #define US3D_UG_FWD_MIN_CTAS 5
 #endif
