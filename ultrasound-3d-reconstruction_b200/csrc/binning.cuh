@@ -191,6 +191,9 @@ static inline cudaError_t launch_rect_scatter(int64_t n, int gx, int64_t n_bucke
 // l holds its elements 2l (x0) and 2l + 1 (x1). A compare-exchange of stride h >= 2 pairs
 // lane l with lane l ^ h/2 (same slot); a mirror pass over blocks of `size` pairs element
 // e with e ^ (size - 1), i.e. slot 0 of lane l with slot 1 of lane l ^ (size/2 - 1).
+// (Four keys per lane, 128-element segments and four fewer shared-memory passes for a 1024-key
+// tile, measured slower on every renderer: bin stage 1.07 -> 1.10-1.17 ms for 16 headline
+// frames, UltraGS forward 0.343 -> 0.365 ms. The compare-exchanges are the same network's.)
 template <bool PAY>
 struct SortEl;  // a key with (PAY) or without its int payload
 template <>
