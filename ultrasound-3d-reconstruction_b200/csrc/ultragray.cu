@@ -844,7 +844,13 @@ ckpt_coef_kernel(int W, int H, const long long* __restrict__ header, const int* 
 
 // Thread per instance of a checkpointed ray: the far part of its gradient from the suffix sum at
 // its first far sample, the samples inside its window [first sample past t_gauss, first far
-// sample) and its echo range |t - t_gauss| <= radius visited in sample order.
+// sample) and its echo range |t - t_gauss| <= radius visited in sample order. The ray's
+// instances go out in chunks of CKPT_CHUNK; a block first finds each instance's sample range and
+// then hands the instances to its threads in order of that range's length (a counting sort on
+// CKPT_BINS classes), so that the lanes of a warp sweep similar numbers of samples. Which thread
+// computes an instance does not change its partial.
+constexpr int CKPT_CHUNK = 512;
+constexpr int CKPT_BINS = 32;  // classes of 8 samples
 __global__ void __launch_bounds__(128)
 backward_ckpt_kernel(int W, int H, const int* __restrict__ ray_start, const int* __restrict__ sorted_gid,
                      const int* __restrict__ sorted_inst, const long long* __restrict__ header,
@@ -853,6 +859,10 @@ backward_ckpt_kernel(int W, int H, const int* __restrict__ ray_start, const int*
                      const int* __restrict__ mono, const float* __restrict__ t_pix, const float4* __restrict__ aux,
                      const float4* __restrict__ b_pos, const float4* __restrict__ b_coef,
                      const float* __restrict__ b_suffix, float wr, float4* __restrict__ partial) {
+    __shared__ int s_key[CKPT_CHUNK];  // length class << 16 | rank within the class
+    __shared__ int s_ord[CKPT_CHUNK];  // chunk positions ordered by class
+    __shared__ int s_yt[CKPT_CHUNK], s_ya[CKPT_CHUNK], s_yb[CKPT_CHUNK];
+    __shared__ int s_bin[CKPT_BINS];
     if (header[H_FLAGS] != 0) return;
     const int x = blockIdx.x;
     if (!mono[x]) return;
@@ -860,40 +870,74 @@ backward_ckpt_kernel(int W, int H, const int* __restrict__ ray_start, const int*
     const RayGeo rg = ray_geo(x, ray_o, ray_d, a_ele, pert);
     const float* t = t_pix + (int64_t)x * H;
     const int64_t row = (int64_t)x * H;
-    for (int k = blockIdx.y * blockDim.x + threadIdx.x; k < n; k += gridDim.y * blockDim.x) {
-        Rec r;
-        const int g = sorted_gid[s0 + k];
-        load_rec(rec + (int64_t)REC_F4 * g, r);
-        const float4 a = aux[s0 + k];
-        const float t_gauss = a.x, radius = a.y;
-        const int y_far = __float_as_int(a.w);
-        float dmu[3] = {0.f, 0.f, 0.f}, ds[3] = {0.f, 0.f, 0.f}, dR[9], dP[9], dtau_raw = 0.f;
-        float dsh[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int k0 = blockIdx.y * CKPT_CHUNK; k0 < n; k0 += gridDim.y * CKPT_CHUNK) {
+        const int nc = min(CKPT_CHUNK, n - k0);
+        __syncthreads();  // the previous chunk's arrays are read to the end
+        if (threadIdx.x < CKPT_BINS) s_bin[threadIdx.x] = 0;
+        __syncthreads();
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            const float4 a = aux[s0 + k0 + j];
+            const float t_gauss = a.x, radius = a.y;
+            const int y_far = __float_as_int(a.w);
+            const int y_t = first_sample(t, H, [&](float tp) { return tp > t_gauss; });
+            const int y_e0 = first_sample(t, H, [&](float tp) { return tp >= t_gauss - radius; });
+            const int y_e1 = first_sample(t, H, [&](float tp) { return tp > t_gauss + radius; });
+            const int ya = min(y_t, y_e0), yb = max(y_far, y_e1);
+            s_yt[j] = y_t;
+            s_ya[j] = ya;
+            s_yb[j] = yb;
+            const int bin = min(CKPT_BINS - 1, max(yb - ya, 0) >> 3);
+            s_key[j] = (bin << 16) | atomicAdd(&s_bin[bin], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {  // exclusive scan of the class counts in one warp
+            const int v = s_bin[threadIdx.x];
+            int incl = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                if ((int)threadIdx.x >= o) incl += u;
+            }
+            s_bin[threadIdx.x] = incl - v;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            const int key = s_key[j];
+            s_ord[s_bin[key >> 16] + (key & 0xffff)] = j;
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+            const int j = s_ord[q], k = k0 + j;
+            Rec r;
+            const int g = sorted_gid[s0 + k];
+            load_rec(rec + (int64_t)REC_F4 * g, r);
+            const float4 a = aux[s0 + k];
+            const float t_gauss = a.x, radius = a.y;
+            const int y_far = __float_as_int(a.w);
+            float dmu[3] = {0.f, 0.f, 0.f}, ds[3] = {0.f, 0.f, 0.f}, dR[9], dP[9], dtau_raw = 0.f;
+            float dsh[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            dR[i] = 0.f;
-            dP[i] = 0.f;
+            for (int i = 0; i < 9; ++i) {
+                dR[i] = 0.f;
+                dP[i] = 0.f;
+            }
+            // the far factor, as the per-sample path evaluates it
+            const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, 3.0e38f, wr);
+            const float far_exp = __expf(-psi);
+            const float far_T = r.tau + (1.0f - r.tau) * far_exp;
+            const int y_t = s_yt[j], ya = s_ya[j], yb = s_yb[j];
+            for (int y = ya; y < yb; ++y) {
+                const float4 cf = b_coef[row + y];
+                if (cf.x == 0.0f && cf.z == 0.0f && cf.w == 0.0f) continue;  // skipped sample: every term is zero
+                const float4 pt = b_pos[row + y];
+                const bool need_t = y >= y_t && y < y_far;
+                const bool need_e = fabsf(t_gauss - pt.w) <= radius;
+                if (need_t || need_e) near_terms(rg, r, wr, pt, cf, need_t, need_e, dP, dR, ds, dmu, dtau_raw, dsh);
+            }
+            float far_dT = 0.0f;
+            if (y_far < H && far_T > 1e-6f) far_dT = b_suffix[row + y_far] / far_T;
+            instance_epilogue(rg, r, wr, far_dT, far_exp, dP, dR, ds, dmu, dtau_raw, dsh, quats, g,
+                              partial + (int64_t)PARTIAL_F4 * sorted_inst[s0 + k]);
         }
-        // the far factor, as the per-sample path evaluates it
-        const float psi = ray_integral(rg.o, rg.d, r.mu, r.s, r.R, 3.0e38f, wr);
-        const float far_exp = __expf(-psi);
-        const float far_T = r.tau + (1.0f - r.tau) * far_exp;
-        const int y_t = first_sample(t, H, [&](float tp) { return tp > t_gauss; });
-        const int y_e0 = first_sample(t, H, [&](float tp) { return tp >= t_gauss - radius; });
-        const int y_e1 = first_sample(t, H, [&](float tp) { return tp > t_gauss + radius; });
-        const int ya = min(y_t, y_e0), yb = max(y_far, y_e1);
-        for (int y = ya; y < yb; ++y) {
-            const float4 cf = b_coef[row + y];
-            if (cf.x == 0.0f && cf.z == 0.0f && cf.w == 0.0f) continue;  // skipped sample: every term is zero
-            const float4 pt = b_pos[row + y];
-            const bool need_t = y >= y_t && y < y_far;
-            const bool need_e = fabsf(t_gauss - pt.w) <= radius;
-            if (need_t || need_e) near_terms(rg, r, wr, pt, cf, need_t, need_e, dP, dR, ds, dmu, dtau_raw, dsh);
-        }
-        float far_dT = 0.0f;
-        if (y_far < H && far_T > 1e-6f) far_dT = b_suffix[row + y_far] / far_T;
-        instance_epilogue(rg, r, wr, far_dT, far_exp, dP, dR, ds, dmu, dtau_raw, dsh, quats, g,
-                          partial + (int64_t)PARTIAL_F4 * sorted_inst[s0 + k]);
     }
 }
 
