@@ -543,6 +543,7 @@ far_prefix_kernel(int W, int H, const long long* __restrict__ header, const int*
 // multiplies its checkpoint T_far by the window factors of the listed instances it has passed
 // but not left (t_gauss < t < tcw) and adds their echo terms, as the reference does.
 constexpr int LIST_CAP = 192;
+constexpr int SCAN_ROUND = 4;  // chunks of FWD_SAMPLES instances listed per block barrier
 
 __global__ void __launch_bounds__(FWD_SAMPLES)
 forward_ckpt_kernel(int W, int H, const int* __restrict__ ray_start, const int* __restrict__ sorted_gid,
@@ -553,9 +554,9 @@ forward_ckpt_kernel(int W, int H, const int* __restrict__ ray_start, const int* 
                     float wr, float* __restrict__ image, float4* __restrict__ pixel_state) {
     __shared__ float4 s_rec[LIST_CAP * REC_F4];
     __shared__ float4 s_aux[LIST_CAP];
-    __shared__ int s_list[LIST_CAP + FWD_SAMPLES];
-    __shared__ int s_n;
-    __shared__ int s_warp[FWD_SAMPLES / 32];
+    constexpr int NW = FWD_SAMPLES / 32;
+    __shared__ int s_list[LIST_CAP + SCAN_ROUND * FWD_SAMPLES];
+    __shared__ int s_cnt[2][SCAN_ROUND * NW];  // kept instances per (chunk, warp), double-buffered
     if (header[H_FLAGS] != 0) return;
     const int x = blockIdx.x;
     if (!mono[x]) return;
@@ -578,33 +579,43 @@ forward_ckpt_kernel(int W, int H, const int* __restrict__ ray_start, const int* 
     }
     float num = 0.0f, den = 0.0f, sacc = 0.0f;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) s_n = 0;
-    __syncthreads();
-    for (int k0 = 0; k0 < n; k0 += FWD_SAMPLES) {
-        // list the instances of this chunk that matter to the tile (order kept)
-        const int k = k0 + threadIdx.x;
-        bool keep = false;
-        if (k < n) {
-            const float4 a = aux[s0 + k];
-            const int y_far = __float_as_int(a.w);
-            keep = (y_far > y0 && a.x < t_hi) || (a.x + a.y >= t_lo && a.x - a.y <= t_hi);
-        }
-        const unsigned bits = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) s_warp[warp] = __popc(bits);
-        __syncthreads();
-        int base = s_n;
-        for (int w2 = 0; w2 < warp; ++w2) base += s_warp[w2];
-        if (keep) s_list[base + __popc(bits & ((1u << lane) - 1u))] = k;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int tot = s_n;
-            for (int w2 = 0; w2 < FWD_SAMPLES / 32; ++w2) tot += s_warp[w2];
-            s_n = tot;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    int nl = 0, par = 0;  // listed instances (the same in every thread), s_cnt buffer
+    for (int k0 = 0; k0 < n; k0 += SCAN_ROUND * FWD_SAMPLES) {
+        // list the instances of these chunks that matter to the tile (order kept): each chunk's
+        // warps count by ballot, one barrier publishes the counts, every thread then knows the
+        // offset of its own (chunk, warp) and the new list length
+        bool keep[SCAN_ROUND];
+        unsigned bits[SCAN_ROUND];
+#pragma unroll
+        for (int u = 0; u < SCAN_ROUND; ++u) {
+            const int k = k0 + u * FWD_SAMPLES + threadIdx.x;
+            keep[u] = false;
+            if (k < n) {
+                const float4 a = aux[s0 + k];
+                const int y_far = __float_as_int(a.w);
+                keep[u] = (y_far > y0 && a.x < t_hi) || (a.x + a.y >= t_lo && a.x - a.y <= t_hi);
+            }
+            bits[u] = __ballot_sync(0xffffffffu, keep[u]);
+            if (lane == 0) s_cnt[par][u * NW + warp] = __popc(bits[u]);
         }
         __syncthreads();
-        const int nl = s_n;
-        const bool last = k0 + FWD_SAMPLES >= n;
+        int off = nl;
+#pragma unroll
+        for (int u = 0; u < SCAN_ROUND; ++u) {
+            int base = off;
+            for (int w2 = 0; w2 < NW; ++w2) {
+                const int c = s_cnt[par][u * NW + w2];
+                if (w2 < warp) base += c;
+                off += c;
+            }
+            if (keep[u]) s_list[base + __popc(bits[u] & lt_mask)] = k0 + u * FWD_SAMPLES + threadIdx.x;
+        }
+        nl = off;
+        par ^= 1;
+        const bool last = k0 + SCAN_ROUND * FWD_SAMPLES >= n;
         if (nl < LIST_CAP && !last) continue;
+        __syncthreads();  // the list entries are written
         // stage and shade the listed instances (at most LIST_CAP at a time, in list order)
         for (int b0 = 0; b0 < nl; b0 += LIST_CAP) {
             const int nb = min(LIST_CAP, nl - b0);
@@ -638,8 +649,7 @@ forward_ckpt_kernel(int W, int H, const int* __restrict__ ray_start, const int* 
             }
             __syncthreads();
         }
-        if (threadIdx.x == 0) s_n = 0;
-        __syncthreads();
+        nl = 0;
     }
     if (!valid) return;
     float out = 0.0f;
